@@ -1,0 +1,185 @@
+/* wsg.h -- C ABI of libwsg, the B200 (sm_100a) w-gridder for WSClean.
+ *
+ * Two layers, both plain C (no CUDA or torch types in any signature):
+ *
+ *  1. The stateful gridder that replaces WSClean's WGriddingGridder_Simple<NumT>
+ *     behind its WGriddingGridderBase interface
+ *     (wgridder/wgriddinggridder_simple.h:8-22, ctor :64-68).  One
+ *     wsg_gridder_* entry point per virtual method; the C++ adapter
+ *     wsclean_b200/host/wgriddinggridder_b200.h turns the status codes back into
+ *     std::runtime_error so WSClean's ThreadedScheduler rethrow path
+ *     (scheduling/threadedscheduler.cpp:63-67) keeps working.
+ *
+ *  2. The raw operators ms2dirty / dirty2ms with ducc0's full argument set
+ *     (external/wgridder/ducc0/wgridder/wgridder.h:1696-1729): negate_v,
+ *     divide_by_n, sigma range, center_x/center_y, weights and mask.
+ *
+ * Pointers may be host (pageable or pinned) or device (cudaMalloc / managed)
+ * memory; the library asks the CUDA runtime which one it got and stages host
+ * buffers through the context's stream.  The caller owns every buffer for the
+ * duration of the call.  Every function returns WSG_OK (0) or an error code;
+ * wsg_last_error() gives the message for the calling thread.
+ *
+ * Thread safety: a context (wsg_ctx) or gridder is used by one thread at a
+ * time; different contexts are independent (each owns its stream, buffers and
+ * cuFFT plans), matching one gridder per -parallel-gridding worker
+ * (scheduling/threadedscheduler.cpp:54-58).
+ */
+#ifndef WSG_H
+#define WSG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WSG_ABI_VERSION 1
+
+/* Status codes.  WSG_ERR_INVALID covers the reference's MR_assert checks
+ * (odd image size, unsorted or non-positive frequencies, too many channels or
+ * w planes, no kernel for the requested epsilon). */
+enum {
+  WSG_OK = 0,
+  WSG_ERR_INVALID = 1,
+  WSG_ERR_CUDA = 2,
+  WSG_ERR_NOMEM = 3,
+  WSG_ERR_CUFFT = 4,
+  WSG_ERR_STATE = 5,
+  WSG_ERR_INTERNAL = 7
+};
+
+/* Arithmetic forms.  MIXED: FP32 kernel evaluation, spreading, grid and FFT;
+ * FP64 uvw->pixel scaling, phases, w-screen, image accumulation and
+ * correction.  FP64: everything in FP64 (the plain form). */
+enum { WSG_PREC_MIXED = 0, WSG_PREC_FP64 = 1 };
+/* element types */
+enum { WSG_C64 = 0, WSG_C128 = 1 };   /* complex<float>, complex<double> */
+enum { WSG_F32 = 0, WSG_F64 = 1 };    /* float, double */
+
+typedef struct wsg_ctx wsg_ctx;
+typedef struct wsg_gridder wsg_gridder;
+
+/* ---------------------------------------------------------------- context */
+
+/* An execution context on one CUDA device: its own stream, buffer cache and
+ * cuFFT plans.  device < 0 selects the current device. */
+int wsg_ctx_create(int device, wsg_ctx **out);
+int wsg_ctx_destroy(wsg_ctx *ctx);
+/* Optional: run on a caller-provided cudaStream_t (passed as void*). */
+int wsg_ctx_set_stream(wsg_ctx *ctx, void *stream);
+/* Releases the cached device buffers and cuFFT plans (they regrow on demand). */
+int wsg_ctx_release_buffers(wsg_ctx *ctx);
+
+/* ------------------------------------------------------- raw operators */
+
+/* ducc0's argument set (wgridder.h:1696-1729).  uvw: nrows x 3 doubles in
+ * metres; freq: nchan doubles in Hz, ascending; wgt: nrows x nchan of
+ * wgt_type or NULL (all ones); mask: nrows x nchan uint8 or NULL.  The dirty
+ * image is npix_x x npix_y, x-major (index i*npix_y + j, ducc0's dirty(i,j)). */
+typedef struct {
+  size_t nrows, nchan;
+  const double *uvw;
+  const double *freq;
+  const void *wgt;
+  int wgt_type;          /* WSG_F32 / WSG_F64 */
+  const uint8_t *mask;
+  size_t npix_x, npix_y;
+  double pixsize_x, pixsize_y;
+  double epsilon;
+  int do_wgridding;
+  int negate_v;
+  int divide_by_n;
+  double sigma_min, sigma_max;
+  double center_x, center_y;
+  int precision;         /* WSG_PREC_MIXED / WSG_PREC_FP64 */
+  int vis_type;          /* WSG_C64 / WSG_C128 */
+  int dirty_type;        /* WSG_F32 / WSG_F64 */
+} wsg_args;
+
+/* Fills a wsg_args with ducc0's defaults (negate_v=0, divide_by_n=1,
+ * sigma 1.1..2.6, no shift, MIXED, c64, f32). */
+void wsg_args_init(wsg_args *a);
+
+/* Replaces ducc0::ms2dirty (wgridder.h:1696-1710): dirty = gridded image of
+ * vis (nrows x nchan of vis_type).  If accumulate != 0 the result is added to
+ * dirty instead of overwriting it. */
+int wsg_ms2dirty(wsg_ctx *ctx, const wsg_args *a, const void *vis, void *dirty,
+                 int accumulate);
+/* Replaces ducc0::dirty2ms (wgridder.h:1712-1729), the exact adjoint. */
+int wsg_dirty2ms(wsg_ctx *ctx, const wsg_args *a, const void *dirty, void *vis);
+
+/* -------------------------------------- WGriddingGridder_Simple replacement */
+
+typedef struct {
+  size_t width, height;       /* untrimmed image (ActualInversionWidth/Height) */
+  size_t width_t, height_t;   /* trimmed image that is gridded */
+  double pixel_size_x, pixel_size_y;
+  double l_shift, m_shift;
+  size_t nthreads;            /* accepted for interface parity; unused */
+  double epsilon;
+  size_t verbosity;           /* 0..2 as in the reference */
+  int tuning;                 /* accepted; the GPU schedule is always used */
+  int precision;              /* WSG_PREC_MIXED (NumT=float) / WSG_PREC_FP64 (NumT=double) */
+  int device;                 /* CUDA device, <0 = current */
+} wsg_gridder_params;
+
+/* WGriddingGridder_Simple ctor (wgriddinggridder_simple.h:64-68). */
+int wsg_gridder_create(const wsg_gridder_params *p, wsg_gridder **out);
+int wsg_gridder_destroy(wsg_gridder *g);
+/* MemoryUsage (wgriddinggridder_simple.cpp:27-40): host-side budget figures
+ * WSClean uses to size its row chunks. */
+int wsg_gridder_memory_usage(const wsg_gridder *g, size_t *constant, size_t *per_vis);
+/* InitializeInversion (wgriddinggridder_simple.cpp:42-44): zero the image. */
+int wsg_gridder_initialize_inversion(wsg_gridder *g);
+/* AddInversionData (wgriddinggridder_simple.cpp:46-65): grid nrows x nchan
+ * complex<float> visibilities and add the image to the accumulator. */
+int wsg_gridder_add_inversion_data(wsg_gridder *g, size_t nrows, size_t nchan,
+                                   const double *uvw, const double *freq,
+                                   const void *vis);
+/* FinalizeImage (wgriddinggridder_simple.cpp:67-70). */
+int wsg_gridder_finalize_image(wsg_gridder *g, double factor);
+/* RealImage (wgriddinggridder_simple.cpp:72-83): writes width x height floats,
+ * index x + y*width, NaN outside the trimmed box. */
+int wsg_gridder_real_image(wsg_gridder *g, float *image);
+/* InitializePrediction (wgriddinggridder_simple.cpp:85-94): image is
+ * width x height floats, index x + y*width. */
+int wsg_gridder_initialize_prediction(wsg_gridder *g, const float *image);
+/* PredictVisibilities (wgriddinggridder_simple.cpp:96-115): writes nrows x
+ * nchan complex<float>. */
+int wsg_gridder_predict_visibilities(wsg_gridder *g, size_t nrows, size_t nchan,
+                                     const double *uvw, const double *freq,
+                                     void *vis);
+/* The gridder's execution context (for stats). */
+wsg_ctx *wsg_gridder_ctx(wsg_gridder *g);
+
+/* ------------------------------------------------------ stats / errors */
+
+/* Parameters and per-phase timings of the last operator call on a context
+ * (the analogue of ducc0's verbosity report and TimerHierarchy,
+ * wgridder.h:1535-1576 and infra/timers.h:69). Times are CUDA-event ms. */
+typedef struct {
+  size_t nrows, nchan, nvis;          /* nvis = active visibilities */
+  size_t nu, nv, nplanes, supp;       /* grid, w planes, kernel support W */
+  size_t plane_batch;                 /* planes resident per pass */
+  size_t band_rows;                   /* u rows that hold data (FFT pruning) */
+  size_t degree;                      /* kernel polynomial degree */
+  double sigma, beta, e0, kernel_err; /* chosen kernel and its error estimate */
+  double wmin, wmax, dw, nshift;
+  double ms_prep, ms_sort, ms_grid, ms_fft, ms_screen, ms_total;
+  size_t device_bytes;                /* device memory held by the context */
+  int gridding;                       /* 1 ms2dirty, 0 dirty2ms */
+  int precision;
+} wsg_stats;
+
+int wsg_get_stats(const wsg_ctx *ctx, wsg_stats *out);
+/* Message of the last failed call on this thread ("" if none). */
+const char *wsg_last_error(void);
+int wsg_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WSG_H */

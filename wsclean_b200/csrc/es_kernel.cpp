@@ -1,0 +1,385 @@
+// Host-side kernel mathematics and grid-parameter choice for libwsg.
+//
+// Reference counterparts (external/wgridder/ducc0/):
+//   es_phi               <- esknew                   math/gridding_kernel.cc:1538-1543
+//   available_kernels    <- getAvailableKernels      math/gridding_kernel.h:397-421
+//   fit_poly_kernel      <- getCoeffs/PolynomialKernel math/gridding_kernel.cc:28-75
+//   KernelTransform      <- GLFullCorrection/corfunc math/gridding_kernel.h:74-126
+//   choose_grid          <- Params::getNuNv + countRanges' plane placement
+//                           wgridder/wgridder.h:1503-1576, :690-699
+// The kernel table itself (es_kernel_db.inc) is generated by
+// wsclean_b200/kernel_db.py from an aliasing-error minimisation, and the
+// polynomial fit, quadrature and cost model are this library's own.
+#include <algorithm>
+#include <cmath>
+#include <limits>
+
+#include "wsg_internal.h"
+
+namespace wsg {
+
+namespace {
+
+struct TableRow {
+  int W;
+  double sigma, err1d, beta, e0;
+};
+
+const TableRow kTable[] = {
+#include "es_kernel_db.inc"
+};
+
+// FP32 arithmetic (kernel values, grid accumulation, FFT) limits the
+// achievable accuracy; kernels are never credited with less than this.
+constexpr double kFp32ErrFloor = 3e-7;
+constexpr int kMaxWFp32 = 8;
+
+// Gauss-Legendre nodes/weights on [-1,1] by Newton iteration on P_n.
+void gauss_legendre(int n, std::vector<double> &x, std::vector<double> &w) {
+  x.resize(n);
+  w.resize(n);
+  for (int i = 0; i < n; ++i) {
+    double z = std::cos(M_PI * (i + 0.75) / (n + 0.5));
+    double dp = 0;
+    for (int it = 0; it < 100; ++it) {
+      double p0 = 1.0, p1 = 0.0;
+      for (int j = 1; j <= n; ++j) {
+        double p2 = p1;
+        p1 = p0;
+        p0 = ((2.0 * j - 1.0) * z * p1 - (j - 1.0) * p2) / j;
+      }
+      dp = n * (z * p0 - p1) / (z * z - 1.0);
+      double dz = p0 / dp;
+      z -= dz;
+      if (std::fabs(dz) < 1e-16) break;
+    }
+    x[i] = z;
+    w[i] = 2.0 / ((1.0 - z * z) * dp * dp);
+  }
+}
+
+// Solves the (n x n) system A c = y in long double, partial pivoting.
+bool solve_ld(std::vector<long double> A, std::vector<long double> y, int n,
+              std::vector<long double> &c) {
+  for (int col = 0; col < n; ++col) {
+    int piv = col;
+    for (int r = col + 1; r < n; ++r)
+      if (std::fabs((double)A[r * n + col]) > std::fabs((double)A[piv * n + col]))
+        piv = r;
+    if (A[piv * n + col] == 0) return false;
+    if (piv != col) {
+      for (int k = 0; k < n; ++k) std::swap(A[col * n + k], A[piv * n + k]);
+      std::swap(y[col], y[piv]);
+    }
+    for (int r = col + 1; r < n; ++r) {
+      long double f = A[r * n + col] / A[col * n + col];
+      if (f == 0) continue;
+      for (int k = col; k < n; ++k) A[r * n + k] -= f * A[col * n + k];
+      y[r] -= f * y[col];
+    }
+  }
+  c.assign(n, 0);
+  for (int r = n - 1; r >= 0; --r) {
+    long double s = y[r];
+    for (int k = r + 1; k < n; ++k) s -= A[r * n + k] * c[k];
+    c[r] = s / A[r * n + r];
+  }
+  return true;
+}
+
+}  // namespace
+
+double es_phi(double t, int W, double beta, double e0) {
+  double s = (1.0 - t) * (1.0 + t);
+  if (s < 0) return 0.0;
+  return std::exp(beta * W * (std::pow(s, e0) - 1.0));
+}
+
+std::vector<KernelSpec> available_kernels(double epsilon, int ndim, bool fp32,
+                                          double sigma_min, double sigma_max) {
+  std::vector<KernelSpec> out;
+  const int wmax = fp32 ? kMaxWFp32 : kMaxW;
+  for (int W = 4; W <= wmax; ++W) {
+    const TableRow *best = nullptr;
+    for (const auto &r : kTable) {
+      if (r.W != W || r.sigma < sigma_min - 1e-9 || r.sigma > sigma_max + 1e-9)
+        continue;
+      double err = ndim * r.err1d;
+      if (fp32) err = std::max(err, kFp32ErrFloor);
+      if (err > epsilon) continue;
+      if (!best || r.sigma < best->sigma) best = &r;
+    }
+    if (best) {
+      double err = ndim * best->err1d;
+      if (fp32) err = std::max(err, kFp32ErrFloor);
+      out.push_back({W, best->sigma, err, best->beta, best->e0});
+    }
+  }
+  require(!out.empty(),
+          "no appropriate kernel found for epsilon=" + std::to_string(epsilon) +
+              (fp32 ? " in mixed precision (use FP64 for tighter epsilon)" : ""));
+  return out;
+}
+
+PolyKernel fit_poly_kernel(const KernelSpec &k, double target_err) {
+  const int W = k.W;
+  PolyKernel best;
+  // Test points: 97 per piece, including the piece edges.
+  const int ntest = 97;
+  for (int D = W + 1; D <= std::min(kMaxDeg, W + 10); ++D) {
+    const int n = D + 1;
+    std::vector<long double> A(n * n);
+    std::vector<double> xs(n);
+    for (int i = 0; i < n; ++i) {  // Chebyshev points of the first kind
+      xs[i] = std::cos(M_PI * (i + 0.5) / n);
+      long double p = 1;
+      for (int j = 0; j < n; ++j) {
+        A[i * n + j] = p;
+        p *= xs[i];
+      }
+    }
+    PolyKernel pk;
+    pk.W = W;
+    pk.D = D;
+    pk.coef.assign((size_t)n * W, 0.0);
+    double maxerr = 0;
+    bool ok = true;
+    for (int piece = 0; piece < W; ++piece) {
+      std::vector<long double> y(n), c;
+      for (int i = 0; i < n; ++i) {
+        double t = -1.0 + (2.0 * piece + 1.0 + xs[i]) / W;
+        y[i] = es_phi(t, W, k.beta, k.e0);
+      }
+      if (!solve_ld(A, y, n, c)) {
+        ok = false;
+        break;
+      }
+      for (int j = 0; j < n; ++j) pk.coef[(size_t)j * W + piece] = (double)c[j];
+      for (int s = 0; s < ntest; ++s) {
+        double x = -1.0 + 2.0 * s / (ntest - 1);
+        double t = -1.0 + (2.0 * piece + 1.0 + x) / W;
+        double v = 0;
+        for (int j = n - 1; j >= 0; --j) v = v * x + pk.coef[(size_t)j * W + piece];
+        maxerr = std::max(maxerr, std::fabs(v - es_phi(t, W, k.beta, k.e0)));
+      }
+    }
+    if (!ok) continue;
+    pk.max_err = maxerr;
+    best = pk;
+    if (maxerr <= target_err) break;
+  }
+  if (best.W == 0) throw std::runtime_error("kernel polynomial fit failed");
+  return best;
+}
+
+KernelTransform::KernelTransform(const KernelSpec &k) : W_(k.W) {
+  // composite rule on [0,1]: 64 panels x 16 nodes; phi has a branch point at
+  // t=1 which a single global rule resolves only to ~1e-12.
+  std::vector<double> gx, gw;
+  gauss_legendre(16, gx, gw);
+  const int npan = 64;
+  for (int p = 0; p < npan; ++p) {
+    double a = double(p) / npan, h = 1.0 / npan;
+    for (size_t i = 0; i < gx.size(); ++i) {
+      double t = a + 0.5 * h * (gx[i] + 1.0);
+      t_.push_back(t);
+      wphi_.push_back(0.5 * h * gw[i] * es_phi(t, k.W, k.beta, k.e0));
+    }
+  }
+}
+
+double KernelTransform::operator()(double nu) const {
+  // (W/2) * 2 * int_0^1 phi(t) cos(pi W nu t) dt
+  double s = 0;
+  const double f = M_PI * W_ * nu;
+  for (size_t i = 0; i < t_.size(); ++i) s += wphi_[i] * std::cos(f * t_[i]);
+  return W_ * s;
+}
+
+ChebCorr fit_cheb_corr(const KernelTransform &tr, double vmax) {
+  ChebCorr best;
+  double ymax = std::max(vmax * vmax, 1e-30);
+  for (int n = 8; n <= kMaxCheb; n += 4) {
+    ChebCorr cc;
+    cc.ymax = ymax;
+    cc.n = n;
+    cc.c.assign(n, 0.0);
+    std::vector<double> fv(n);
+    for (int k = 0; k < n; ++k) {
+      double xk = std::cos(M_PI * (k + 0.5) / n);
+      double y = 0.5 * (xk + 1.0) * ymax;
+      fv[k] = tr.corfunc(std::sqrt(y));
+    }
+    for (int j = 0; j < n; ++j) {
+      double s = 0;
+      for (int k = 0; k < n; ++k) s += fv[k] * std::cos(M_PI * j * (k + 0.5) / n);
+      cc.c[j] = (j == 0 ? 1.0 : 2.0) * s / n;
+    }
+    double maxrel = 0;
+    for (int s = 0; s <= 200; ++s) {
+      double y = ymax * s / 200.0;
+      double x = 2.0 * y / ymax - 1.0;
+      double b1 = 0, b2 = 0;  // Clenshaw
+      for (int j = n - 1; j >= 1; --j) {
+        double b0 = 2.0 * x * b1 - b2 + cc.c[j];
+        b2 = b1;
+        b1 = b0;
+      }
+      double v = x * b1 - b2 + cc.c[0];
+      double ref = tr.corfunc(std::sqrt(y));
+      maxrel = std::max(maxrel, std::fabs(v - ref) / std::fabs(ref));
+    }
+    cc.max_rel_err = maxrel;
+    best = cc;
+    if (maxrel < 2e-15) break;
+  }
+  return best;
+}
+
+size_t good_size_cufft(size_t n) {
+  if (n <= 2) return 2;
+  size_t best = 2 * n;
+  for (size_t f2 = 1; f2 < best; f2 *= 2)
+    for (size_t f3 = f2; f3 < best; f3 *= 3)
+      for (size_t f5 = f3; f5 < best; f5 *= 5)
+        for (size_t f7 = f5; f7 < best; f7 *= 7)
+          if (f7 >= n) best = std::min(best, f7);
+  return best;
+}
+
+namespace {
+
+int ceil_log2(uint64_t v) {
+  int b = 0;
+  while ((uint64_t(1) << b) < v) ++b;
+  return b;
+}
+
+// Occupied u band for a grid size: rows within W/2+2 cells of the largest
+// |u| (in cells) hold all footprints.
+void set_band(GridPlan &g) {
+  double umax_cells = g.umax * g.px * double(g.nu);
+  double L = std::ceil(umax_cells + 0.5 * g.kernel.W + 2.0);
+  if (!(L >= 0) || 2.0 * L + 1.0 >= double(g.nu)) {
+    g.band_full = true;
+    g.Lu = g.nu / 2;
+    g.band_rows = g.nu;
+  } else {
+    g.band_full = false;
+    g.Lu = size_t(L);
+    g.band_rows = 2 * g.Lu + 1;
+  }
+}
+
+}  // namespace
+
+void choose_grid(GridPlan &g, double sigma_min, double sigma_max, int tile) {
+  require(g.nx % 2 == 0, "nx_dirty must be even");
+  require(g.ny % 2 == 0, "ny_dirty must be even");
+  require(g.eps > 0, "epsilon must be positive");
+  require(g.px > 0, "pixsize_x must be positive");
+  require(g.py > 0, "pixsize_y must be positive");
+  // n-1 range over the image corners (and axes crossings), as the reference
+  // does in getNuNv (wgridder.h:1507-1525).
+  double xmin = g.lshift - 0.5 * g.nx * g.px, xmax = xmin + (g.nx - 1) * g.px;
+  double ymin = g.mshift - 0.5 * g.ny * g.py, ymax = ymin + (g.ny - 1) * g.py;
+  std::vector<double> xe{xmin, xmax}, ye{ymin, ymax};
+  if (xmin * xmax < 0) xe.push_back(0.0);
+  if (ymin * ymax < 0) ye.push_back(0.0);
+  g.nm1min = 1e300;
+  g.nm1max = -1e300;
+  for (double xc : xe)
+    for (double yc : ye) {
+      double r2 = xc * xc + yc * yc;
+      double nv = (r2 <= 1.0) ? std::sqrt(1.0 - r2) - 1.0 : -std::sqrt(r2 - 1.0) - 1.0;
+      g.nm1min = std::min(g.nm1min, nv);
+      g.nm1max = std::max(g.nm1max, nv);
+    }
+  g.lmshift = (g.lshift != 0) || (g.mshift != 0);
+  g.nshift = g.do_w ? -0.5 * (g.nm1max + g.nm1min) : 0.0;
+  g.shifting = g.lmshift || (g.nshift != 0);
+  double nmax = std::max(std::fabs(g.nm1max + g.nshift), std::fabs(g.nm1min + g.nshift));
+  if (g.do_w) require(nmax > 0, "image too small for w-gridding (n-1 range is zero)");
+
+  auto cands = available_kernels(g.eps, g.do_w ? 3 : 2, g.fp32, sigma_min, sigma_max);
+  // Cost model (seconds): FFT-stage memory traffic per plane -- pruned pass
+  // along v over the occupied u band, pass along u over the image columns,
+  // w-screen over the image -- plus the spreading work nvis*W^3.
+  const double cs = g.fp32 ? 8.0 : 16.0;
+  const double hbm = 5.0e12;
+  const double c_cell = g.fp32 ? 2.0e-13 : 1.2e-12;
+  double best = 1e300;
+  KernelSpec bestk{};
+  size_t bnu = 0, bnv = 0;
+  for (const auto &k : cands) {
+    GridPlan t = g;
+    t.kernel = k;
+    t.nu = 2 * good_size_cufft(size_t(g.nx * k.sigma * 0.5) + 1);
+    t.nv = 2 * good_size_cufft(size_t(g.ny * k.sigma * 0.5) + 1);
+    set_band(t);
+    double planes = 1;
+    if (g.do_w) {
+      double of = std::min(double(t.nu) / g.nx, double(t.nv) / g.ny);
+      double dw = 0.5 / of / nmax;
+      planes = std::floor((g.wmax_d - g.wmin_d) / dw + k.W);
+    }
+    double per_plane = cs * (3.0 * t.band_rows * t.nv + 2.0 * t.nu * g.ny + 1.0 * g.nx * g.ny);
+    double fft = planes * per_plane / hbm;
+    double grid = double(g.nvis) * k.W * k.W * (g.do_w ? k.W : 1) * c_cell;
+    double cost = fft + grid;
+    if (cost < best) {
+      best = cost;
+      bestk = k;
+      bnu = t.nu;
+      bnv = t.nv;
+    }
+  }
+  g.kernel = bestk;
+  g.nu = bnu;
+  g.nv = bnv;
+  g.ofactor = std::min(double(g.nu) / g.nx, double(g.nv) / g.ny);
+  const int W = bestk.W;
+  g.nsafe = (W + 1) / 2;
+  g.ushift = W * (-0.5) + 1 + double(g.nu);
+  g.vshift = W * (-0.5) + 1 + double(g.nv);
+  g.maxiu0 = int(g.nu + g.nsafe) - W;
+  g.maxiv0 = int(g.nv + g.nsafe) - W;
+  require(g.nu >= size_t(2 * g.nsafe) && g.nv >= size_t(2 * g.nsafe), "grid too small");
+  require(g.nu + size_t(g.nsafe) < 65535 && g.nv + size_t(g.nsafe) < 65535, "grid too large");
+  if (g.do_w) {
+    g.dw = 0.5 / g.ofactor / nmax;
+    g.xdw = 1.0 / g.dw;
+    g.nplanes = size_t((g.wmax_d - g.wmin_d) / g.dw + W);
+    require(g.nplanes < (size_t(1) << 16), "too many w planes");
+    g.wmin = (g.wmin_d + g.wmax_d) * 0.5 - 0.5 * (double(g.nplanes) - 1) * g.dw;
+    g.wshift = g.dw - (0.5 * W * g.dw) - g.wmin;
+  } else {
+    g.dw = g.xdw = g.wmin = g.wshift = 0;
+    g.nplanes = 1;
+  }
+  set_band(g);
+  double target = g.fp32 ? std::max(0.02 * g.kernel.err, 2e-8) : 0.02 * g.kernel.err;
+  g.poly = fit_poly_kernel(g.kernel, target);
+
+  g.T = tile;
+  g.ntu = int((g.nu + 1) / tile) + 1;
+  g.ntv = int((g.nv + 1) / tile) + 1;
+  g.nwmin = g.do_w ? int(g.nplanes) - W + 1 : 1;
+  uint64_t nbins = uint64_t(g.ntu) * g.ntv * g.nwmin;
+  int bin_bits = ceil_log2(nbins);
+  require(bin_bits <= 30, "too many (tile, w-plane) bins for 31-bit sort keys");
+  int tbits = ceil_log2(uint64_t(tile));
+  g.lbits = std::min(tbits, (30 - bin_bits) / 2);
+  g.key_bits = bin_bits + 2 * g.lbits;
+}
+
+size_t plan_bytes(const GridPlan &g, size_t planes, bool gridding) {
+  size_t cs = g.fp32 ? 8 : 16;
+  size_t band = g.band_rows * planes * g.nv * cs;
+  size_t full = g.nu * planes * g.nv * cs;
+  size_t h = planes * g.ny * g.nu * cs;
+  (void)gridding;
+  return band + full + h;
+}
+
+}  // namespace wsg

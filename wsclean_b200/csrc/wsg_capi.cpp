@@ -1,0 +1,195 @@
+// extern "C" layer of libwsg: maps C++ exceptions to status codes and keeps
+// a per-thread error message (the reference throws std::runtime_error from
+// MR_assert; the C++ adapter in wsclean_b200/host rethrows from the codes).
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "../../include/wsg.h"
+#include "wsg_context.h"
+
+#include <memory>
+
+// A context handle either owns its Context or views the one inside a gridder.
+struct wsg_ctx {
+  std::unique_ptr<wsg::Context> own;
+  wsg::Context *ctx = nullptr;
+};
+struct wsg_gridder {
+  wsg::Gridder impl;
+  wsg_ctx view;
+  explicit wsg_gridder(const wsg_gridder_params &p) : impl(p) { view.ctx = &impl.context(); }
+};
+
+namespace {
+thread_local std::string g_last_error;
+
+template <typename F>
+int guarded(F &&f) {
+  try {
+    f();
+    g_last_error.clear();
+    return WSG_OK;
+  } catch (const wsg::InvalidArgument &e) {
+    g_last_error = e.what();
+    return WSG_ERR_INVALID;
+  } catch (const wsg::OutOfMemory &e) {
+    g_last_error = e.what();
+    return WSG_ERR_NOMEM;
+  } catch (const std::bad_alloc &e) {
+    g_last_error = "host allocation failed";
+    return WSG_ERR_NOMEM;
+  } catch (const wsg::CufftError &e) {
+    g_last_error = e.what();
+    return WSG_ERR_CUFFT;
+  } catch (const wsg::CudaError &e) {
+    g_last_error = e.what();
+    return WSG_ERR_CUDA;
+  } catch (const std::exception &e) {
+    g_last_error = e.what();
+    return WSG_ERR_INTERNAL;
+  }
+}
+}  // namespace
+
+extern "C" {
+
+int wsg_abi_version(void) { return WSG_ABI_VERSION; }
+
+const char *wsg_last_error(void) { return g_last_error.c_str(); }
+
+void wsg_args_init(wsg_args *a) {
+  std::memset(a, 0, sizeof(*a));
+  a->wgt_type = WSG_F32;
+  a->do_wgridding = 1;
+  a->negate_v = 0;
+  a->divide_by_n = 1;
+  a->sigma_min = 1.1;
+  a->sigma_max = 2.6;
+  a->precision = WSG_PREC_MIXED;
+  a->vis_type = WSG_C64;
+  a->dirty_type = WSG_F32;
+}
+
+int wsg_ctx_create(int device, wsg_ctx **out) {
+  return guarded([&] {
+    wsg::require(out != nullptr, "out is NULL");
+    auto *h = new wsg_ctx;
+    try {
+      h->own.reset(new wsg::Context(device));
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    h->ctx = h->own.get();
+    *out = h;
+  });
+}
+
+int wsg_ctx_destroy(wsg_ctx *ctx) {
+  return guarded([&] {
+    wsg::require(ctx == nullptr || ctx->own != nullptr, "a gridder's context is destroyed with the gridder");
+    delete ctx;
+  });
+}
+
+int wsg_ctx_set_stream(wsg_ctx *ctx, void *stream) {
+  return guarded([&] {
+    wsg::require(ctx != nullptr, "ctx is NULL");
+    ctx->ctx->stream = stream ? reinterpret_cast<cudaStream_t>(stream) : ctx->ctx->own_stream;
+  });
+}
+
+int wsg_ctx_release_buffers(wsg_ctx *ctx) {
+  return guarded([&] {
+    wsg::require(ctx != nullptr, "ctx is NULL");
+    ctx->ctx->release_buffers();
+  });
+}
+
+int wsg_ms2dirty(wsg_ctx *ctx, const wsg_args *a, const void *vis, void *dirty, int accumulate) {
+  return guarded([&] {
+    wsg::require(ctx && a, "ctx and args are required");
+    ctx->ctx->ms2dirty(*a, vis, dirty, accumulate);
+  });
+}
+
+int wsg_dirty2ms(wsg_ctx *ctx, const wsg_args *a, const void *dirty, void *vis) {
+  return guarded([&] {
+    wsg::require(ctx && a, "ctx and args are required");
+    ctx->ctx->dirty2ms(*a, dirty, vis);
+  });
+}
+
+int wsg_get_stats(const wsg_ctx *ctx, wsg_stats *out) {
+  return guarded([&] {
+    wsg::require(ctx && out, "ctx and out are required");
+    *out = ctx->ctx->stats;
+  });
+}
+
+int wsg_gridder_create(const wsg_gridder_params *p, wsg_gridder **out) {
+  return guarded([&] {
+    wsg::require(p && out, "params and out are required");
+    *out = new wsg_gridder(*p);
+  });
+}
+
+int wsg_gridder_destroy(wsg_gridder *g) {
+  return guarded([&] { delete g; });
+}
+
+int wsg_gridder_memory_usage(const wsg_gridder *g, size_t *constant, size_t *per_vis) {
+  return guarded([&] {
+    wsg::require(g && constant && per_vis, "NULL argument");
+    g->impl.memory_usage(*constant, *per_vis);
+  });
+}
+
+int wsg_gridder_initialize_inversion(wsg_gridder *g) {
+  return guarded([&] {
+    wsg::require(g, "gridder is NULL");
+    g->impl.initialize_inversion();
+  });
+}
+
+int wsg_gridder_add_inversion_data(wsg_gridder *g, size_t nrows, size_t nchan, const double *uvw,
+                                   const double *freq, const void *vis) {
+  return guarded([&] {
+    wsg::require(g, "gridder is NULL");
+    g->impl.add_inversion_data(nrows, nchan, uvw, freq, vis);
+  });
+}
+
+int wsg_gridder_finalize_image(wsg_gridder *g, double factor) {
+  return guarded([&] {
+    wsg::require(g, "gridder is NULL");
+    g->impl.finalize_image(factor);
+  });
+}
+
+int wsg_gridder_real_image(wsg_gridder *g, float *image) {
+  return guarded([&] {
+    wsg::require(g && image, "NULL argument");
+    g->impl.real_image(image);
+  });
+}
+
+int wsg_gridder_initialize_prediction(wsg_gridder *g, const float *image) {
+  return guarded([&] {
+    wsg::require(g, "gridder is NULL");
+    g->impl.initialize_prediction(image);
+  });
+}
+
+int wsg_gridder_predict_visibilities(wsg_gridder *g, size_t nrows, size_t nchan,
+                                     const double *uvw, const double *freq, void *vis) {
+  return guarded([&] {
+    wsg::require(g && vis, "NULL argument");
+    g->impl.predict_visibilities(nrows, nchan, uvw, freq, vis);
+  });
+}
+
+wsg_ctx *wsg_gridder_ctx(wsg_gridder *g) { return g ? &g->view : nullptr; }
+
+}  // extern "C"

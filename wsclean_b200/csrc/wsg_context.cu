@@ -1,0 +1,1049 @@
+// Host orchestration of libwsg: execution contexts, buffer cache, cuFFT plans,
+// and the ms2dirty / dirty2ms drivers (the analogues of ducc0's
+// Params::x2dirty and Params::dirty2x, wgridder.h:1430-1501).
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_select.cuh>
+#include <thrust/iterator/counting_iterator.h>
+
+#include "wsg_context.h"
+#include "wsg_device.cuh"
+
+namespace wsg {
+
+// ------------------------------------------------------------ utilities
+
+void cuda_check(cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return;
+  cudaGetLastError();
+  if (e == cudaErrorMemoryAllocation)
+    throw OutOfMemory(std::string(what) + ": " + cudaGetErrorString(e));
+  throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define CK(x) cuda_check((x), #x)
+
+static void cufft_check(cufftResult r, const char *what) {
+  if (r == CUFFT_SUCCESS) return;
+  if (r == CUFFT_ALLOC_FAILED) throw OutOfMemory(std::string(what) + ": cuFFT allocation failed");
+  throw CufftError(std::string(what) + ": cuFFT error " + std::to_string(int(r)));
+}
+#define CF(x) cufft_check((x), #x)
+
+bool is_device_pointer(const void *p) {
+  if (!p) return false;
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+void *DevBuf::ensure(size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  if (n < bytes) {
+    release();
+    cuda_check(cudaMalloc(&p, bytes), "cudaMalloc");
+    n = bytes;
+  }
+  return p;
+}
+
+void DevBuf::release() {
+  if (p) cudaFree(p);
+  p = nullptr;
+  n = 0;
+}
+
+static int env_int(const char *name, int dflt) {
+  const char *s = std::getenv(name);
+  return (s && *s) ? std::atoi(s) : dflt;
+}
+
+// --------------------------------------------------------------- context
+
+Context::Context(int dev) {
+  if (dev < 0) CK(cudaGetDevice(&dev));
+  device = dev;
+  CK(cudaSetDevice(device));
+  CK(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
+  stream = own_stream;
+  CK(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
+  for (auto &e : ev) CK(cudaEventCreate(&e));
+  std::memset(&stats, 0, sizeof(stats));
+}
+
+Context::~Context() {
+  cudaSetDevice(device);
+  if (stream) cudaStreamSynchronize(stream);
+  for (auto &kv : fft_plans) cufftDestroy(kv.second);
+  for (auto *b : all_buffers()) b->release();
+  for (auto &e : ev) cudaEventDestroy(e);
+  if (own_stream) cudaStreamDestroy(own_stream);
+}
+
+std::vector<DevBuf *> Context::all_buffers() {
+  return {&b_uvw, &b_fovc, &b_vis, &b_wgt, &b_mask, &b_keys_a, &b_keys_b, &b_vals_a,
+          &b_vals_b, &b_cub, &b_rec, &b_chunks, &b_small, &b_band, &b_full_fwd,
+          &b_full_adj, &b_H, &b_img, &b_img2, &b_acc, &b_cf, &b_fftwork, &b_out};
+}
+
+void Context::release_buffers() {
+  CK(cudaSetDevice(device));
+  CK(cudaStreamSynchronize(stream));
+  for (auto &kv : fft_plans) cufftDestroy(kv.second);
+  fft_plans.clear();
+  for (auto *b : all_buffers()) b->release();
+  fwd_layout = adj_layout = {};
+  fwd_L = 0;
+  H_clean = false;
+}
+
+size_t Context::device_bytes() {
+  size_t s = 0;
+  for (auto *b : all_buffers()) s += b->n;
+  return s;
+}
+
+cufftHandle Context::fft_plan(int n, int istride, int idist, int ostride, int odist,
+                              int batch, bool dbl) {
+  auto key = std::make_tuple(n, istride, idist, ostride, odist, batch, int(dbl));
+  auto it = fft_plans.find(key);
+  if (it != fft_plans.end()) return it->second;
+  cufftHandle h;
+  CF(cufftCreate(&h));
+  CF(cufftSetAutoAllocation(h, 0));
+  int nn = n, inembed = n, onembed = n;
+  size_t work = 0;
+  CF(cufftMakePlanMany(h, 1, &nn, &inembed, istride, idist, &onembed, ostride, odist,
+                       dbl ? CUFFT_Z2Z : CUFFT_C2C, batch, &work));
+  fft_work_need = std::max(fft_work_need, work);
+  fft_plans[key] = h;
+  return h;
+}
+
+void Context::fft_exec(cufftHandle h, void *in, void *out, int dir, bool dbl) {
+  void *work = b_fftwork.ensure(std::max<size_t>(fft_work_need, 256));
+  CF(cufftSetStream(h, stream));
+  CF(cufftSetWorkArea(h, work));
+  if (dbl)
+    CF(cufftExecZ2Z(h, reinterpret_cast<cufftDoubleComplex *>(in),
+                    reinterpret_cast<cufftDoubleComplex *>(out), dir));
+  else
+    CF(cufftExecC2C(h, reinterpret_cast<cufftComplex *>(in),
+                    reinterpret_cast<cufftComplex *>(out), dir));
+}
+
+// ------------------------------------------------------------ staging
+
+// Returns a device pointer holding `bytes` of p: p itself if it is device
+// memory, else a copy in buf (asynchronous on the context stream).
+const void *Context::stage_in(const void *p, size_t bytes, DevBuf &buf) {
+  if (!p) return nullptr;
+  if (is_device_pointer(p)) return p;
+  void *d = buf.ensure(bytes);
+  CK(cudaMemcpyAsync(d, p, bytes, cudaMemcpyHostToDevice, stream));
+  return d;
+}
+
+// ------------------------------------------------------------- planning
+
+namespace {
+
+DevGeom make_geom(const GridPlan &g) {
+  DevGeom d{};
+  d.nu = int(g.nu);
+  d.nv = int(g.nv);
+  d.W = g.kernel.W;
+  d.nsafe = g.nsafe;
+  d.maxiu0 = g.maxiu0;
+  d.maxiv0 = g.maxiv0;
+  d.px = g.px;
+  d.py = g.py;
+  d.ushift = g.ushift;
+  d.vshift = g.vshift;
+  d.wmin = g.wmin;
+  d.dw = g.dw;
+  d.xdw = g.xdw;
+  d.wshift = g.wshift;
+  d.nplanes = int(g.nplanes);
+  d.do_w = g.do_w;
+  d.lshift = g.lshift;
+  d.mshift = g.mshift;
+  d.nshift = g.nshift;
+  d.vfac = g.negate_v ? -1.0 : 1.0;
+  d.shifting = g.shifting;
+  d.T = g.T;
+  d.ntu = g.ntu;
+  d.ntv = g.ntv;
+  d.nwmin = g.nwmin;
+  d.lbits = g.lbits;
+  int tb = 0;
+  while ((1 << tb) < g.T) ++tb;
+  d.qshift = tb - g.lbits;
+  d.inactive_key = 1u << g.key_bits;
+  d.Lu = int(g.Lu);
+  d.band_rows = int(g.band_rows);
+  d.band_full = g.band_full;
+  return d;
+}
+
+template <typename R>
+DevKernel<R> make_kernel(const PolyKernel &pk) {
+  DevKernel<R> k;
+  std::memset(&k, 0, sizeof(k));
+  k.D = pk.D;
+  for (int j = 0; j <= pk.D; ++j)
+    for (int i = 0; i < pk.W; ++i) k.c[j][i] = R(pk.coef[size_t(j) * pk.W + i]);
+  return k;
+}
+
+TileLayout make_layout(int T, int W) {
+  TileLayout tl;
+  tl.S = T + W - 1;
+  tl.RS = tl.S | 1;  // odd row stride
+  int ps = tl.S * tl.RS;
+  tl.PS = ps + ((8 - (ps % 32)) + 32) % 32;  // plane stride = 8 mod 32
+  return tl;
+}
+
+int launch_blocks(size_t n, int threads) {
+  size_t b = (n + threads - 1) / threads;
+  return int(std::min<size_t>(std::max<size_t>(b, 1), 65535 * 8));
+}
+
+}  // namespace
+
+// Kernel template dispatch over the support W.
+template <typename R>
+struct GridKernels {
+  static constexpr int NWARP = sizeof(R) == 4 ? 8 : 16;
+  static constexpr int SB = sizeof(R) == 4 ? 256 : 64;
+  template <int W>
+  static constexpr int ppl() {
+    return (sizeof(R) == 4 && W * W > 32) ? 2 : 1;
+  }
+  static size_t smem_bytes(const TileLayout &tl, int W, bool spread) {
+    size_t kst = 3 * W + 1;
+    size_t s = sizeof(R) * (2 * size_t(W) * tl.PS + SB * kst + 2 * SB) + 4 * SB;
+    (void)spread;
+    return (s + 15) & ~size_t(15);
+  }
+  template <int W>
+  static void run(bool spread, dim3 grid, size_t smem, cudaStream_t st, const GridArgs &a,
+                  const DevGeom &g, const DevKernel<R> &kc) {
+    constexpr int P = ppl<W>();
+    if (spread) {
+      auto fn = k_spread<R, W, P, NWARP>;
+      cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+                 "smem attribute");
+      fn<<<grid, NWARP * 32, smem, st>>>(a, g, kc);
+    } else {
+      auto fn = k_interp<R, W, P, NWARP>;
+      cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+                 "smem attribute");
+      fn<<<grid, NWARP * 32, smem, st>>>(a, g, kc);
+    }
+    cuda_check(cudaGetLastError(), spread ? "k_spread launch" : "k_interp launch");
+  }
+  template <int W>
+  static int occupancy(bool spread, size_t smem) {
+    constexpr int P = ppl<W>();
+    int nb = 0;
+    if (spread)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_spread<R, W, P, NWARP>, NWARP * 32, smem);
+    else
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_interp<R, W, P, NWARP>, NWARP * 32, smem);
+    return std::max(nb, 1);
+  }
+  static void dispatch(int W, bool spread, int nsm, size_t smem, cudaStream_t st, const GridArgs &a,
+                       const DevGeom &g, const DevKernel<R> &kc) {
+    auto go = [&](auto wc) {
+      constexpr int WW = decltype(wc)::value;
+      if constexpr (sizeof(R) == 4 && WW > 8) {
+        throw std::runtime_error("support too large for mixed precision");
+      } else {
+        // set the smem attribute before asking for the occupancy
+        constexpr int P = ppl<WW>();
+        if (spread)
+          cuda_check(cudaFuncSetAttribute(k_spread<R, WW, P, NWARP>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+                     "smem attribute");
+        else
+          cuda_check(cudaFuncSetAttribute(k_interp<R, WW, P, NWARP>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+                     "smem attribute");
+        int occ = occupancy<WW>(spread, smem);
+        dim3 grid(nsm * occ);
+        run<WW>(spread, grid, smem, st, a, g, kc);
+      }
+    };
+    switch (W) {
+      case 4: go(std::integral_constant<int, 4>{}); break;
+      case 5: go(std::integral_constant<int, 5>{}); break;
+      case 6: go(std::integral_constant<int, 6>{}); break;
+      case 7: go(std::integral_constant<int, 7>{}); break;
+      case 8: go(std::integral_constant<int, 8>{}); break;
+      case 9: go(std::integral_constant<int, 9>{}); break;
+      case 10: go(std::integral_constant<int, 10>{}); break;
+      case 11: go(std::integral_constant<int, 11>{}); break;
+      case 12: go(std::integral_constant<int, 12>{}); break;
+      case 13: go(std::integral_constant<int, 13>{}); break;
+      case 14: go(std::integral_constant<int, 14>{}); break;
+      case 15: go(std::integral_constant<int, 15>{}); break;
+      case 16: go(std::integral_constant<int, 16>{}); break;
+      default: throw std::runtime_error("unsupported kernel support");
+    }
+  }
+};
+
+// ------------------------------------------------------------ the driver
+
+namespace {
+
+template <typename TW, typename TV>
+void launch_scan(Context &cx, const wsg_args &a, const Staged &s, bool gridding, TV *vis_out,
+                 ScanOut *d_out) {
+  int nb = launch_blocks(a.nrows, 256);
+  nb = std::min(nb, cx.num_sms * 8);
+  k_scan<TV, TW><<<nb, 256, 0, cx.stream>>>(
+      a.nrows, int(a.nchan), s.uvw, s.fovc, reinterpret_cast<const TV *>(s.vis),
+      reinterpret_cast<const TW *>(s.wgt), s.mask, gridding ? 1 : 0, a.negate_v ? -1.0 : 1.0,
+      d_out, vis_out);
+  cuda_check(cudaGetLastError(), "k_scan launch");
+}
+
+template <typename TW, typename TV>
+void launch_keys(Context &cx, const wsg_args &a, const Staged &s, bool gridding, const DevGeom &g,
+                 uint32_t *keys, uint32_t *vals) {
+  int nb = launch_blocks(a.nrows, 256);
+  k_keys<TV, TW><<<nb, 256, 0, cx.stream>>>(a.nrows, int(a.nchan), s.uvw, s.fovc,
+                                            reinterpret_cast<const TV *>(s.vis),
+                                            reinterpret_cast<const TW *>(s.wgt), s.mask,
+                                            gridding ? 1 : 0, g, keys, vals);
+  cuda_check(cudaGetLastError(), "k_keys launch");
+}
+
+template <typename R, typename TW, typename TV>
+void launch_records(Context &cx, size_t nvis, const wsg_args &a, const Staged &s, bool gridding,
+                    const DevGeom &g, const uint32_t *sidx, void *rec) {
+  int nb = launch_blocks(nvis, 256);
+  k_records<R, TV, TW><<<nb, 256, 0, cx.stream>>>(
+      nvis, int(a.nchan), sidx, s.uvw, s.fovc, reinterpret_cast<const TV *>(s.vis),
+      reinterpret_cast<const TW *>(s.wgt), gridding ? 1 : 0, g,
+      reinterpret_cast<typename RecOf<R>::type *>(rec));
+  cuda_check(cudaGetLastError(), "k_records launch");
+}
+
+// type-dispatch helpers over (weight type, vis type)
+template <typename F>
+void with_types(const wsg_args &a, F &&f) {
+  bool wd = a.wgt && a.wgt_type == WSG_F64;
+  bool vd = a.vis_type == WSG_C128;
+  if (wd && vd) f((double *)nullptr, (double2 *)nullptr);
+  else if (wd) f((double *)nullptr, (float2 *)nullptr);
+  else if (vd) f((float *)nullptr, (double2 *)nullptr);
+  else f((float *)nullptr, (float2 *)nullptr);
+}
+
+}  // namespace
+
+void Context::validate(const wsg_args &a) {
+  require(a.uvw && a.freq, "uvw and freq are required");
+  require(a.nrows < (size_t(1) << 32), "too many rows in the MS");
+  require(a.nchan < (size_t(1) << 16), "too many channels in the MS");
+  require(a.nrows * a.nchan < (size_t(1) << 31), "at most 2^31-1 visibilities per call");
+  require(a.npix_x % 2 == 0, "nx_dirty must be even");
+  require(a.npix_y % 2 == 0, "ny_dirty must be even");
+  require(a.epsilon > 0, "epsilon must be positive");
+  require(a.pixsize_x > 0, "pixsize_x must be positive");
+  require(a.pixsize_y > 0, "pixsize_y must be positive");
+  require(a.precision == WSG_PREC_MIXED || a.precision == WSG_PREC_FP64, "bad precision");
+  require(a.vis_type == WSG_C64 || a.vis_type == WSG_C128, "bad vis_type");
+  require(a.dirty_type == WSG_F32 || a.dirty_type == WSG_F64, "bad dirty_type");
+  require(a.sigma_min > 1.0 && a.sigma_max >= a.sigma_min, "bad sigma range");
+}
+
+// Scans the data, chooses the grid, sorts and builds records.  Returns false
+// if no visibility is active.
+template <typename R>
+bool Context::prepare(const wsg_args &a, const Staged &s, bool gridding, void *vis_out_dev,
+                      GridPlan &gp) {
+  const size_t nvis_tot = a.nrows * a.nchan;
+  // freq checks (Baselines ctor, wgridder.h:300-309) and f/c
+  std::vector<double> freq(a.nchan), fovc(a.nchan);
+  if (is_device_pointer(a.freq))
+    CK(cudaMemcpy(freq.data(), a.freq, a.nchan * sizeof(double), cudaMemcpyDeviceToHost));
+  else
+    std::memcpy(freq.data(), a.freq, a.nchan * sizeof(double));
+  for (size_t i = 0; i < a.nchan; ++i) {
+    require(freq[i] > 0, "negative channel frequency encountered");
+    if (i > 0) require(freq[i] >= freq[i - 1], "channel frequencies must be sorted in ascending order");
+    fovc[i] = freq[i] / kSpeedOfLight;
+  }
+  double *d_fovc = reinterpret_cast<double *>(b_fovc.ensure(a.nchan * sizeof(double)));
+  CK(cudaMemcpyAsync(d_fovc, fovc.data(), a.nchan * sizeof(double), cudaMemcpyHostToDevice, stream));
+  Staged st = s;
+  st.fovc = d_fovc;
+
+  // scan
+  ScanOut h0{};
+  h0.wmin_bits = 0x7ff0000000000000ull;
+  ScanOut *d_scan = reinterpret_cast<ScanOut *>(b_small.ensure(4096));
+  CK(cudaMemcpyAsync(d_scan, &h0, sizeof(h0), cudaMemcpyHostToDevice, stream));
+  with_types(a, [&](auto *tw, auto *tv) {
+    using TW = std::remove_pointer_t<decltype(tw)>;
+    using TV = std::remove_pointer_t<decltype(tv)>;
+    launch_scan<TW, TV>(*this, a, st, gridding, reinterpret_cast<TV *>(vis_out_dev), d_scan);
+  });
+  ScanOut hs;
+  CK(cudaMemcpyAsync(&hs, d_scan, sizeof(hs), cudaMemcpyDeviceToHost, stream));
+  CK(cudaStreamSynchronize(stream));
+  gp.nvis = hs.nvis;
+  if (gp.nvis == 0) return false;
+  auto bits2d = [](unsigned long long b) {
+    double d;
+    std::memcpy(&d, &b, 8);
+    return d;
+  };
+  gp.wmin_d = bits2d(hs.wmin_bits);
+  gp.wmax_d = bits2d(hs.wmax_bits);
+  gp.umax = bits2d(hs.umax_bits);
+  gp.vmax = bits2d(hs.vmax_bits);
+
+  int tile = env_int("WSG_TILE", sizeof(R) == 4 ? 16 : 8);
+  choose_grid(gp, a.sigma_min, a.sigma_max, tile);
+  DevGeom g = make_geom(gp);
+
+  // keys + sort
+  uint32_t *ka = reinterpret_cast<uint32_t *>(b_keys_a.ensure(nvis_tot * 4));
+  uint32_t *kb = reinterpret_cast<uint32_t *>(b_keys_b.ensure(nvis_tot * 4));
+  uint32_t *va = reinterpret_cast<uint32_t *>(b_vals_a.ensure(nvis_tot * 4));
+  uint32_t *vb = reinterpret_cast<uint32_t *>(b_vals_b.ensure(nvis_tot * 4));
+  with_types(a, [&](auto *tw, auto *tv) {
+    using TW = std::remove_pointer_t<decltype(tw)>;
+    using TV = std::remove_pointer_t<decltype(tv)>;
+    launch_keys<TW, TV>(*this, a, st, gridding, g, ka, va);
+  });
+  size_t tmp = 0;
+  int end_bit = gp.key_bits + 1;
+  CK(cub::DeviceRadixSort::SortPairs(nullptr, tmp, ka, kb, va, vb, int(nvis_tot), 0, end_bit, stream));
+  void *dtmp = b_cub.ensure(tmp);
+  CK(cub::DeviceRadixSort::SortPairs(dtmp, tmp, ka, kb, va, vb, int(nvis_tot), 0, end_bit, stream));
+
+  // records
+  void *rec = b_rec.ensure(gp.nvis * sizeof(typename RecOf<R>::type));
+  with_types(a, [&](auto *tw, auto *tv) {
+    using TW = std::remove_pointer_t<decltype(tw)>;
+    using TV = std::remove_pointer_t<decltype(tv)>;
+    launch_records<R, TW, TV>(*this, gp.nvis, a, st, gridding, g, vb, rec);
+  });
+
+  // chunk boundaries
+  int *chunks = reinterpret_cast<int *>(b_chunks.ensure((gp.nvis + 1) * sizeof(int)));
+  int *d_nch = reinterpret_cast<int *>(reinterpret_cast<char *>(b_small.p) + 1024);
+  ChunkStartPred pred{kb, 2 * gp.lbits, chunk_size};
+  thrust::counting_iterator<int> it(0);
+  tmp = 0;
+  CK(cub::DeviceSelect::If(nullptr, tmp, it, chunks, d_nch, int(gp.nvis), pred, stream));
+  dtmp = b_cub.ensure(std::max(tmp, b_cub.n));
+  CK(cub::DeviceSelect::If(dtmp, tmp, it, chunks, d_nch, int(gp.nvis), pred, stream));
+  return true;
+}
+
+namespace {
+
+ScreenArgs make_screen(const GridPlan &g, const double *d_cf, const ChebCorr &cc, size_t P) {
+  ScreenArgs s{};
+  s.nx = int(g.nx);
+  s.ny = int(g.ny);
+  s.nu = int(g.nu);
+  s.nv = int(g.nv);
+  s.px = g.px;
+  s.py = g.py;
+  s.x0 = g.lshift - 0.5 * g.nx * g.px;
+  s.y0 = g.mshift - 0.5 * g.ny * g.py;
+  s.nshift = g.nshift;
+  s.dw = g.dw;
+  s.wmin = g.wmin;
+  s.do_w = g.do_w;
+  s.divide_by_n = g.do_w && g.divide_by_n;
+  s.P = int(P);
+  s.cfu = d_cf;
+  s.cfv = d_cf + g.nx / 2 + 1;
+  s.ncheb = cc.n;
+  s.ymax = cc.ymax;
+  for (int i = 0; i < cc.n && i < kDMaxCheb; ++i) s.cheb[i] = cc.c[i];
+  return s;
+}
+
+}  // namespace
+
+// Grid-correction tables for the chosen kernel, uploaded to b_cf.
+ChebCorr Context::upload_corrections(const GridPlan &g) {
+  KernelTransform tr(g.kernel);
+  std::vector<double> cf(g.nx / 2 + 1 + g.ny / 2 + 1);
+  for (size_t i = 0; i <= g.nx / 2; ++i) cf[i] = tr.corfunc(double(i) / g.nu);
+  for (size_t i = 0; i <= g.ny / 2; ++i) cf[g.nx / 2 + 1 + i] = tr.corfunc(double(i) / g.nv);
+  double *d = reinterpret_cast<double *>(b_cf.ensure(cf.size() * sizeof(double)));
+  CK(cudaMemcpyAsync(d, cf.data(), cf.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+  ChebCorr cc;
+  if (g.do_w) {
+    double vmax = 0.5 / g.ofactor * 1.0000001;
+    // pixels beyond the horizon use (sqrt(r^2-1)-1)*dw (wgridder.h:1376-1377)
+    double xmin = g.lshift - 0.5 * g.nx * g.px, xmax = xmin + (g.nx - 1) * g.px;
+    double ymin = g.mshift - 0.5 * g.ny * g.py, ymax = ymin + (g.ny - 1) * g.py;
+    for (double xc : {xmin, xmax})
+      for (double yc : {ymin, ymax}) {
+        double r2 = xc * xc + yc * yc;
+        if (r2 > 1.0) vmax = std::max(vmax, std::fabs((std::sqrt(r2 - 1.0) - 1.0) * g.dw));
+      }
+    cc = fit_cheb_corr(tr, std::min(vmax, 1.0));
+  } else {
+    cc.n = 1;
+    cc.c = {1.0};
+    cc.ymax = 1.0;
+  }
+  cheb_err = cc.max_rel_err;
+  return cc;
+}
+
+size_t Context::choose_planes(const GridPlan &g, bool gridding) {
+  size_t total = 0, freeb = 0;
+  CK(cudaMemGetInfo(&freeb, &total));
+  size_t held = b_band.n + b_H.n + (gridding ? b_full_fwd.n : b_full_adj.n);
+  double budget = 0.55 * double(total);
+  size_t avail = size_t(std::min<double>(budget, double(freeb + held) - 2e9));
+  size_t per = plan_bytes(g, 1, gridding);
+  size_t P = std::max<size_t>(1, std::min<size_t>(g.nplanes, per ? avail / per : g.nplanes));
+  int lim = env_int("WSG_MAX_PLANES", 0);
+  if (lim > 0) P = std::min<size_t>(P, size_t(lim));
+  return std::min(P, g.nplanes);
+}
+
+template <typename R>
+void Context::grid_core(const wsg_args &a, const Staged &s, double *img, bool accumulate) {
+  const bool dbl = sizeof(R) == 8;
+  GridPlan gp;
+  gp.nx = a.npix_x;
+  gp.ny = a.npix_y;
+  gp.px = a.pixsize_x;
+  gp.py = a.pixsize_y;
+  gp.eps = a.epsilon;
+  gp.do_w = a.do_wgridding != 0;
+  gp.fp32 = !dbl;
+  gp.gridding = true;
+  gp.negate_v = a.negate_v != 0;
+  gp.divide_by_n = a.divide_by_n != 0;
+  gp.lshift = a.center_x;
+  gp.mshift = a.negate_v ? -a.center_y : a.center_y;
+  const size_t npix = a.npix_x * a.npix_y;
+
+  CK(cudaEventRecord(ev[0], stream));
+  if (!accumulate) CK(cudaMemsetAsync(img, 0, npix * sizeof(double), stream));
+  if (!prepare<R>(a, s, true, nullptr, gp)) {
+    record_stats(gp, true, 0);
+    return;
+  }
+  CK(cudaEventRecord(ev[1], stream));
+  ChebCorr cc = upload_corrections(gp);
+  DevGeom g = make_geom(gp);
+  DevKernel<R> kc = make_kernel<R>(gp.poly);
+  const size_t P = choose_planes(gp, true);
+  const size_t cs = 2 * sizeof(R);
+  const size_t nv = gp.nv, nu = gp.nu;
+  char *band = reinterpret_cast<char *>(b_band.ensure(gp.band_rows * P * nv * cs));
+  char *full = reinterpret_cast<char *>(b_full_fwd.ensure(nu * P * nv * cs));
+  char *H = reinterpret_cast<char *>(b_H.ensure(P * gp.ny * nu * cs));
+  H_clean = false;
+  // invariant of the full grid: rows outside the u band are zero
+  Layout lay{nu, nv, P, cs};
+  if (!(lay == fwd_layout)) {
+    CK(cudaMemsetAsync(full, 0, nu * P * nv * cs, stream));
+    fwd_layout = lay;
+    fwd_L = 0;
+  }
+  const size_t L = gp.band_full ? nu / 2 : gp.Lu;
+  if (!gp.band_full && fwd_L > L) {
+    const size_t rowb = P * nv * cs;
+    CK(cudaMemsetAsync(full + (L + 1) * rowb, 0, (fwd_L - L) * rowb, stream));
+    CK(cudaMemsetAsync(full + (nu - fwd_L) * rowb, 0, (fwd_L - L) * rowb, stream));
+  }
+  fwd_L = gp.band_full ? nu / 2 : L;
+
+  const TileLayout tl = make_layout(gp.T, gp.kernel.W);
+  const size_t smem = GridKernels<R>::smem_bytes(tl, gp.kernel.W, true);
+  int *counter = reinterpret_cast<int *>(reinterpret_cast<char *>(b_small.p) + 2048);
+  int *d_nch = reinterpret_cast<int *>(reinterpret_cast<char *>(b_small.p) + 1024);
+  int *d_err = reinterpret_cast<int *>(reinterpret_cast<char *>(b_small.p) + 3072);
+  CK(cudaMemsetAsync(d_err, 0, sizeof(int), stream));
+  GridArgs ga{};
+  ga.err = d_err;
+  ga.rec = b_rec.p;
+  ga.chunk_start = reinterpret_cast<const int *>(b_chunks.p);
+  ga.nchunks = d_nch;
+  ga.counter = counter;
+  ga.nvis = int(gp.nvis);
+  ga.grid = band;
+  ga.P = int(P);
+  ga.tl = tl;
+  ga.sb = GridKernels<R>::SB;
+
+  const int dir = CUFFT_INVERSE;
+  float t_grid = 0, t_fft = 0, t_screen = 0;
+  for (size_t pb0 = 0; pb0 < gp.nplanes; pb0 += P) {
+    const size_t npl = std::min(P, gp.nplanes - pb0);
+    CK(cudaEventRecord(ev[2], stream));
+    CK(cudaMemsetAsync(band, 0, gp.band_rows * P * nv * cs, stream));
+    CK(cudaMemsetAsync(counter, 0, sizeof(int), stream));
+    ga.pb0 = int(pb0);
+    ga.pb1 = int(pb0 + npl);
+    GridKernels<R>::dispatch(gp.kernel.W, true, num_sms, smem, stream, ga, g, kc);
+    CK(cudaEventRecord(ev[3], stream));
+    // pass 1: along v over the band rows (out of place into the full grid)
+    if (gp.band_full) {
+      cufftHandle h = fft_plan(int(nv), 1, int(nv), 1, int(nv), int(nu * P), dbl);
+      fft_exec(h, band, full, dir, dbl);
+    } else {
+      const size_t rowb = P * nv * cs;
+      cufftHandle hlo = fft_plan(int(nv), 1, int(nv), 1, int(nv), int((L + 1) * P), dbl);
+      fft_exec(hlo, band, full, dir, dbl);
+      cufftHandle hhi = fft_plan(int(nv), 1, int(nv), 1, int(nv), int(L * P), dbl);
+      fft_exec(hhi, band + (L + 1) * rowb, full + (nu - L) * rowb, dir, dbl);
+    }
+    // pass 2: along u over the image columns, into H[p][j][u]
+    {
+      const int half = int(gp.ny / 2);
+      cufftHandle h2 = fft_plan(int(nu), int(P * nv), 1, 1, int(nu), half, dbl);
+      for (size_t p = 0; p < npl; ++p) {
+        // grid columns [0, ny/2) are image columns [ny/2, ny)
+        fft_exec(h2, full + (p * nv) * cs, H + (p * gp.ny + half) * nu * cs, dir, dbl);
+        // grid columns [nv-ny/2, nv) are image columns [0, ny/2)
+        fft_exec(h2, full + (p * nv + nv - half) * cs, H + (p * gp.ny) * nu * cs, dir, dbl);
+      }
+    }
+    CK(cudaEventRecord(ev[4], stream));
+    ScreenArgs sa = make_screen(gp, reinterpret_cast<const double *>(b_cf.p), cc, P);
+    sa.pb0 = int(pb0);
+    sa.npl = int(npl);
+    dim3 sg((gp.nx + 31) / 32, (gp.ny + 31) / 32);
+    k_screen_add<R><<<sg, 256, 0, stream>>>(sa, H, img);
+    cuda_check(cudaGetLastError(), "k_screen_add launch");
+    CK(cudaEventRecord(ev[5], stream));
+    CK(cudaEventSynchronize(ev[5]));
+    float t;
+    CK(cudaEventElapsedTime(&t, ev[2], ev[3]));
+    t_grid += t;
+    CK(cudaEventElapsedTime(&t, ev[3], ev[4]));
+    t_fft += t;
+    CK(cudaEventElapsedTime(&t, ev[4], ev[5]));
+    t_screen += t;
+  }
+  check_device_error(d_err);
+  float t_prep;
+  CK(cudaEventElapsedTime(&t_prep, ev[0], ev[1]));
+  record_stats(gp, true, P);
+  stats.ms_prep = t_prep;
+  stats.ms_grid = t_grid;
+  stats.ms_fft = t_fft;
+  stats.ms_screen = t_screen;
+  if (verbosity > 0) print_report(gp, true, P);
+}
+
+template <typename R>
+void Context::degrid_core(const wsg_args &a, const Staged &s, const double *img, void *vis_out) {
+  const bool dbl = sizeof(R) == 8;
+  GridPlan gp;
+  gp.nx = a.npix_x;
+  gp.ny = a.npix_y;
+  gp.px = a.pixsize_x;
+  gp.py = a.pixsize_y;
+  gp.eps = a.epsilon;
+  gp.do_w = a.do_wgridding != 0;
+  gp.fp32 = !dbl;
+  gp.gridding = false;
+  gp.negate_v = a.negate_v != 0;
+  gp.divide_by_n = a.divide_by_n != 0;
+  gp.lshift = a.center_x;
+  gp.mshift = a.negate_v ? -a.center_y : a.center_y;
+
+  CK(cudaEventRecord(ev[0], stream));
+  if (!prepare<R>(a, s, false, vis_out, gp)) {
+    record_stats(gp, false, 0);
+    return;
+  }
+  CK(cudaEventRecord(ev[1], stream));
+  ChebCorr cc = upload_corrections(gp);
+  DevGeom g = make_geom(gp);
+  DevKernel<R> kc = make_kernel<R>(gp.poly);
+  const size_t P = choose_planes(gp, false);
+  const size_t cs = 2 * sizeof(R);
+  const size_t nv = gp.nv, nu = gp.nu;
+  char *band = reinterpret_cast<char *>(b_band.ensure(gp.band_rows * P * nv * cs));
+  char *full = reinterpret_cast<char *>(b_full_adj.ensure(nu * P * nv * cs));
+  char *H = reinterpret_cast<char *>(b_H.ensure(P * gp.ny * nu * cs));
+  // invariant of the adjoint full grid: columns outside the image columns are zero
+  Layout lay{nu, nv, P, cs};
+  if (!(lay == adj_layout)) {
+    CK(cudaMemsetAsync(full, 0, nu * P * nv * cs, stream));
+    adj_layout = lay;
+  }
+  // H entries outside the image rows must be zero
+  if (!H_clean || !(lay == H_layout)) {
+    const size_t nxh = gp.nx / 2;
+    CK(cudaMemset2DAsync(H + nxh * cs, nu * cs, 0, (nu - gp.nx) * cs, P * gp.ny, stream));
+    H_clean = true;
+    H_layout = lay;
+  }
+  const TileLayout tl = make_layout(gp.T, gp.kernel.W);
+  const size_t smem = GridKernels<R>::smem_bytes(tl, gp.kernel.W, false);
+  int *counter = reinterpret_cast<int *>(reinterpret_cast<char *>(b_small.p) + 2048);
+  int *d_nch = reinterpret_cast<int *>(reinterpret_cast<char *>(b_small.p) + 1024);
+  int *d_err = reinterpret_cast<int *>(reinterpret_cast<char *>(b_small.p) + 3072);
+  CK(cudaMemsetAsync(d_err, 0, sizeof(int), stream));
+  GridArgs ga{};
+  ga.err = d_err;
+  ga.rec = b_rec.p;
+  ga.chunk_start = reinterpret_cast<const int *>(b_chunks.p);
+  ga.nchunks = d_nch;
+  ga.counter = counter;
+  ga.nvis = int(gp.nvis);
+  ga.grid = band;
+  ga.P = int(P);
+  ga.tl = tl;
+  ga.sb = GridKernels<R>::SB;
+  ga.vis_out = vis_out;
+  ga.vis_double = a.vis_type == WSG_C128;
+  const bool multi = P < gp.nplanes;
+  ga.acc = multi ? b_acc.ensure(gp.nvis * cs) : nullptr;
+
+  const int dir = CUFFT_FORWARD;
+  const size_t L = gp.band_full ? nu / 2 : gp.Lu;
+  float t_grid = 0, t_fft = 0, t_screen = 0;
+  for (size_t pb0 = 0; pb0 < gp.nplanes; pb0 += P) {
+    const size_t npl = std::min(P, gp.nplanes - pb0);
+    CK(cudaEventRecord(ev[2], stream));
+    ScreenArgs sa = make_screen(gp, reinterpret_cast<const double *>(b_cf.p), cc, P);
+    sa.pb0 = int(pb0);
+    sa.npl = int(npl);
+    dim3 sg((gp.nx + 31) / 32, (gp.ny + 31) / 32);
+    k_screen_put<R><<<sg, 256, 0, stream>>>(sa, img, H);
+    cuda_check(cudaGetLastError(), "k_screen_put launch");
+    CK(cudaEventRecord(ev[3], stream));
+    // pass 2 (transposed): along u, H[p][j][u] -> image columns of the full grid
+    {
+      const int half = int(gp.ny / 2);
+      cufftHandle h2 = fft_plan(int(nu), 1, int(nu), int(P * nv), 1, half, dbl);
+      for (size_t p = 0; p < npl; ++p) {
+        fft_exec(h2, H + (p * gp.ny + half) * nu * cs, full + (p * nv) * cs, dir, dbl);
+        fft_exec(h2, H + (p * gp.ny) * nu * cs, full + (p * nv + nv - half) * cs, dir, dbl);
+      }
+    }
+    // pass 1 (transposed): along v over the band rows, into the band grid
+    if (gp.band_full) {
+      cufftHandle h = fft_plan(int(nv), 1, int(nv), 1, int(nv), int(nu * P), dbl);
+      fft_exec(h, full, band, dir, dbl);
+    } else {
+      const size_t rowb = P * nv * cs;
+      cufftHandle hlo = fft_plan(int(nv), 1, int(nv), 1, int(nv), int((L + 1) * P), dbl);
+      fft_exec(hlo, full, band, dir, dbl);
+      cufftHandle hhi = fft_plan(int(nv), 1, int(nv), 1, int(nv), int(L * P), dbl);
+      fft_exec(hhi, full + (nu - L) * rowb, band + (L + 1) * rowb, dir, dbl);
+    }
+    CK(cudaEventRecord(ev[4], stream));
+    CK(cudaMemsetAsync(counter, 0, sizeof(int), stream));
+    ga.pb0 = int(pb0);
+    ga.pb1 = int(pb0 + npl);
+    ga.first_pass = pb0 == 0;
+    ga.last_pass = pb0 + npl >= gp.nplanes;
+    GridKernels<R>::dispatch(gp.kernel.W, false, num_sms, smem, stream, ga, g, kc);
+    CK(cudaEventRecord(ev[5], stream));
+    CK(cudaEventSynchronize(ev[5]));
+    float t;
+    CK(cudaEventElapsedTime(&t, ev[2], ev[3]));
+    t_screen += t;
+    CK(cudaEventElapsedTime(&t, ev[3], ev[4]));
+    t_fft += t;
+    CK(cudaEventElapsedTime(&t, ev[4], ev[5]));
+    t_grid += t;
+  }
+  check_device_error(d_err);
+  float t_prep;
+  CK(cudaEventElapsedTime(&t_prep, ev[0], ev[1]));
+  record_stats(gp, false, P);
+  stats.ms_prep = t_prep;
+  stats.ms_grid = t_grid;
+  stats.ms_fft = t_fft;
+  stats.ms_screen = t_screen;
+  if (verbosity > 0) print_report(gp, false, P);
+}
+
+void Context::check_device_error(const int *d_err) {
+  int h = 0;
+  CK(cudaMemcpyAsync(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost, stream));
+  CK(cudaStreamSynchronize(stream));
+  if (h) throw std::runtime_error("internal error: a visibility record fell outside its tile");
+}
+
+void Context::record_stats(const GridPlan &g, bool gridding, size_t P) {
+  std::memset(&stats, 0, sizeof(stats));
+  stats.nvis = g.nvis;
+  stats.nu = g.nu;
+  stats.nv = g.nv;
+  stats.nplanes = g.nplanes;
+  stats.supp = g.kernel.W;
+  stats.plane_batch = P;
+  stats.band_rows = g.band_rows;
+  stats.degree = g.poly.D;
+  stats.sigma = g.ofactor;
+  stats.beta = g.kernel.beta;
+  stats.e0 = g.kernel.e0;
+  stats.kernel_err = g.kernel.err;
+  stats.wmin = g.wmin_d;
+  stats.wmax = g.wmax_d;
+  stats.dw = g.dw;
+  stats.nshift = g.nshift;
+  stats.gridding = gridding;
+  stats.precision = g.fp32 ? WSG_PREC_MIXED : WSG_PREC_FP64;
+  stats.device_bytes = device_bytes();
+}
+
+void Context::print_report(const GridPlan &g, bool gridding, size_t P) {
+  std::printf("%s:\n  dirty=(%zux%zu), grid=(%zux%zu", gridding ? "Gridding" : "Degridding", g.nx,
+              g.ny, g.nu, g.nv);
+  if (g.do_w) std::printf("x%zu", g.nplanes);
+  std::printf("), supp=%d, eps=%g (kernel %.3g, sigma %.2f)\n", g.kernel.W, g.eps, g.kernel.err,
+              g.kernel.sigma);
+  std::printf("  nvis=%zu, w=[%g; %g], dw=%g, planes per pass=%zu, u band rows=%zu\n", g.nvis,
+              g.wmin_d, g.wmax_d, g.dw, P, g.band_rows);
+  std::fflush(stdout);
+}
+
+// ------------------------------------------------------- public drivers
+
+void Context::ms2dirty(const wsg_args &a, const void *vis, void *dirty, int accumulate) {
+  validate(a);
+  require(vis && dirty, "vis and dirty are required");
+  CK(cudaSetDevice(device));
+  const size_t nvis = a.nrows * a.nchan;
+  const size_t vbytes = nvis * (a.vis_type == WSG_C128 ? 16 : 8);
+  Staged s;
+  s.uvw = reinterpret_cast<const double *>(stage_in(a.uvw, a.nrows * 3 * sizeof(double), b_uvw));
+  s.vis = stage_in(vis, vbytes, b_vis);
+  s.wgt = stage_in(a.wgt, nvis * (a.wgt_type == WSG_F64 ? 8 : 4), b_wgt);
+  s.mask = reinterpret_cast<const uint8_t *>(stage_in(a.mask, nvis, b_mask));
+  const size_t npix = a.npix_x * a.npix_y;
+  const size_t dsz = a.dirty_type == WSG_F64 ? 8 : 4;
+  double *img = reinterpret_cast<double *>(b_img.ensure(npix * sizeof(double)));
+  const bool ddev = is_device_pointer(dirty);
+  if (accumulate) {
+    const void *din = ddev ? dirty : stage_in(dirty, npix * dsz, b_out);
+    int nb = launch_blocks(npix, 256);
+    if (a.dirty_type == WSG_F64)
+      k_load_image<double><<<nb, 256, 0, stream>>>(npix, (const double *)din, img, 0);
+    else
+      k_load_image<float><<<nb, 256, 0, stream>>>(npix, (const float *)din, img, 0);
+  }
+  if (a.precision == WSG_PREC_FP64)
+    grid_core<double>(a, s, img, accumulate != 0);
+  else
+    grid_core<float>(a, s, img, accumulate != 0);
+  // convert/copy out
+  void *dout = ddev ? dirty : b_out.ensure(npix * dsz);
+  int nb = launch_blocks(npix, 256);
+  if (a.dirty_type == WSG_F64)
+    k_store_image<double><<<nb, 256, 0, stream>>>(npix, img, (double *)dout);
+  else
+    k_store_image<float><<<nb, 256, 0, stream>>>(npix, img, (float *)dout);
+  cuda_check(cudaGetLastError(), "k_store_image launch");
+  if (!ddev) CK(cudaMemcpyAsync(dirty, dout, npix * dsz, cudaMemcpyDeviceToHost, stream));
+  CK(cudaEventRecord(ev[6], stream));
+  CK(cudaStreamSynchronize(stream));
+  float t;
+  CK(cudaEventElapsedTime(&t, ev[0], ev[6]));
+  stats.ms_total = t;
+  stats.nrows = a.nrows;
+  stats.nchan = a.nchan;
+}
+
+void Context::dirty2ms(const wsg_args &a, const void *dirty, void *vis) {
+  validate(a);
+  require(vis && dirty, "vis and dirty are required");
+  CK(cudaSetDevice(device));
+  const size_t nvis = a.nrows * a.nchan;
+  const size_t vbytes = nvis * (a.vis_type == WSG_C128 ? 16 : 8);
+  Staged s;
+  s.uvw = reinterpret_cast<const double *>(stage_in(a.uvw, a.nrows * 3 * sizeof(double), b_uvw));
+  s.wgt = stage_in(a.wgt, nvis * (a.wgt_type == WSG_F64 ? 8 : 4), b_wgt);
+  s.mask = reinterpret_cast<const uint8_t *>(stage_in(a.mask, nvis, b_mask));
+  const size_t npix = a.npix_x * a.npix_y;
+  const size_t dsz = a.dirty_type == WSG_F64 ? 8 : 4;
+  const void *din = stage_in(dirty, npix * dsz, b_out);
+  double *img = reinterpret_cast<double *>(b_img.ensure(npix * sizeof(double)));
+  int nb = launch_blocks(npix, 256);
+  if (a.dirty_type == WSG_F64)
+    k_load_image<double><<<nb, 256, 0, stream>>>(npix, (const double *)din, img, 0);
+  else
+    k_load_image<float><<<nb, 256, 0, stream>>>(npix, (const float *)din, img, 0);
+  cuda_check(cudaGetLastError(), "k_load_image launch");
+  degrid_from_image(a, s, img, vis, vbytes);
+}
+
+void Context::degrid_from_image(const wsg_args &a, const Staged &s, const double *img, void *vis,
+                                size_t vbytes) {
+  const bool vdev = is_device_pointer(vis);
+  void *vout = vdev ? vis : b_vis.ensure(vbytes);
+  // inactive visibilities are zeroed by the scan; with no active ones at all
+  // the whole output is zero
+  CK(cudaMemsetAsync(vout, 0, vbytes, stream));
+  if (a.precision == WSG_PREC_FP64)
+    degrid_core<double>(a, s, img, vout);
+  else
+    degrid_core<float>(a, s, img, vout);
+  if (!vdev) CK(cudaMemcpyAsync(vis, vout, vbytes, cudaMemcpyDeviceToHost, stream));
+  CK(cudaEventRecord(ev[6], stream));
+  CK(cudaStreamSynchronize(stream));
+  float t;
+  CK(cudaEventElapsedTime(&t, ev[0], ev[6]));
+  stats.ms_total = t;
+  stats.nrows = a.nrows;
+  stats.nchan = a.nchan;
+}
+
+// ----------------------------------------------------- stateful gridder
+
+Gridder::Gridder(const wsg_gridder_params &p) : prm(p), ctx(p.device) {
+  require(p.verbosity <= 2, "verbosity must be 0, 1, or 2");
+  require(p.width_t <= p.width && p.height_t <= p.height, "trimmed size exceeds image size");
+  require(p.width_t % 2 == 0 && p.height_t % 2 == 0, "trimmed image size must be even");
+  ctx.verbosity = int(p.verbosity);
+}
+
+wsg_args Gridder::args(size_t nrows, size_t nchan, const double *uvw, const double *freq) const {
+  wsg_args a;
+  wsg_args_init(&a);
+  a.nrows = nrows;
+  a.nchan = nchan;
+  a.uvw = uvw;
+  a.freq = freq;
+  a.npix_x = prm.width_t;
+  a.npix_y = prm.height_t;
+  a.pixsize_x = prm.pixel_size_x;
+  a.pixsize_y = prm.pixel_size_y;
+  a.epsilon = prm.epsilon;
+  a.do_wgridding = 1;
+  // WSClean's call pattern (wgriddinggridder_simple.cpp:56-58)
+  a.negate_v = 1;
+  a.divide_by_n = 0;
+  a.sigma_min = 1.1;
+  a.sigma_max = 2.0;
+  a.center_x = -prm.l_shift;
+  a.center_y = -prm.m_shift;
+  a.precision = prm.precision;
+  a.vis_type = WSG_C64;
+  a.dirty_type = WSG_F64;
+  return a;
+}
+
+void Gridder::memory_usage(size_t &constant, size_t &per_vis) const {
+  // host-side figures for WSClean's row chunking: the trimmed image plus the
+  // staging of one chunk; per visibility the device sort keys, indices and
+  // record (the host holds nothing extra per visibility)
+  constant = prm.width_t * prm.height_t * sizeof(double);
+  per_vis = 8;
+}
+
+void Gridder::initialize_inversion() {
+  CK(cudaSetDevice(ctx.device));
+  void *p = ctx.b_img2.ensure(prm.width_t * prm.height_t * sizeof(double));
+  CK(cudaMemsetAsync(p, 0, prm.width_t * prm.height_t * sizeof(double), ctx.stream));
+  CK(cudaStreamSynchronize(ctx.stream));
+  have_img = true;
+}
+
+void Gridder::add_inversion_data(size_t nrows, size_t nchan, const double *uvw, const double *freq,
+                                 const void *vis) {
+  require(have_img, "InitializeInversion must be called first");
+  wsg_args a = args(nrows, nchan, uvw, freq);
+  ctx.validate(a);
+  CK(cudaSetDevice(ctx.device));
+  const size_t nvis = nrows * nchan;
+  Staged s;
+  s.uvw = reinterpret_cast<const double *>(ctx.stage_in(uvw, nrows * 3 * sizeof(double), ctx.b_uvw));
+  s.vis = ctx.stage_in(vis, nvis * 8, ctx.b_vis);
+  double *img = reinterpret_cast<double *>(ctx.b_img2.p);
+  if (a.precision == WSG_PREC_FP64)
+    ctx.grid_core<double>(a, s, img, true);
+  else
+    ctx.grid_core<float>(a, s, img, true);
+  CK(cudaStreamSynchronize(ctx.stream));
+}
+
+void Gridder::finalize_image(double f) {
+  require(have_img, "no image to finalize");
+  size_t n = prm.width_t * prm.height_t;
+  k_scale<<<launch_blocks(n, 256), 256, 0, ctx.stream>>>(n, reinterpret_cast<double *>(ctx.b_img2.p), f);
+  cuda_check(cudaGetLastError(), "k_scale launch");
+  CK(cudaStreamSynchronize(ctx.stream));
+}
+
+void Gridder::real_image(float *out) {
+  require(have_img, "no image available");
+  size_t n = prm.width * prm.height;
+  const bool odev = is_device_pointer(out);
+  float *d = odev ? out : reinterpret_cast<float *>(ctx.b_out.ensure(n * sizeof(float)));
+  int dx = int((prm.width - prm.width_t) / 2), dy = int((prm.height - prm.height_t) / 2);
+  k_retrim<<<launch_blocks(n, 256), 256, 0, ctx.stream>>>(
+      int(prm.width_t), int(prm.height_t), int(prm.width), int(prm.height), dx, dy,
+      reinterpret_cast<const double *>(ctx.b_img2.p), d);
+  cuda_check(cudaGetLastError(), "k_retrim launch");
+  if (!odev) CK(cudaMemcpyAsync(out, d, n * sizeof(float), cudaMemcpyDeviceToHost, ctx.stream));
+  CK(cudaStreamSynchronize(ctx.stream));
+}
+
+void Gridder::initialize_prediction(const float *image) {
+  require(image != nullptr, "image is required");
+  CK(cudaSetDevice(ctx.device));
+  size_t n = prm.width * prm.height;
+  const float *d = reinterpret_cast<const float *>(ctx.stage_in(image, n * sizeof(float), ctx.b_out));
+  double *img = reinterpret_cast<double *>(ctx.b_img2.ensure(prm.width_t * prm.height_t * sizeof(double)));
+  int dx = int((prm.width - prm.width_t) / 2), dy = int((prm.height - prm.height_t) / 2);
+  k_untrim<<<launch_blocks(prm.width_t * prm.height_t, 256), 256, 0, ctx.stream>>>(
+      int(prm.width_t), int(prm.height_t), int(prm.width), dx, dy, d, img);
+  cuda_check(cudaGetLastError(), "k_untrim launch");
+  CK(cudaStreamSynchronize(ctx.stream));
+  have_img = true;
+}
+
+void Gridder::predict_visibilities(size_t nrows, size_t nchan, const double *uvw, const double *freq,
+                                   void *vis) {
+  require(have_img, "InitializePrediction must be called first");
+  wsg_args a = args(nrows, nchan, uvw, freq);
+  ctx.validate(a);
+  CK(cudaSetDevice(ctx.device));
+  Staged s;
+  s.uvw = reinterpret_cast<const double *>(ctx.stage_in(uvw, nrows * 3 * sizeof(double), ctx.b_uvw));
+  ctx.degrid_from_image(a, s, reinterpret_cast<const double *>(ctx.b_img2.p), vis, nrows * nchan * 8);
+}
+
+template bool Context::prepare<float>(const wsg_args &, const Staged &, bool, void *, GridPlan &);
+template bool Context::prepare<double>(const wsg_args &, const Staged &, bool, void *, GridPlan &);
+template void Context::grid_core<float>(const wsg_args &, const Staged &, double *, bool);
+template void Context::grid_core<double>(const wsg_args &, const Staged &, double *, bool);
+template void Context::degrid_core<float>(const wsg_args &, const Staged &, const double *, void *);
+template void Context::degrid_core<double>(const wsg_args &, const Staged &, const double *, void *);
+
+}  // namespace wsg

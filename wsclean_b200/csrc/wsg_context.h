@@ -1,0 +1,120 @@
+// Execution context and stateful gridder of libwsg (host side, internal).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <map>
+#include <tuple>
+#include <vector>
+
+#include "../../include/wsg.h"
+#include "wsg_internal.h"
+
+namespace wsg {
+
+void cuda_check(cudaError_t e, const char *what);
+bool is_device_pointer(const void *p);
+
+// Grow-only device buffer.
+struct DevBuf {
+  void *p = nullptr;
+  size_t n = 0;
+  void *ensure(size_t bytes);
+  void release();
+};
+
+struct Layout {
+  size_t nu = 0, nv = 0, P = 0, cs = 0;
+  bool operator==(const Layout &o) const {
+    return nu == o.nu && nv == o.nv && P == o.P && cs == o.cs;
+  }
+};
+
+// Device pointers of one call's inputs.
+struct Staged {
+  const double *uvw = nullptr;
+  const double *fovc = nullptr;
+  const void *vis = nullptr;
+  const void *wgt = nullptr;
+  const uint8_t *mask = nullptr;
+};
+
+class Context {
+ public:
+  explicit Context(int device);
+  ~Context();
+  Context(const Context &) = delete;
+  Context &operator=(const Context &) = delete;
+
+  void ms2dirty(const wsg_args &a, const void *vis, void *dirty, int accumulate);
+  void dirty2ms(const wsg_args &a, const void *dirty, void *vis);
+  void release_buffers();
+  size_t device_bytes();
+  void validate(const wsg_args &a);
+
+  const void *stage_in(const void *p, size_t bytes, DevBuf &buf);
+  template <typename R>
+  void grid_core(const wsg_args &a, const Staged &s, double *img, bool accumulate);
+  template <typename R>
+  void degrid_core(const wsg_args &a, const Staged &s, const double *img, void *vis_out);
+  void degrid_from_image(const wsg_args &a, const Staged &s, const double *img, void *vis,
+                         size_t vbytes);
+
+  int device = 0;
+  cudaStream_t stream = nullptr, own_stream = nullptr;
+  int num_sms = 148;
+  int verbosity = 0;
+  int chunk_size = 1024;
+  wsg_stats stats;
+  double cheb_err = 0;
+
+  // buffers
+  DevBuf b_uvw, b_fovc, b_vis, b_wgt, b_mask;
+  DevBuf b_keys_a, b_keys_b, b_vals_a, b_vals_b, b_cub, b_rec, b_chunks, b_small;
+  DevBuf b_band, b_full_fwd, b_full_adj, b_H;
+  DevBuf b_img, b_img2, b_acc, b_cf, b_fftwork, b_out;
+
+ private:
+  std::vector<DevBuf *> all_buffers();
+  template <typename R>
+  bool prepare(const wsg_args &a, const Staged &s, bool gridding, void *vis_out_dev, GridPlan &gp);
+  ChebCorr upload_corrections(const GridPlan &g);
+  size_t choose_planes(const GridPlan &g, bool gridding);
+  cufftHandle fft_plan(int n, int istride, int idist, int ostride, int odist, int batch, bool dbl);
+  void fft_exec(cufftHandle h, void *in, void *out, int dir, bool dbl);
+  void record_stats(const GridPlan &g, bool gridding, size_t P);
+  void check_device_error(const int *d_err);
+  void print_report(const GridPlan &g, bool gridding, size_t P);
+
+  cudaEvent_t ev[8];
+  std::map<std::tuple<int, int, int, int, int, int, int>, cufftHandle> fft_plans;
+  size_t fft_work_need = 0;
+  Layout fwd_layout, adj_layout, H_layout;
+  size_t fwd_L = 0;
+  bool H_clean = false;
+};
+
+// WGriddingGridder_Simple replacement (wgridder/wgriddinggridder_simple.h:34-144).
+class Gridder {
+ public:
+  explicit Gridder(const wsg_gridder_params &p);
+  void memory_usage(size_t &constant, size_t &per_vis) const;
+  void initialize_inversion();
+  void add_inversion_data(size_t nrows, size_t nchan, const double *uvw, const double *freq,
+                          const void *vis);
+  void finalize_image(double f);
+  void real_image(float *out);
+  void initialize_prediction(const float *image);
+  void predict_visibilities(size_t nrows, size_t nchan, const double *uvw, const double *freq,
+                            void *vis);
+  Context &context() { return ctx; }
+
+ private:
+  wsg_args args(size_t nrows, size_t nchan, const double *uvw, const double *freq) const;
+  wsg_gridder_params prm;
+  Context ctx;
+  bool have_img = false;
+};
+
+}  // namespace wsg

@@ -1,0 +1,133 @@
+// Internal host-side declarations of libwsg (not part of the C ABI).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace wsg {
+
+constexpr double kSpeedOfLight = 299792458.0;  // wgridder.h:297
+constexpr int kMaxW = 16;
+constexpr int kMaxDeg = 24;
+constexpr int kMaxCheb = 48;
+
+// Thrown for invalid arguments (the reference's MR_assert); mapped to
+// WSG_ERR_INVALID at the C ABI.
+struct InvalidArgument : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+struct OutOfMemory : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+struct CufftError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+inline void require(bool ok, const std::string &msg) {
+  if (!ok) throw InvalidArgument(msg);
+}
+
+// One row of the generated ES kernel table.
+struct KernelSpec {
+  int W;
+  double sigma;   // tabulated oversampling factor
+  double err;     // error estimate for the requested dimensionality
+  double beta;    // phi(t) = exp(beta*W*((1-t^2)^e0 - 1))
+  double e0;
+};
+
+// ES kernel value phi(t), |t|<=1.
+double es_phi(double t, int W, double beta, double e0);
+
+// Candidate kernels: for every support W allowed by the precision, the
+// smallest tabulated sigma in [sigma_min, sigma_max] whose error estimate
+// (ndim * err1d, floored for FP32 arithmetic) is <= epsilon.  Throws
+// InvalidArgument if none qualifies.
+std::vector<KernelSpec> available_kernels(double epsilon, int ndim, bool fp32,
+                                          double sigma_min, double sigma_max);
+
+// W pieces of degree D in the local coordinate x in [-1,1]; piece k covers
+// t in [-1+2k/W, -1+2(k+1)/W].  coef[j*W + k] multiplies x^j.
+struct PolyKernel {
+  int W = 0, D = 0;
+  std::vector<double> coef;
+  double max_err = 0;  // max |poly - phi| on a dense test grid
+};
+PolyKernel fit_poly_kernel(const KernelSpec &k, double target_err);
+
+// Fourier transform of the kernel in grid-cell units,
+// Phi(nu) = (W/2) int_{-1}^{1} phi(t) cos(pi W nu t) dt,
+// by composite Gauss-Legendre quadrature (exact to FP64 rounding for
+// |nu| <= 2).  The grid correction is 1/Phi.
+class KernelTransform {
+ public:
+  explicit KernelTransform(const KernelSpec &k);
+  double operator()(double nu) const;
+  double corfunc(double nu) const { return 1.0 / (*this)(nu); }
+
+ private:
+  int W_;
+  std::vector<double> t_, wphi_;
+};
+
+// Chebyshev interpolant of corfunc(v) as a function of y = v^2 on
+// [0, ymax]; evaluated on the device by Clenshaw recurrence.
+struct ChebCorr {
+  double ymax = 0;
+  int n = 0;  // number of coefficients
+  std::vector<double> c;
+  double max_rel_err = 0;
+};
+ChebCorr fit_cheb_corr(const KernelTransform &tr, double vmax);
+
+// Smallest n' >= n whose prime factors are 2,3,5,7 (fast cuFFT sizes).
+size_t good_size_cufft(size_t n);
+
+// Everything one ms2dirty/dirty2ms call needs to know, in FP64.
+struct GridPlan {
+  // inputs
+  size_t nx = 0, ny = 0;
+  double px = 0, py = 0;
+  double eps = 0;
+  bool do_w = true, fp32 = true, gridding = true;
+  bool negate_v = false, divide_by_n = true;
+  double lshift = 0, mshift = 0;
+  // scan results
+  size_t nvis = 0;
+  double wmin_d = 0, wmax_d = 0, umax = 0, vmax = 0;
+  // chosen kernel and grid
+  KernelSpec kernel{};
+  PolyKernel poly;
+  size_t nu = 0, nv = 0;
+  double ofactor = 0;
+  double nm1min = 0, nm1max = 0, nshift = 0;
+  bool lmshift = false, shifting = false;
+  double wmin = 0, dw = 0, xdw = 0, wshift = 0;
+  size_t nplanes = 1;
+  int nsafe = 0, maxiu0 = 0, maxiv0 = 0;
+  double ushift = 0, vshift = 0;
+  // occupied u band: rows [0, Lu] and [nu-Lu, nu), or all rows
+  size_t Lu = 0, band_rows = 0;
+  bool band_full = false;
+  // bins and sort keys
+  int T = 16;
+  int ntu = 0, ntv = 0, nwmin = 1;
+  int lbits = 0;      // sort bits per axis for the position inside a tile
+  int key_bits = 0;   // total key bits (<= 31)
+};
+
+// Parameter choice (the analogue of ducc0 Params::getNuNv, wgridder.h:1503-1576,
+// and the w-plane placement of countRanges, wgridder.h:690-699).  The cost
+// model is this implementation's own, calibrated for the B200 kernels.
+void choose_grid(GridPlan &g, double sigma_min, double sigma_max, int tile);
+
+// Nominal device bytes for one pass with `planes` planes resident.
+size_t plan_bytes(const GridPlan &g, size_t planes, bool gridding);
+
+}  // namespace wsg
