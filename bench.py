@@ -1,0 +1,455 @@
+#!/usr/bin/env python
+"""Headline benchmark: Mvis/s of the w-gridding adjoint pair (ms2dirty +
+dirty2ms) at 4096^2 on ~8.1M visibilities, mixed precision (FP32 bulk, FP64
+coordinates / w-phase / image accumulation / correction) at epsilon 1e-5,
+with the plain FP64 GPU form (epsilon 1e-12) and the relative RMS error
+against an FP64 direct Fourier transform reported beside it.
+
+A step = one ms2dirty of the visibilities + one dirty2ms of the model image
+over the whole workload.  ``value`` times steps with inputs resident in HBM
+(CUDA events on the gridder's stream); ``e2e`` times the same steps through
+the public API from pinned host buffers (H2D of uvw + data, D2H of the
+result inside the timed region).
+
+Workload (synthetic, seeded): 128 antennas uniform within 6 km, 8 s cadence
+over 997 timesteps (8128 baselines -> 8,103,616 visibilities), one channel at
+150 MHz, dec -30 deg, |w| scaled to 30% of max|uv|, 200 power-law point
+sources; 4096^2 image at 5" pixels.
+
+--impl reference times the reference's own CPU w-gridder (ducc0 as vendored
+by WSClean, compiled from the reference sources into oracle/_ref) on the same
+workload with all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "Mvis/s ms2dirty+dirty2ms @4096²: FP32-mixed vs FP64 GPU, rel err vs FP64 DFT"
+UNIT = "Mvis/s"
+EPS_MIXED, EPS_FP64 = 1e-5, 1e-12
+# Grid chosen by the reference (ducc0) for this workload, from its verbosity-1
+# report (oracle/_ref run on the same seeded data): mixed eps 1e-5 -> 7392^2 x
+# 14 planes; FP64 eps 1e-12 -> 7392^2 x 22 planes.  Used only for the
+# algorithmic-bytes roofline so that it does not depend on this library's
+# own (smaller) grid choice.
+DUCC_GRID = {"mixed": (7392, 7392, 14), "fp64": (7392, 7392, 22)}
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    return ap.parse_args()
+
+
+def algorithmic_bytes(nvis, nrows, nx, ny, grid, s_vis, s_grid):
+    """Bytes per call of one direction (ms2dirty or dirty2ms)."""
+    nu, nv, npl = grid
+    return (nvis * s_vis + nrows * 24 + npl * 3 * s_grid * nu * nv
+            + npl * 16 * nx * ny + 2 * 8 * nx * ny)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax.append(float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def workload():
+    from wsclean_b200 import synth
+    c = synth.config2()
+    rng = np.random.default_rng(12)
+    nx = c["npix_x"]
+    ix, iy, flux = synth.point_sky(c["nsrc"], nx, nx, rng)
+    return c, ix, iy, flux
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl" if args.impl == "ours" else "gloo",
+                                timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return world, rank, local, pg
+
+
+def run_reference(args, world, rank):
+    """The reference's CPU w-gridder (compiled ducc0) on the same workload."""
+    if rank != 0:
+        return
+    import oracle as O
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "compiled reference (oracle/_ref) missing"}))
+        return
+    c, ix, iy, flux = workload()
+    from wsclean_b200 import synth
+    uvw, freq, nx, px = c["uvw"], c["freq"], c["npix_x"], c["pixsize"]
+    nvis = uvw.shape[0] * len(freq)
+    # the gridder's run time does not depend on the values: seeded noise
+    # stands in for the sky visibilities so no GPU is touched here
+    g = np.random.default_rng(3)
+    vis = (g.normal(size=(uvw.shape[0], len(freq)))
+           + 1j * g.normal(size=(uvw.shape[0], len(freq)))).astype(np.complex64)
+    model = synth.sky_image(nx, nx, ix, iy, flux).astype(np.float32)
+    cores = os.cpu_count()
+    kw = dict(prec="float", negate_v=True, divide_by_n=False, sigma_min=1.1, sigma_max=2.0,
+              nthreads=cores)
+
+    def step():
+        t0 = time.perf_counter()
+        O.ref_ms2dirty(uvw, freq, vis, nx, nx, px, px, EPS_MIXED, **kw)
+        O.ref_dirty2ms(uvw, freq, model, px, px, EPS_MIXED, **kw)
+        return time.perf_counter() - t0
+
+    for _ in range(min(args.warmup, 1)):
+        step()
+    ts = [step() for _ in range(args.steps)]
+    tot = sum(ts)
+    value = nvis * len(ts) / tot / 1e6
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": len(ts), "warmup": min(args.warmup, 1), "ms_per_step": 1e3 * tot / len(ts),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded Earth-rotation observation, 200 point sources)",
+        "config": {"workload": "config-2 adjoint pair: 8.1M vis, 4096^2 @ 5\", eps 1e-5",
+                   "nvis": nvis, "npix": nx, "instance": "ducc0 <float,float>",
+                   "wsclean_args": "negate_v, no divide_by_n, sigma 1.1..2.0"},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": "full workload per step (one ms2dirty + one dirty2ms)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+
+
+def dft_pixels(uvw, freq, vis, nx, ny, px, py, pix, torch, dev):
+    """FP64 direct sum of the ms2dirty image at flat pixel indices (GPU, torch)."""
+    from wsclean_b200 import synth
+    i, j = pix // ny, pix % ny
+    l, m = synth.pixel_lm(i.astype(float), j.astype(float), nx, ny, px, py)
+    nm1 = -(l * l + m * m) / (np.sqrt(1 - l * l - m * m) + 1)
+    Lm = torch.as_tensor(np.stack([l, -m, -nm1]), dtype=torch.float64, device=dev)
+    out = torch.zeros(len(pix), dtype=torch.float64, device=dev)
+    U = torch.as_tensor(uvw, dtype=torch.float64, device=dev)
+    V = torch.as_tensor(vis, dtype=torch.complex128, device=dev)
+    for c, f in enumerate(freq):
+        for r0 in range(0, U.shape[0], 1 << 20):
+            ph = (U[r0:r0 + (1 << 20)] * (f / synth.C_LIGHT)) @ Lm
+            ph = ph - torch.round(ph)
+            out += (V[r0:r0 + (1 << 20), c:c + 1] * torch.exp(2j * math.pi * ph)).real.sum(0)
+    return out.cpu().numpy()
+
+
+def rel_rms(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.sqrt(np.sum(np.abs(a - b) ** 2) / np.sum(np.abs(b) ** 2)))
+
+
+def run_ours(args, world, rank, local, pg):
+    import torch
+    from wsclean_b200 import synth
+    from wsclean_b200.gridder import Context
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    c, ix, iy, flux = workload()
+    uvw, freq, nx, px = c["uvw"], c["freq"], c["npix_x"], c["pixsize"]
+    nrows, nchan = uvw.shape[0], len(freq)
+    nvis = nrows * nchan
+    vis64 = synth.predict_vis(uvw, freq, nx, nx, px, px, ix, iy, flux, device=dev)
+    noise = np.random.default_rng(3).normal(size=vis64.shape) * 0.1
+    vis64 = vis64 + noise + 1j * np.random.default_rng(4).normal(size=vis64.shape) * 0.1
+    model = synth.sky_image(nx, nx, ix, iy, flux)
+
+    ctx = Context(local)
+    kw = dict(negate_v=True, divide_by_n=False, sigma_min=1.1, sigma_max=2.0)
+    d_uvw = torch.as_tensor(uvw, device=dev)
+    d_freq = torch.as_tensor(freq, device=dev)
+    forms = {
+        "mixed": dict(eps=EPS_MIXED, vis=torch.as_tensor(vis64.astype(np.complex64), device=dev),
+                      model=torch.as_tensor(model.astype(np.float32), device=dev),
+                      dirty=torch.zeros((nx, nx), dtype=torch.float32, device=dev),
+                      out=torch.zeros((nrows, nchan), dtype=torch.complex64, device=dev)),
+        "fp64": dict(eps=EPS_FP64, vis=torch.as_tensor(vis64, device=dev),
+                     model=torch.as_tensor(model, device=dev),
+                     dirty=torch.zeros((nx, nx), dtype=torch.float64, device=dev),
+                     out=torch.zeros((nrows, nchan), dtype=torch.complex128, device=dev)),
+    }
+    stream = torch.cuda.current_stream(dev)
+
+    def call_pair(form, f):
+        ctx.ms2dirty(d_uvw, d_freq, f["vis"], nx, nx, px, px, f["eps"], precision=form,
+                     dirty=f["dirty"], **kw)
+        st1 = ctx.stats()
+        ctx.dirty2ms(d_uvw, d_freq, f["model"], px, px, f["eps"], precision=form, vis=f["out"], **kw)
+        st2 = ctx.stats()
+        return st1, st2
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        if pg is not None:
+            pg.barrier()
+        torch.cuda.synchronize(dev)
+
+    def timed(form, steps, warmup):
+        f = forms[form]
+        for _ in range(warmup):
+            call_pair(form, f)
+        barrier()
+        t_ms = t_dm = 0.0
+        phases = {}
+        l0 = ctx.stats()["kernel_launches"]
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        for _ in range(steps):
+            # the library runs on its own stream and synchronises before
+            # returning, so events on the current stream bracket each call
+            ev[0].record(stream)
+            st1 = None
+            ctx.ms2dirty(d_uvw, d_freq, f["vis"], nx, nx, px, px, f["eps"], precision=form,
+                         dirty=f["dirty"], **kw)
+            ev[1].record(stream)
+            st1 = ctx.stats()
+            ctx.dirty2ms(d_uvw, d_freq, f["model"], px, px, f["eps"], precision=form,
+                         vis=f["out"], **kw)
+            ev[2].record(stream)
+            st2 = ctx.stats()
+            torch.cuda.synchronize(dev)
+            t_ms += ev[0].elapsed_time(ev[1])
+            t_dm += ev[1].elapsed_time(ev[2])
+            for k in ("ms_prep", "ms_grid", "ms_fft", "ms_screen", "ms_total"):
+                phases.setdefault("ms2dirty_" + k, []).append(st1[k])
+                phases.setdefault("dirty2ms_" + k, []).append(st2[k])
+        barrier()
+        launches = ctx.stats()["kernel_launches"] - l0
+        tt = torch.tensor([t_ms, t_dm], dtype=torch.float64, device=dev)
+        if pg is not None:
+            pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        t_ms, t_dm = float(tt[0]), float(tt[1])
+        return t_ms, t_dm, {k: statistics.median(v) for k, v in phases.items()}, launches, st1, st2
+
+    # ---- timed region (mixed, the headline)
+    sampler = ClockSampler(local)
+    sampler.start()
+    t_ms, t_dm, phases, launches, st1, st2 = timed("mixed", args.steps, args.warmup)
+    clocks = sampler.stop()
+    ms_per_step = (t_ms + t_dm) / args.steps
+    value = world * nvis * args.steps / ((t_ms + t_dm) / 1e3) / 1e6
+    grid_info = {"nu": st1["nu"], "nv": st1["nv"], "nplanes": st1["nplanes"], "W": st1["supp"],
+                 "sigma": round(st1["sigma"], 4), "u_band_rows": st1["band_rows"]}
+
+    # ---- FP64 plain form (same workload)
+    fp64 = None
+    if not args.no_fp64:
+        k64 = max(2, args.steps // 3)
+        t64_ms, t64_dm, ph64, _, s64, _ = timed("fp64", k64, 1)
+        fp64 = {"value": world * nvis * k64 / ((t64_ms + t64_dm) / 1e3) / 1e6,
+                "ms2dirty_mvis_s": world * nvis * k64 / (t64_ms / 1e3) / 1e6,
+                "dirty2ms_mvis_s": world * nvis * k64 / (t64_dm / 1e3) / 1e6,
+                "ms_per_step": (t64_ms + t64_dm) / k64,
+                "grid": {"nu": s64["nu"], "nplanes": s64["nplanes"], "W": s64["supp"]}}
+
+    # ---- accuracy (outside the timed region): FP64 direct sums
+    rng = np.random.default_rng(99)
+    acc = {}
+    pix = rng.integers(0, nx * nx, 64)
+    vsel = rng.choice(nvis, 10000, replace=False)
+    dft_img = dft_pixels(uvw, freq, vis64, nx, nx, px, px, pix, torch, dev)
+    dft_vis = synth.predict_vis(uvw[vsel // nchan], freq, nx, nx, px, px, ix, iy, flux,
+                                device=dev)[:, 0] if nchan == 1 else None
+    for form in ("mixed",) + (() if args.no_fp64 else ("fp64",)):
+        f = forms[form]
+        call_pair(form, f)
+        torch.cuda.synchronize(dev)
+        img = f["dirty"].double().cpu().numpy().ravel()[pix]
+        acc[form] = {"ms2dirty_rel_rms_vs_dft": rel_rms(img, dft_img)}
+        if dft_vis is not None:
+            acc[form]["dirty2ms_rel_rms_vs_dft"] = rel_rms(
+                f["out"].cpu().numpy().ravel()[vsel], dft_vis)
+        # adjointness: |<y, A x> - <A^H y, x>| / (|y| |A x|)
+        g = torch.Generator(device="cpu").manual_seed(5)
+        x = torch.randn((nx, nx), generator=g, dtype=torch.float64).to(dev)
+        y = (torch.randn((nrows, nchan), generator=g, dtype=torch.float64)
+             + 1j * torch.randn((nrows, nchan), generator=g, dtype=torch.float64)).to(dev)
+        Ax = ctx.dirty2ms(d_uvw, d_freq, x, px, px, f["eps"], precision=form,
+                          vis_dtype=np.complex128, **kw)
+        Aty = ctx.ms2dirty(d_uvw, d_freq, y, nx, nx, px, px, f["eps"], precision=form,
+                           dirty_dtype=np.float64, **kw)
+        a = torch.vdot(y.ravel(), Ax.ravel()).real.item()
+        b = torch.vdot(Aty.ravel().to(torch.complex128), x.ravel().to(torch.complex128)).real.item()
+        acc[form]["adjoint_mismatch"] = abs(a - b) / (y.norm().item() * Ax.norm().item())
+        del x, y, Ax, Aty
+
+    # ---- end to end from pinned host buffers through the public API
+    h_uvw = torch.as_tensor(uvw).pin_memory()
+    h_freq = torch.as_tensor(freq)
+    h_vis = forms["mixed"]["vis"].cpu().pin_memory()
+    h_model = forms["mixed"]["model"].cpu().pin_memory()
+    h_dirty = torch.zeros((nx, nx), dtype=torch.float32).pin_memory()
+    h_out = torch.zeros((nrows, nchan), dtype=torch.complex64).pin_memory()
+
+    def e2e_step():
+        ctx.ms2dirty(h_uvw, h_freq, h_vis, nx, nx, px, px, EPS_MIXED, precision="mixed",
+                     dirty=h_dirty, **kw)
+        ctx.dirty2ms(h_uvw, h_freq, h_model, px, px, EPS_MIXED, precision="mixed", vis=h_out, **kw)
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    torch.cuda.synchronize(dev)
+    te = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=dev)
+    if pg is not None:
+        pg.all_reduce(te, op=pg.ReduceOp.MAX)
+    e2e_val = world * nvis * args.steps / float(te[0]) / 1e6
+    h2d = 2 * h_uvw.numel() * 8 + h_vis.numel() * 8 + h_model.numel() * 4 + 2 * nchan * 8
+    d2h = h_dirty.numel() * 4 + h_out.numel() * 8
+
+    # ---- roofline of the pipeline (algorithmic bytes, the reference's grid)
+    B = (algorithmic_bytes(nvis, nrows, nx, nx, DUCC_GRID["mixed"], 8, 8) * 2)
+    achieved = B / (ms_per_step / 1e3) / 1e9
+    peaks_path = os.path.join(HERE, "MEASURED_PEAKS.json")
+    peak, peak_src = 6650.0, "fallback"
+    if os.path.exists(peaks_path):
+        with open(peaks_path) as fh:
+            peak, peak_src = float(json.load(fh)["hbm_gbs"]), "measured"
+
+    # ---- CPU baseline (reference, rank 0, N=1)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            import oracle as O
+            if O.ref_available():
+                cores = os.cpu_count()
+                vis32 = forms["mixed"]["vis"].cpu().numpy()
+                m32 = forms["mixed"]["model"].cpu().numpy()
+                rk = dict(prec="float", negate_v=True, divide_by_n=False, sigma_min=1.1,
+                          sigma_max=2.0, nthreads=cores)
+                t0 = time.perf_counter()
+                O.ref_ms2dirty(uvw, freq, vis32, nx, nx, px, px, EPS_MIXED, **rk)
+                O.ref_dirty2ms(uvw, freq, m32, px, px, EPS_MIXED, **rk)
+                tc = time.perf_counter() - t0
+                cpu = {"value": nvis / tc / 1e6, "unit": UNIT, "cores": cores, "kind": "reference",
+                       "sample": "full workload, one ms2dirty + one dirty2ms, ducc0 <float,float> "
+                                 "at eps 1e-5 with WSClean's arguments"}
+        except Exception as e:  # reported, not fatal
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"failed: {e}"}
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 coords/phase/accumulate)",
+            "data": "synthetic (seeded Earth-rotation observation, 200 point sources)",
+            "config": {"workload": "config-2 adjoint pair: 8.1M vis, 4096^2 @ 5\", eps 1e-5",
+                       "nvis": nvis, "npix": nx, "parallelism": f"replicas x{world}",
+                       "l2": "inputs and grids larger than L2 (uvw 194 MB, grids GBs)",
+                       "grid": grid_info},
+            "ms2dirty_mvis_s": world * nvis * args.steps / (t_ms / 1e3) / 1e6,
+            "dirty2ms_mvis_s": world * nvis * args.steps / (t_dm / 1e3) / 1e6,
+            "fp64": fp64,
+            "mixed_over_fp64": (value / fp64["value"]) if fp64 else None,
+            "accuracy": acc,
+            "phases_ms": phases,
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "roofline": {"bound": "hbm", "kernel": "ms2dirty+dirty2ms pipeline",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "peak_source": peak_src,
+                         "bytes_per_step": B},
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "gpu_launches": launches,
+        }
+        print(json.dumps(out))
+    ctx.close()
+
+
+def main():
+    args = parse_args()
+    world, rank, local, pg = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local, pg)
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -171,9 +171,19 @@ typedef struct {
   size_t device_bytes;                /* device memory held by the context */
   int gridding;                       /* 1 ms2dirty, 0 dirty2ms */
   int precision;
+  size_t kernel_launches;             /* libwsg kernels launched by this process so far
+                                         (cuFFT/CUB library kernels not counted) */
 } wsg_stats;
 
 int wsg_get_stats(const wsg_ctx *ctx, wsg_stats *out);
+/* Host-only planning query: the grid, kernel and w-plane choice the library
+ * would make for these arguments and data statistics (active visibility
+ * count, |w| range and max |u|,|v| in wavelengths), without touching a GPU
+ * (ducc0 reports the same parameters at verbosity 1, wgridder.h:1535-1560).
+ * Fills nu, nv, nplanes, supp, band_rows, degree, sigma, beta, e0,
+ * kernel_err, wmin, wmax, dw, nshift and precision. */
+int wsg_plan_grid(const wsg_args *a, size_t nvis, double wmin, double wmax, double umax,
+                  double vmax, wsg_stats *out);
 /* Message of the last failed call on this thread ("" if none). */
 const char *wsg_last_error(void);
 int wsg_abi_version(void);

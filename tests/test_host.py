@@ -1,0 +1,123 @@
+"""Host-side checks that need no GPU: the C ABI library loads and exports
+every symbol include/wsg.h declares, struct layouts agree with the Python
+binding, the planning logic (kernel and grid choice) and error paths."""
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from wsclean_b200 import _lib as L
+from wsclean_b200 import gridder as G
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "wsg.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(wsg_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_exports_every_declared_symbol():
+    lib = L.lib()
+    names = declared_functions()
+    assert len(names) >= 20
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(names) == set(L.EXPORTED)
+    assert lib.wsg_abi_version() == 1
+
+
+def test_struct_layouts_match_binding(tmp_path):
+    prog = tmp_path / "layout.c"
+    prog.write_text(r'''
+#include <stdio.h>
+#include <stddef.h>
+#include "wsg.h"
+int main(void) {
+  printf("%zu %zu %zu %zu %zu\n", sizeof(wsg_args), sizeof(wsg_stats), sizeof(wsg_gridder_params),
+         offsetof(wsg_args, dirty_type), offsetof(wsg_stats, kernel_launches));
+  return 0;
+}''')
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(prog), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
+    got = [int(x) for x in out]
+    want = [ctypes.sizeof(L.WsgArgs), ctypes.sizeof(L.WsgStats), ctypes.sizeof(L.WsgGridderParams),
+            L.WsgArgs.dirty_type.offset, L.WsgStats.kernel_launches.offset]
+    assert got == want
+
+
+ARCSEC = np.pi / 180 / 3600
+
+
+def plan(**kw):
+    base = dict(npix_x=4096, npix_y=4096, pixsize_x=5 * ARCSEC, pixsize_y=5 * ARCSEC, epsilon=1e-5,
+                nvis=8_103_616, wmin=0.0, wmax=1764.0, umax=5756.0)
+    base.update(kw)
+    return G.plan_grid(**base)
+
+
+def test_plan_mixed_bench_workload():
+    s = plan()
+    assert s["supp"] <= 8 and s["kernel_err"] <= 1e-5
+    assert s["nu"] % 2 == 0 and s["nu"] >= 1.1 * 4096
+    # the u band: max|u| * pixsize * nu + W/2 + 2 cells on each side
+    L_ = np.ceil(5756.0 * 5 * ARCSEC * s["nu"] + s["supp"] / 2 + 2)
+    assert s["band_rows"] == 2 * L_ + 1
+    # w planes: (wmax-wmin)/dw + W planes, dw = 0.5/sigma/max|n-1+nshift|
+    assert s["nplanes"] == int(1764.0 / s["dw"] + s["supp"])
+
+
+def test_plan_fp64_uses_wider_kernel():
+    m = plan()
+    d = plan(precision="fp64", epsilon=1e-12)
+    assert d["supp"] > m["supp"] and d["kernel_err"] <= 1e-12
+    assert d["precision"] == L.WSG_PREC_FP64
+
+
+def test_plan_error_decreases_with_epsilon():
+    errs = [plan(precision="fp64", epsilon=e)["kernel_err"] for e in (1e-3, 1e-6, 1e-9, 1e-12)]
+    assert all(b < a for a, b in zip(errs, errs[1:]))
+
+
+def test_plan_no_w():
+    s = plan(do_wgridding=False)
+    assert s["nplanes"] == 1 and s["nshift"] == 0.0
+
+
+@pytest.mark.parametrize("bad", [dict(npix_x=4095), dict(epsilon=0.0), dict(pixsize_x=-1.0),
+                                 dict(epsilon=1e-9)])
+def test_plan_rejects_invalid(bad):
+    with pytest.raises(L.InvalidArgument):
+        plan(**bad)
+
+
+def test_no_gpu_fails_loudly():
+    """Without a GPU the product path raises; it never falls back to the CPU."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("GPU present")
+    with pytest.raises(L.WsgError):
+        G.Context(0)
+
+
+def test_kernel_table_consistent():
+    """Monotone error in W at fixed sigma, and one row refitted from scratch."""
+    from wsclean_b200 import kernel_db
+    rows = []
+    path = os.path.join(ROOT, "wsclean_b200", "csrc", "es_kernel_db.inc")
+    for line in open(path):
+        if line.startswith("{"):
+            W, s, e, b, e0 = [float(x) for x in line.strip("{},\n").split(",")]
+            rows.append((int(W), s, e, b, e0))
+    tab = {(W, s): (e, b, e0) for W, s, e, b, e0 in rows}
+    for s in (1.5, 2.0):
+        errs = [tab[(W, s)][0] for W in range(4, 12)]
+        assert all(b < a for a, b in zip(errs, errs[1:]))
+    e, b, e0 = tab[(6, 1.5)]
+    assert kernel_db.err1d(6, 1.5, b, e0) == pytest.approx(e, rel=1e-6)

@@ -27,6 +27,7 @@ EXPORTED = [
     "wsg_gridder_finalize_image", "wsg_gridder_real_image",
     "wsg_gridder_initialize_prediction", "wsg_gridder_predict_visibilities",
     "wsg_gridder_ctx", "wsg_get_stats", "wsg_last_error", "wsg_abi_version",
+    "wsg_plan_grid",
 ]
 
 c_size_t, c_double, c_int, c_void_p = ctypes.c_size_t, ctypes.c_double, ctypes.c_int, ctypes.c_void_p
@@ -71,6 +72,7 @@ class WsgStats(ctypes.Structure):
         ("ms_fft", c_double), ("ms_screen", c_double), ("ms_total", c_double),
         ("device_bytes", c_size_t),
         ("gridding", c_int), ("precision", c_int),
+        ("kernel_launches", c_size_t),
     ]
 
     def as_dict(self):
@@ -122,6 +124,8 @@ def lib():
         L.wsg_gridder_ctx.argtypes = [vp]
         L.wsg_gridder_ctx.restype = vp
         L.wsg_get_stats.argtypes = [vp, P(WsgStats)]
+        L.wsg_plan_grid.argtypes = [P(WsgArgs), c_size_t, c_double, c_double, c_double,
+                                    c_double, P(WsgStats)]
         L.wsg_last_error.restype = ctypes.c_char_p
         L.wsg_abi_version.restype = c_int
         for name in EXPORTED:

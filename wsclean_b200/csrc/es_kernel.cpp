@@ -173,15 +173,24 @@ PolyKernel fit_poly_kernel(const KernelSpec &k, double target_err) {
 }
 
 KernelTransform::KernelTransform(const KernelSpec &k) : W_(k.W) {
-  // composite rule on [0,1]: 64 panels x 16 nodes; phi has a branch point at
-  // t=1 which a single global rule resolves only to ~1e-12.
+  // Composite Gauss-Legendre on [0,1]: 8 uniform panels on [0,1/2], then 40
+  // panels halving toward t=1, 16 nodes each.  phi has a branch point at t=1;
+  // uniform panels resolve it only to ~1e-7 (W=4) .. 1e-11 (W=8) relative,
+  // the graded mesh to ~1e-15 for |nu| <= 1.
   std::vector<double> gx, gw;
   gauss_legendre(16, gx, gw);
-  const int npan = 64;
-  for (int p = 0; p < npan; ++p) {
-    double a = double(p) / npan, h = 1.0 / npan;
+  std::vector<double> edges;
+  for (int i = 0; i <= 8; ++i) edges.push_back(0.0625 * i);
+  double a = 0.5;
+  for (int i = 0; i < 40; ++i) {
+    a = 1.0 - 0.5 * (1.0 - a);
+    edges.push_back(a);
+  }
+  edges.push_back(1.0);
+  for (size_t p = 0; p + 1 < edges.size(); ++p) {
+    double lo = edges[p], h = edges[p + 1] - edges[p];
     for (size_t i = 0; i < gx.size(); ++i) {
-      double t = a + 0.5 * h * (gx[i] + 1.0);
+      double t = lo + 0.5 * h * (gx[i] + 1.0);
       t_.push_back(t);
       wphi_.push_back(0.5 * h * gw[i] * es_phi(t, k.W, k.beta, k.e0));
     }
@@ -196,10 +205,28 @@ double KernelTransform::operator()(double nu) const {
   return W_ * s;
 }
 
+double ChebCorr::operator()(double v) const {
+  double x = 2.0 * (v * v) / ymax - 1.0;
+  double b1 = 0, b2 = 0;  // Clenshaw
+  for (int j = n - 1; j >= 1; --j) {
+    double b0 = 2.0 * x * b1 - b2 + c[j];
+    b2 = b1;
+    b1 = b0;
+  }
+  return x * b1 - b2 + c[0];
+}
+
 ChebCorr fit_cheb_corr(const KernelTransform &tr, double vmax) {
   ChebCorr best;
   double ymax = std::max(vmax * vmax, 1e-30);
-  for (int n = 8; n <= kMaxCheb; n += 4) {
+  // check points (fixed) with their exact values
+  const int ntest = 65;
+  std::vector<double> vt(ntest), ref(ntest);
+  for (int s = 0; s < ntest; ++s) {
+    vt[s] = std::sqrt(ymax * s / (ntest - 1.0));
+    ref[s] = tr.corfunc(vt[s]);
+  }
+  for (int n = 12; n <= kMaxCheb; n += 6) {
     ChebCorr cc;
     cc.ymax = ymax;
     cc.n = n;
@@ -207,8 +234,7 @@ ChebCorr fit_cheb_corr(const KernelTransform &tr, double vmax) {
     std::vector<double> fv(n);
     for (int k = 0; k < n; ++k) {
       double xk = std::cos(M_PI * (k + 0.5) / n);
-      double y = 0.5 * (xk + 1.0) * ymax;
-      fv[k] = tr.corfunc(std::sqrt(y));
+      fv[k] = tr.corfunc(std::sqrt(0.5 * (xk + 1.0) * ymax));
     }
     for (int j = 0; j < n; ++j) {
       double s = 0;
@@ -216,22 +242,12 @@ ChebCorr fit_cheb_corr(const KernelTransform &tr, double vmax) {
       cc.c[j] = (j == 0 ? 1.0 : 2.0) * s / n;
     }
     double maxrel = 0;
-    for (int s = 0; s <= 200; ++s) {
-      double y = ymax * s / 200.0;
-      double x = 2.0 * y / ymax - 1.0;
-      double b1 = 0, b2 = 0;  // Clenshaw
-      for (int j = n - 1; j >= 1; --j) {
-        double b0 = 2.0 * x * b1 - b2 + cc.c[j];
-        b2 = b1;
-        b1 = b0;
-      }
-      double v = x * b1 - b2 + cc.c[0];
-      double ref = tr.corfunc(std::sqrt(y));
-      maxrel = std::max(maxrel, std::fabs(v - ref) / std::fabs(ref));
-    }
+    for (int s = 0; s < ntest; ++s)
+      maxrel = std::max(maxrel, std::fabs(cc(vt[s]) - ref[s]) / std::fabs(ref[s]));
     cc.max_rel_err = maxrel;
-    best = cc;
-    if (maxrel < 2e-15) break;
+    bool better = best.n == 0 || maxrel < best.max_rel_err;
+    if (better) best = cc;
+    if (maxrel < 1e-14 || !better) break;
   }
   return best;
 }

@@ -192,4 +192,46 @@ int wsg_gridder_predict_visibilities(wsg_gridder *g, size_t nrows, size_t nchan,
 
 wsg_ctx *wsg_gridder_ctx(wsg_gridder *g) { return g ? &g->view : nullptr; }
 
+int wsg_plan_grid(const wsg_args *a, size_t nvis, double wmin, double wmax, double umax,
+                  double vmax, wsg_stats *out) {
+  return guarded([&] {
+    wsg::require(a && out, "NULL argument");
+    wsg::GridPlan g;
+    g.nx = a->npix_x;
+    g.ny = a->npix_y;
+    g.px = a->pixsize_x;
+    g.py = a->pixsize_y;
+    g.eps = a->epsilon;
+    g.do_w = a->do_wgridding != 0;
+    g.fp32 = a->precision != WSG_PREC_FP64;
+    g.negate_v = a->negate_v != 0;
+    g.divide_by_n = a->divide_by_n != 0;
+    g.lshift = a->center_x;
+    g.mshift = a->negate_v ? -a->center_y : a->center_y;
+    g.nvis = nvis;
+    g.wmin_d = wmin;
+    g.wmax_d = wmax;
+    g.umax = umax;
+    g.vmax = vmax;
+    wsg::choose_grid(g, a->sigma_min, a->sigma_max, g.fp32 ? 16 : 8);
+    std::memset(out, 0, sizeof(*out));
+    out->nvis = nvis;
+    out->nu = g.nu;
+    out->nv = g.nv;
+    out->nplanes = g.nplanes;
+    out->supp = g.kernel.W;
+    out->band_rows = g.band_rows;
+    out->degree = g.poly.D;
+    out->sigma = g.ofactor;
+    out->beta = g.kernel.beta;
+    out->e0 = g.kernel.e0;
+    out->kernel_err = g.kernel.err;
+    out->wmin = wmin;
+    out->wmax = wmax;
+    out->dw = g.dw;
+    out->nshift = g.nshift;
+    out->precision = g.fp32 ? WSG_PREC_MIXED : WSG_PREC_FP64;
+  });
+}
+
 }  // extern "C"

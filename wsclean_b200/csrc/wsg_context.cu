@@ -5,6 +5,7 @@
 #include <cufft.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -23,6 +24,9 @@
 #include "wsg_device.cuh"
 
 namespace wsg {
+
+// libwsg kernels launched by this process (cuFFT and CUB kernels excluded).
+std::atomic<size_t> g_kernel_launches{0};
 
 // ------------------------------------------------------------ utilities
 
@@ -107,6 +111,7 @@ void Context::release_buffers() {
   for (auto &kv : fft_plans) cufftDestroy(kv.second);
   fft_plans.clear();
   for (auto *b : all_buffers()) b->release();
+  corr_valid = false;
   fwd_layout = adj_layout = {};
   fwd_L = 0;
   H_clean = false;
@@ -258,6 +263,7 @@ struct GridKernels {
       fn<<<grid, NWARP * 32, smem, st>>>(a, g, kc);
     }
     cuda_check(cudaGetLastError(), spread ? "k_spread launch" : "k_interp launch");
+  g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
   }
   template <int W>
   static int occupancy(bool spread, size_t smem) {
@@ -324,6 +330,7 @@ void launch_scan(Context &cx, const wsg_args &a, const Staged &s, bool gridding,
       reinterpret_cast<const TW *>(s.wgt), s.mask, gridding ? 1 : 0, a.negate_v ? -1.0 : 1.0,
       d_out, vis_out);
   cuda_check(cudaGetLastError(), "k_scan launch");
+  g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
 template <typename TW, typename TV>
@@ -335,6 +342,7 @@ void launch_keys(Context &cx, const wsg_args &a, const Staged &s, bool gridding,
                                             reinterpret_cast<const TW *>(s.wgt), s.mask,
                                             gridding ? 1 : 0, g, keys, vals);
   cuda_check(cudaGetLastError(), "k_keys launch");
+  g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
 template <typename R, typename TW, typename TV>
@@ -346,6 +354,7 @@ void launch_records(Context &cx, size_t nvis, const wsg_args &a, const Staged &s
       reinterpret_cast<const TW *>(s.wgt), gridding ? 1 : 0, g,
       reinterpret_cast<typename RecOf<R>::type *>(rec));
   cuda_check(cudaGetLastError(), "k_records launch");
+  g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
 // type-dispatch helpers over (weight type, vis type)
@@ -492,17 +501,13 @@ ScreenArgs make_screen(const GridPlan &g, const double *d_cf, const ChebCorr &cc
 
 }  // namespace
 
-// Grid-correction tables for the chosen kernel, uploaded to b_cf.
+// Grid-correction tables for the chosen kernel: 1/Phi as a Chebyshev series
+// in v^2 (evaluated per pixel on the device for the w term) and the 1-D u/v
+// correction arrays; cached per geometry, uploaded to b_cf.
 ChebCorr Context::upload_corrections(const GridPlan &g) {
-  KernelTransform tr(g.kernel);
-  std::vector<double> cf(g.nx / 2 + 1 + g.ny / 2 + 1);
-  for (size_t i = 0; i <= g.nx / 2; ++i) cf[i] = tr.corfunc(double(i) / g.nu);
-  for (size_t i = 0; i <= g.ny / 2; ++i) cf[g.nx / 2 + 1 + i] = tr.corfunc(double(i) / g.nv);
-  double *d = reinterpret_cast<double *>(b_cf.ensure(cf.size() * sizeof(double)));
-  CK(cudaMemcpyAsync(d, cf.data(), cf.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
-  ChebCorr cc;
+  double vmax = 0.5 * std::max(double(g.nx) / g.nu, double(g.ny) / g.nv) * 1.0000001;
   if (g.do_w) {
-    double vmax = 0.5 / g.ofactor * 1.0000001;
+    vmax = std::max(vmax, 0.5 / g.ofactor * 1.0000001);
     // pixels beyond the horizon use (sqrt(r^2-1)-1)*dw (wgridder.h:1376-1377)
     double xmin = g.lshift - 0.5 * g.nx * g.px, xmax = xmin + (g.nx - 1) * g.px;
     double ymin = g.mshift - 0.5 * g.ny * g.py, ymax = ymin + (g.ny - 1) * g.py;
@@ -511,13 +516,21 @@ ChebCorr Context::upload_corrections(const GridPlan &g) {
         double r2 = xc * xc + yc * yc;
         if (r2 > 1.0) vmax = std::max(vmax, std::fabs((std::sqrt(r2 - 1.0) - 1.0) * g.dw));
       }
-    cc = fit_cheb_corr(tr, std::min(vmax, 1.0));
-  } else {
-    cc.n = 1;
-    cc.c = {1.0};
-    cc.ymax = 1.0;
+    vmax = std::min(vmax, 1.0);
   }
+  auto key = std::make_tuple(g.kernel.W, g.kernel.beta, g.kernel.e0, g.nx, g.ny, g.nu, g.nv, vmax);
+  if (corr_valid && key == corr_key) return corr_cc;
+  KernelTransform tr(g.kernel);
+  ChebCorr cc = fit_cheb_corr(tr, vmax);
+  std::vector<double> cf(g.nx / 2 + 1 + g.ny / 2 + 1);
+  for (size_t i = 0; i <= g.nx / 2; ++i) cf[i] = cc(double(i) / g.nu);
+  for (size_t i = 0; i <= g.ny / 2; ++i) cf[g.nx / 2 + 1 + i] = cc(double(i) / g.nv);
+  double *d = reinterpret_cast<double *>(b_cf.ensure(cf.size() * sizeof(double)));
+  CK(cudaMemcpy(d, cf.data(), cf.size() * sizeof(double), cudaMemcpyHostToDevice));
   cheb_err = cc.max_rel_err;
+  corr_key = key;
+  corr_cc = cc;
+  corr_valid = true;
   return cc;
 }
 
@@ -642,6 +655,7 @@ void Context::grid_core(const wsg_args &a, const Staged &s, double *img, bool ac
     dim3 sg((gp.nx + 31) / 32, (gp.ny + 31) / 32);
     k_screen_add<R><<<sg, 256, 0, stream>>>(sa, H, img);
     cuda_check(cudaGetLastError(), "k_screen_add launch");
+  g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     CK(cudaEventRecord(ev[5], stream));
     CK(cudaEventSynchronize(ev[5]));
     float t;
@@ -695,7 +709,8 @@ void Context::degrid_core(const wsg_args &a, const Staged &s, const double *img,
   char *band = reinterpret_cast<char *>(b_band.ensure(gp.band_rows * P * nv * cs));
   char *full = reinterpret_cast<char *>(b_full_adj.ensure(nu * P * nv * cs));
   char *H = reinterpret_cast<char *>(b_H.ensure(P * gp.ny * nu * cs));
-  // invariant of the adjoint full grid: columns outside the image columns are zero
+  // invariant of the adjoint full grid ([P][nv][nu]): rows v outside the
+  // image columns are zero (never written)
   Layout lay{nu, nv, P, cs};
   if (!(lay == adj_layout)) {
     CK(cudaMemsetAsync(full, 0, nu * P * nv * cs, stream));
@@ -742,26 +757,37 @@ void Context::degrid_core(const wsg_args &a, const Staged &s, const double *img,
     dim3 sg((gp.nx + 31) / 32, (gp.ny + 31) / 32);
     k_screen_put<R><<<sg, 256, 0, stream>>>(sa, img, H);
     cuda_check(cudaGetLastError(), "k_screen_put launch");
+  g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     CK(cudaEventRecord(ev[3], stream));
-    // pass 2 (transposed): along u, H[p][j][u] -> image columns of the full grid
+    // pass 2 (transposed): along u, H[p][j][u] -> rows of the adjoint full
+    // grid, laid out [P][nv][nu] so that this pass writes contiguously
     {
       const int half = int(gp.ny / 2);
-      cufftHandle h2 = fft_plan(int(nu), 1, int(nu), int(P * nv), 1, half, dbl);
+      cufftHandle h2 = fft_plan(int(nu), 1, int(nu), 1, int(nu), half, dbl);
       for (size_t p = 0; p < npl; ++p) {
-        fft_exec(h2, H + (p * gp.ny + half) * nu * cs, full + (p * nv) * cs, dir, dbl);
-        fft_exec(h2, H + (p * gp.ny) * nu * cs, full + (p * nv + nv - half) * cs, dir, dbl);
+        // image columns [ny/2, ny) are grid columns [0, ny/2)
+        fft_exec(h2, H + (p * gp.ny + half) * nu * cs, full + (p * nv) * nu * cs, dir, dbl);
+        // image columns [0, ny/2) are grid columns [nv-ny/2, nv)
+        fft_exec(h2, H + (p * gp.ny) * nu * cs, full + (p * nv + nv - half) * nu * cs, dir, dbl);
       }
     }
-    // pass 1 (transposed): along v over the band rows, into the band grid
-    if (gp.band_full) {
-      cufftHandle h = fft_plan(int(nv), 1, int(nv), 1, int(nv), int(nu * P), dbl);
-      fft_exec(h, full, band, dir, dbl);
-    } else {
-      const size_t rowb = P * nv * cs;
-      cufftHandle hlo = fft_plan(int(nv), 1, int(nv), 1, int(nv), int((L + 1) * P), dbl);
-      fft_exec(hlo, full, band, dir, dbl);
-      cufftHandle hhi = fft_plan(int(nv), 1, int(nv), 1, int(nv), int(L * P), dbl);
-      fft_exec(hhi, full + (nu - L) * rowb, band + (L + 1) * rowb, dir, dbl);
+    // pass 1 (transposed): along v (stride nu) for the band rows u, into the
+    // band grid [band_rows][P][nv]
+    {
+      const int pnv = int(P * nv);
+      for (size_t p = 0; p < npl; ++p) {
+        char *src = full + p * nv * nu * cs;
+        char *dst = band + p * nv * cs;
+        if (gp.band_full) {
+          cufftHandle h = fft_plan(int(nv), int(nu), 1, 1, pnv, int(nu), dbl);
+          fft_exec(h, src, dst, dir, dbl);
+        } else {
+          cufftHandle hlo = fft_plan(int(nv), int(nu), 1, 1, pnv, int(L + 1), dbl);
+          fft_exec(hlo, src, dst, dir, dbl);
+          cufftHandle hhi = fft_plan(int(nv), int(nu), 1, 1, pnv, int(L), dbl);
+          fft_exec(hhi, src + (nu - L) * cs, dst + (L + 1) * P * nv * cs, dir, dbl);
+        }
+      }
     }
     CK(cudaEventRecord(ev[4], stream));
     CK(cudaMemsetAsync(counter, 0, sizeof(int), stream));
@@ -819,6 +845,7 @@ void Context::record_stats(const GridPlan &g, bool gridding, size_t P) {
   stats.gridding = gridding;
   stats.precision = g.fp32 ? WSG_PREC_MIXED : WSG_PREC_FP64;
   stats.device_bytes = device_bytes();
+  stats.kernel_launches = g_kernel_launches.load();
 }
 
 void Context::print_report(const GridPlan &g, bool gridding, size_t P) {
@@ -856,6 +883,8 @@ void Context::ms2dirty(const wsg_args &a, const void *vis, void *dirty, int accu
       k_load_image<double><<<nb, 256, 0, stream>>>(npix, (const double *)din, img, 0);
     else
       k_load_image<float><<<nb, 256, 0, stream>>>(npix, (const float *)din, img, 0);
+    cuda_check(cudaGetLastError(), "k_load_image launch");
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
   }
   if (a.precision == WSG_PREC_FP64)
     grid_core<double>(a, s, img, accumulate != 0);
@@ -869,12 +898,14 @@ void Context::ms2dirty(const wsg_args &a, const void *vis, void *dirty, int accu
   else
     k_store_image<float><<<nb, 256, 0, stream>>>(npix, img, (float *)dout);
   cuda_check(cudaGetLastError(), "k_store_image launch");
+  g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
   if (!ddev) CK(cudaMemcpyAsync(dirty, dout, npix * dsz, cudaMemcpyDeviceToHost, stream));
   CK(cudaEventRecord(ev[6], stream));
   CK(cudaStreamSynchronize(stream));
   float t;
   CK(cudaEventElapsedTime(&t, ev[0], ev[6]));
   stats.ms_total = t;
+  stats.kernel_launches = g_kernel_launches.load();
   stats.nrows = a.nrows;
   stats.nchan = a.nchan;
 }
@@ -899,6 +930,7 @@ void Context::dirty2ms(const wsg_args &a, const void *dirty, void *vis) {
   else
     k_load_image<float><<<nb, 256, 0, stream>>>(npix, (const float *)din, img, 0);
   cuda_check(cudaGetLastError(), "k_load_image launch");
+  g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
   degrid_from_image(a, s, img, vis, vbytes);
 }
 
@@ -919,6 +951,7 @@ void Context::degrid_from_image(const wsg_args &a, const Staged &s, const double
   float t;
   CK(cudaEventElapsedTime(&t, ev[0], ev[6]));
   stats.ms_total = t;
+  stats.kernel_launches = g_kernel_launches.load();
   stats.nrows = a.nrows;
   stats.nchan = a.nchan;
 }
@@ -997,6 +1030,7 @@ void Gridder::finalize_image(double f) {
   size_t n = prm.width_t * prm.height_t;
   k_scale<<<launch_blocks(n, 256), 256, 0, ctx.stream>>>(n, reinterpret_cast<double *>(ctx.b_img2.p), f);
   cuda_check(cudaGetLastError(), "k_scale launch");
+  g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
   CK(cudaStreamSynchronize(ctx.stream));
 }
 
@@ -1010,6 +1044,7 @@ void Gridder::real_image(float *out) {
       int(prm.width_t), int(prm.height_t), int(prm.width), int(prm.height), dx, dy,
       reinterpret_cast<const double *>(ctx.b_img2.p), d);
   cuda_check(cudaGetLastError(), "k_retrim launch");
+  g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
   if (!odev) CK(cudaMemcpyAsync(out, d, n * sizeof(float), cudaMemcpyDeviceToHost, ctx.stream));
   CK(cudaStreamSynchronize(ctx.stream));
 }
@@ -1024,6 +1059,7 @@ void Gridder::initialize_prediction(const float *image) {
   k_untrim<<<launch_blocks(prm.width_t * prm.height_t, 256), 256, 0, ctx.stream>>>(
       int(prm.width_t), int(prm.height_t), int(prm.width), dx, dy, d, img);
   cuda_check(cudaGetLastError(), "k_untrim launch");
+  g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
   CK(cudaStreamSynchronize(ctx.stream));
   have_img = true;
 }

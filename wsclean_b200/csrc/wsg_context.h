@@ -93,6 +93,10 @@ class Context {
   Layout fwd_layout, adj_layout, H_layout;
   size_t fwd_L = 0;
   bool H_clean = false;
+  // correction-table cache
+  std::tuple<int, double, double, size_t, size_t, size_t, size_t, double> corr_key;
+  ChebCorr corr_cc;
+  bool corr_valid = false;
 };
 
 // WGriddingGridder_Simple replacement (wgridder/wgriddinggridder_simple.h:34-144).

@@ -83,6 +83,7 @@ struct ChebCorr {
   int n = 0;  // number of coefficients
   std::vector<double> c;
   double max_rel_err = 0;
+  double operator()(double v) const;
 };
 ChebCorr fit_cheb_corr(const KernelTransform &tr, double vmax);
 

@@ -287,3 +287,25 @@ class WGriddingGridder:
         s = L.WsgStats()
         L.check(L.lib().wsg_get_stats(L.lib().wsg_gridder_ctx(self._h), ctypes.byref(s)))
         return s.as_dict()
+
+
+def plan_grid(npix_x, npix_y, pixsize_x, pixsize_y, epsilon, nvis, wmin, wmax, umax, vmax=None,
+              do_wgridding=True, precision="mixed", negate_v=True, divide_by_n=False,
+              sigma_min=1.1, sigma_max=2.0, center_x=0.0, center_y=0.0):
+    """The grid/kernel/w-plane choice for given data statistics (host only,
+    no GPU): |w| range and max |u|, |v| in wavelengths."""
+    a = L.WsgArgs()
+    L.lib().wsg_args_init(ctypes.byref(a))
+    a.npix_x, a.npix_y = int(npix_x), int(npix_y)
+    a.pixsize_x, a.pixsize_y = float(pixsize_x), float(pixsize_y)
+    a.epsilon = float(epsilon)
+    a.do_wgridding = int(bool(do_wgridding))
+    a.precision = _precision(precision)
+    a.negate_v, a.divide_by_n = int(bool(negate_v)), int(bool(divide_by_n))
+    a.sigma_min, a.sigma_max = float(sigma_min), float(sigma_max)
+    a.center_x, a.center_y = float(center_x), float(center_y)
+    s = L.WsgStats()
+    L.check(L.lib().wsg_plan_grid(ctypes.byref(a), int(nvis), float(wmin), float(wmax),
+                                  float(umax), float(umax if vmax is None else vmax),
+                                  ctypes.byref(s)))
+    return s.as_dict()
