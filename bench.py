@@ -51,11 +51,13 @@ DUCC_GRID = {"mixed": (7392, 7392, 14), "fp64": (7392, 7392, 22)}
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-clocks", action="store_true",
+                    help="do not sample nvidia-smi during the timed region")
     return ap.parse_args()
 
 
@@ -82,7 +84,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -299,7 +301,8 @@ def run_ours(args, world, rank, local, pg):
 
     # ---- timed region (mixed, the headline)
     sampler = ClockSampler(local)
-    sampler.start()
+    if not args.no_clocks:
+        sampler.start()
     t_ms, t_dm, phases, launches, st1, st2 = timed("mixed", args.steps, args.warmup)
     clocks = sampler.stop()
     ms_per_step = (t_ms + t_dm) / args.steps

@@ -126,7 +126,8 @@ PolyKernel fit_poly_kernel(const KernelSpec &k, double target_err) {
   PolyKernel best;
   // Test points: 97 per piece, including the piece edges.
   const int ntest = 97;
-  for (int D = W + 1; D <= std::min(kMaxDeg, W + 10); ++D) {
+  // the device evaluates degree W+4 (lower-degree fits are zero-padded)
+  for (int D = W + 1; D <= std::min(kMaxDeg, W + 4); ++D) {
     const int n = D + 1;
     std::vector<long double> A(n * n);
     std::vector<double> xs(n);
@@ -289,6 +290,29 @@ void set_band(GridPlan &g) {
 
 }  // namespace
 
+// nu = K * 2^m with 2^m >= 2L+1, so that the occupied u band fits one pruned
+// FFT of length 2^m (or K = 1, 2^m = nu when the band covers the grid);
+// the smallest such nu >= n0.
+bool pick_nu(double n0, double umax_px, int W, bool fp32, size_t &nu, int &logM, int &K) {
+  const int mmax = fp32 ? 13 : 12;
+  size_t best = ~size_t(0);
+  for (int m = 8; m <= mmax; ++m) {
+    const size_t M = size_t(1) << m;
+    const size_t k = std::max<size_t>(1, size_t(std::ceil(n0 / double(M))));
+    const size_t n = k * M;
+    const double L = std::ceil(umax_px * double(n) + 0.5 * W + 2.0);
+    const bool full = 2.0 * L + 1.0 >= double(n);
+    if (full ? (k != 1) : (2.0 * L + 1.0 > double(M))) continue;
+    if (n < best) {
+      best = n;
+      nu = n;
+      logM = m;
+      K = int(k);
+    }
+  }
+  return best != ~size_t(0);
+}
+
 void choose_grid(GridPlan &g, double sigma_min, double sigma_max, int tile) {
   require(g.nx % 2 == 0, "nx_dirty must be even");
   require(g.ny % 2 == 0, "ny_dirty must be even");
@@ -318,19 +342,22 @@ void choose_grid(GridPlan &g, double sigma_min, double sigma_max, int tile) {
   if (g.do_w) require(nmax > 0, "image too small for w-gridding (n-1 range is zero)");
 
   auto cands = available_kernels(g.eps, g.do_w ? 3 : 2, g.fp32, sigma_min, sigma_max);
-  // Cost model (seconds): FFT-stage memory traffic per plane -- pruned pass
-  // along v over the occupied u band, pass along u over the image columns,
-  // w-screen over the image -- plus the spreading work nvis*W^3.
+  // Cost model (seconds), per w plane: band grid traffic (zero, spread flush,
+  // v transform), the pruned u transform (band in, image rows out), the
+  // w-screen pass; plus the spreading work nvis * W^3.
   const double cs = g.fp32 ? 8.0 : 16.0;
   const double hbm = 5.0e12;
-  const double c_cell = g.fp32 ? 2.0e-13 : 1.2e-12;
+  const double c_cell = g.fp32 ? 1.0e-13 : 6.0e-13;
+  const double c_fftpt = g.fp32 ? 1.5e-12 : 4.0e-12;
+  const double umax_px = g.umax * g.px;
   double best = 1e300;
   KernelSpec bestk{};
   size_t bnu = 0, bnv = 0;
+  int blogM = 0, bK = 1;
   for (const auto &k : cands) {
     GridPlan t = g;
     t.kernel = k;
-    t.nu = 2 * good_size_cufft(size_t(g.nx * k.sigma * 0.5) + 1);
+    if (!pick_nu(g.nx * k.sigma, umax_px, k.W, g.fp32, t.nu, t.logM, t.K)) continue;
     t.nv = 2 * good_size_cufft(size_t(g.ny * k.sigma * 0.5) + 1);
     set_band(t);
     double planes = 1;
@@ -339,8 +366,11 @@ void choose_grid(GridPlan &g, double sigma_min, double sigma_max, int tile) {
       double dw = 0.5 / of / nmax;
       planes = std::floor((g.wmax_d - g.wmin_d) / dw + k.W);
     }
-    double per_plane = cs * (3.0 * t.band_rows * t.nv + 2.0 * t.nu * g.ny + 1.0 * g.nx * g.ny);
-    double fft = planes * per_plane / hbm;
+    const double M = double(size_t(1) << t.logM);
+    double per_plane = cs * (4.0 * t.band_rows * t.nv + 1.0 * t.band_rows * g.ny +
+                             3.0 * g.nx * g.ny) / hbm +
+                       c_fftpt * g.ny * t.K * M * t.logM / 148.0;
+    double fft = planes * per_plane;
     double grid = double(g.nvis) * k.W * k.W * (g.do_w ? k.W : 1) * c_cell;
     double cost = fft + grid;
     if (cost < best) {
@@ -348,11 +378,16 @@ void choose_grid(GridPlan &g, double sigma_min, double sigma_max, int tile) {
       bestk = k;
       bnu = t.nu;
       bnv = t.nv;
+      blogM = t.logM;
+      bK = t.K;
     }
   }
+  require(bnu > 0, "no grid size satisfies the pruned-FFT layout (image or band too large)");
   g.kernel = bestk;
   g.nu = bnu;
   g.nv = bnv;
+  g.logM = blogM;
+  g.K = bK;
   g.ofactor = std::min(double(g.nu) / g.nx, double(g.nv) / g.ny);
   const int W = bestk.W;
   g.nsafe = (W + 1) / 2;
@@ -374,9 +409,15 @@ void choose_grid(GridPlan &g, double sigma_min, double sigma_max, int tile) {
     g.nplanes = 1;
   }
   set_band(g);
+  if (g.band_full)
+    require(g.K == 1 && (size_t(1) << g.logM) == g.nu, "internal: full band needs K == 1");
+  else
+    require((size_t(1) << g.logM) >= g.band_rows, "internal: band exceeds the pruned FFT");
   double target = g.fp32 ? std::max(0.02 * g.kernel.err, 2e-8) : 0.02 * g.kernel.err;
   g.poly = fit_poly_kernel(g.kernel, target);
 
+  // a tile row plus halo (T + W - 1 cells) is staged by one warp's lanes
+  tile = std::max(1, std::min(tile, 33 - W));
   g.T = tile;
   g.ntu = int((g.nu + 1) / tile) + 1;
   g.ntv = int((g.nv + 1) / tile) + 1;
@@ -390,12 +431,9 @@ void choose_grid(GridPlan &g, double sigma_min, double sigma_max, int tile) {
 }
 
 size_t plan_bytes(const GridPlan &g, size_t planes, bool gridding) {
-  size_t cs = g.fp32 ? 8 : 16;
-  size_t band = g.band_rows * planes * g.nv * cs;
-  size_t full = g.nu * planes * g.nv * cs;
-  size_t h = planes * g.ny * g.nu * cs;
+  const size_t cs = g.fp32 ? 8 : 16;
   (void)gridding;
-  return band + full + h;
+  return planes * cs * (g.band_rows * g.nv + g.ny * g.nx);
 }
 
 }  // namespace wsg

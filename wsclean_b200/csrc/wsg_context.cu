@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -88,6 +89,23 @@ Context::Context(int dev) {
   CK(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
   for (auto &e : ev) CK(cudaEventCreate(&e));
   std::memset(&stats, 0, sizeof(stats));
+  verbosity = env_int("WSG_VERBOSITY", 0);
+}
+
+void Context::mark(const char *what) {
+  if (verbosity < 2) return;
+  marks.emplace_back(what, std::chrono::steady_clock::now());
+}
+
+void Context::print_marks(const char *title) {
+  if (verbosity < 2 || marks.empty()) return;
+  std::printf("  host timeline (%s):", title);
+  for (size_t i = 1; i < marks.size(); ++i)
+    std::printf(" %s %.3f ms;", marks[i].first,
+                std::chrono::duration<double, std::milli>(marks[i].second - marks[i - 1].second).count());
+  std::printf("\n");
+  std::fflush(stdout);
+  marks.clear();
 }
 
 Context::~Context() {
@@ -101,8 +119,8 @@ Context::~Context() {
 
 std::vector<DevBuf *> Context::all_buffers() {
   return {&b_uvw, &b_fovc, &b_vis, &b_wgt, &b_mask, &b_keys_a, &b_keys_b, &b_vals_a,
-          &b_vals_b, &b_cub, &b_rec, &b_chunks, &b_small, &b_band, &b_full_fwd,
-          &b_full_adj, &b_H, &b_img, &b_img2, &b_acc, &b_cf, &b_fftwork, &b_out};
+          &b_vals_b, &b_cub, &b_rec, &b_chunks, &b_small, &b_band, &b_H,
+          &b_img, &b_img2, &b_acc, &b_cf, &b_tw, &b_fftwork, &b_out};
 }
 
 void Context::release_buffers() {
@@ -112,9 +130,7 @@ void Context::release_buffers() {
   fft_plans.clear();
   for (auto *b : all_buffers()) b->release();
   corr_valid = false;
-  fwd_layout = adj_layout = {};
-  fwd_L = 0;
-  H_clean = false;
+  tw_valid = false;
 }
 
 size_t Context::device_bytes() {
@@ -235,17 +251,25 @@ int launch_blocks(size_t n, int threads) {
 // Kernel template dispatch over the support W.
 template <typename R>
 struct GridKernels {
-  static constexpr int NWARP = sizeof(R) == 4 ? 8 : 16;
+  static constexpr int NWARP = 8;
   static constexpr int SB = sizeof(R) == 4 ? 256 : 64;
   template <int W>
   static constexpr int ppl() {
     return (sizeof(R) == 4 && W * W > 32) ? 2 : 1;
   }
   static size_t smem_bytes(const TileLayout &tl, int W, bool spread) {
-    size_t kst = 3 * W + 1;
-    size_t s = sizeof(R) * (2 * size_t(W) * tl.PS + SB * kst + 2 * SB) + 4 * SB;
+    const size_t kst = sizeof(R) == 4 ? ((3 * size_t(W) + 3) & ~size_t(3))
+                                      : ((3 * size_t(W) + 1) & ~size_t(1));
+    const size_t stage = sizeof(R) * (32 * kst + 64) + 128;  // WarpStage<R, W>::bytes
+    size_t tile = ((sizeof(R) * 2 * size_t(W) * tl.PS) + 15) & ~size_t(15);
     (void)spread;
-    return (s + 15) & ~size_t(15);
+    return tile + size_t(NWARP) * stage;
+  }
+  // warps that share one record (more than one when a lane's share of the
+  // W x W (plane, u-row) pairs would exceed PPL)
+  static int groups(int W) {
+    const int ppl = (sizeof(R) == 4 && W * W > 32) ? 2 : 1;
+    return (W * W + 32 * ppl - 1) / (32 * ppl);
   }
   template <int W>
   static void run(bool spread, dim3 grid, size_t smem, cudaStream_t st, const GridArgs &a,
@@ -312,6 +336,47 @@ struct GridKernels {
       case 15: go(std::integral_constant<int, 15>{}); break;
       case 16: go(std::integral_constant<int, 16>{}); break;
       default: throw std::runtime_error("unsupported kernel support");
+    }
+  }
+};
+
+// Pruned u-transform kernels, dispatched over log2(M).
+template <typename R>
+struct ColKernels {
+  template <int LOGM>
+  static void run1(bool bwd, const ColArgs &a, int npl, cudaStream_t st) {
+    constexpr int M = 1 << LOGM;
+    using Cfg = ColCfg<R, M>;
+    const size_t smem = ColSmem<R, M>::bytes();
+    dim3 grid((a.ny + Cfg::NB - 1) / Cfg::NB, npl);
+    if (bwd) {
+      cuda_check(cudaFuncSetAttribute(k_ucol_bwd<R, LOGM>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+                 "smem attribute");
+      k_ucol_bwd<R, LOGM><<<grid, Cfg::THREADS, smem, st>>>(a);
+    } else {
+      cuda_check(cudaFuncSetAttribute(k_ucol_fwd<R, LOGM>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+                 "smem attribute");
+      k_ucol_fwd<R, LOGM><<<grid, Cfg::THREADS, smem, st>>>(a);
+    }
+    cuda_check(cudaGetLastError(), bwd ? "k_ucol_bwd launch" : "k_ucol_fwd launch");
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+  }
+  static void run(int logM, bool bwd, const ColArgs &a, int npl, cudaStream_t st) {
+    switch (logM) {
+      case 8: run1<8>(bwd, a, npl, st); break;
+      case 9: run1<9>(bwd, a, npl, st); break;
+      case 10: run1<10>(bwd, a, npl, st); break;
+      case 11: run1<11>(bwd, a, npl, st); break;
+      case 12: run1<12>(bwd, a, npl, st); break;
+      case 13:
+        if constexpr (sizeof(R) == 4) {
+          run1<13>(bwd, a, npl, st);
+          break;
+        }
+        [[fallthrough]];
+      default: throw std::runtime_error("unsupported pruned FFT length");
     }
   }
 };
@@ -392,6 +457,7 @@ template <typename R>
 bool Context::prepare(const wsg_args &a, const Staged &s, bool gridding, void *vis_out_dev,
                       GridPlan &gp) {
   const size_t nvis_tot = a.nrows * a.nchan;
+  mark("enter");
   // freq checks (Baselines ctor, wgridder.h:300-309) and f/c
   std::vector<double> freq(a.nchan), fovc(a.nchan);
   if (is_device_pointer(a.freq))
@@ -420,7 +486,9 @@ bool Context::prepare(const wsg_args &a, const Staged &s, bool gridding, void *v
   });
   ScanOut hs;
   CK(cudaMemcpyAsync(&hs, d_scan, sizeof(hs), cudaMemcpyDeviceToHost, stream));
+  mark("scan-submit");
   CK(cudaStreamSynchronize(stream));
+  mark("scan-sync");
   gp.nvis = hs.nvis;
   if (gp.nvis == 0) return false;
   auto bits2d = [](unsigned long long b) {
@@ -436,6 +504,7 @@ bool Context::prepare(const wsg_args &a, const Staged &s, bool gridding, void *v
   int tile = env_int("WSG_TILE", sizeof(R) == 4 ? 16 : 8);
   choose_grid(gp, a.sigma_min, a.sigma_max, tile);
   DevGeom g = make_geom(gp);
+  mark("choose_grid");
 
   // keys + sort
   uint32_t *ka = reinterpret_cast<uint32_t *>(b_keys_a.ensure(nvis_tot * 4));
@@ -470,6 +539,7 @@ bool Context::prepare(const wsg_args &a, const Staged &s, bool gridding, void *v
   CK(cub::DeviceSelect::If(nullptr, tmp, it, chunks, d_nch, int(gp.nvis), pred, stream));
   dtmp = b_cub.ensure(std::max(tmp, b_cub.n));
   CK(cub::DeviceSelect::If(dtmp, tmp, it, chunks, d_nch, int(gp.nvis), pred, stream));
+  mark("sort+records-submit");
   return true;
 }
 
@@ -497,6 +567,25 @@ ScreenArgs make_screen(const GridPlan &g, const double *d_cf, const ChebCorr &cc
   s.ymax = cc.ymax;
   for (int i = 0; i < cc.n && i < kDMaxCheb; ++i) s.cheb[i] = cc.c[i];
   return s;
+}
+
+ColArgs make_col(const GridPlan &g, size_t P, const void *tw, void *band, void *H) {
+  ColArgs c{};
+  c.nx = int(g.nx);
+  c.ny = int(g.ny);
+  c.nu = int(g.nu);
+  c.nv = int(g.nv);
+  c.P = int(P);
+  c.L = int(g.Lu);
+  c.band_rows = int(g.band_rows);
+  c.band_full = g.band_full;
+  c.K = g.K;
+  const size_t cs = g.fp32 ? 8 : 16;
+  c.twM = tw;
+  c.twnu = reinterpret_cast<const char *>(tw) + (size_t(1) << g.logM) * cs;
+  c.band = band;
+  c.H = H;
+  return c;
 }
 
 }  // namespace
@@ -534,10 +623,54 @@ ChebCorr Context::upload_corrections(const GridPlan &g) {
   return cc;
 }
 
+// FP64-computed twiddle tables: the per-stage tables of the length-M
+// shared-memory FFT (M entries) and exp(+2 pi i t / nu) for the twist (nu
+// entries), stored in the arithmetic type, cached per (M, nu, type).
+const void *Context::upload_twiddles(const GridPlan &g, bool dbl) {
+  const size_t M = size_t(1) << g.logM;
+  auto key = std::make_tuple(M, g.nu, int(dbl));
+  const size_t cs = dbl ? 16 : 8;
+  if (!(tw_valid && key == tw_key)) {
+    std::vector<double> h(2 * (M + g.nu), 0.0);
+    // per-stage FFT twiddles exp(+2 pi i r k / (NS R)), [r-1][k], stage order
+    size_t off = 0;
+    for (size_t NS = 1; NS < M;) {
+      const size_t R = (M / NS >= 16) ? 16 : M / NS;
+      if (NS > 1) {
+        for (size_t r = 1; r < R; ++r)
+          for (size_t k = 0; k < NS; ++k) {
+            const double f = double(r * k) / double(NS * R);
+            h[2 * (off + (r - 1) * NS + k)] = std::cos(2.0 * M_PI * f);
+            h[2 * (off + (r - 1) * NS + k) + 1] = std::sin(2.0 * M_PI * f);
+          }
+        off += (R - 1) * NS;
+      }
+      NS *= R;
+    }
+    for (size_t t = 0; t < g.nu; ++t) {
+      // reduce t/nu to [-1/2, 1/2] turns before the FP64 sin/cos
+      double f = double(t) / double(g.nu);
+      if (f > 0.5) f -= 1.0;
+      h[2 * (M + t)] = std::cos(2.0 * M_PI * f);
+      h[2 * (M + t) + 1] = std::sin(2.0 * M_PI * f);
+    }
+    void *d = b_tw.ensure((M + g.nu) * cs);
+    if (dbl) {
+      CK(cudaMemcpy(d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+    } else {
+      std::vector<float> hf(h.begin(), h.end());
+      CK(cudaMemcpy(d, hf.data(), hf.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    tw_key = key;
+    tw_valid = true;
+  }
+  return b_tw.p;
+}
+
 size_t Context::choose_planes(const GridPlan &g, bool gridding) {
   size_t total = 0, freeb = 0;
   CK(cudaMemGetInfo(&freeb, &total));
-  size_t held = b_band.n + b_H.n + (gridding ? b_full_fwd.n : b_full_adj.n);
+  size_t held = b_band.n + b_H.n;
   double budget = 0.55 * double(total);
   size_t avail = size_t(std::min<double>(budget, double(freeb + held) - 2e9));
   size_t per = plan_bytes(g, 1, gridding);
@@ -575,28 +708,15 @@ void Context::grid_core(const wsg_args &a, const Staged &s, double *img, bool ac
   ChebCorr cc = upload_corrections(gp);
   DevGeom g = make_geom(gp);
   DevKernel<R> kc = make_kernel<R>(gp.poly);
+  mark("corrections");
   const size_t P = choose_planes(gp, true);
+  mark("choose_planes");
   const size_t cs = 2 * sizeof(R);
-  const size_t nv = gp.nv, nu = gp.nu;
+  const size_t nv = gp.nv;
   char *band = reinterpret_cast<char *>(b_band.ensure(gp.band_rows * P * nv * cs));
-  char *full = reinterpret_cast<char *>(b_full_fwd.ensure(nu * P * nv * cs));
-  char *H = reinterpret_cast<char *>(b_H.ensure(P * gp.ny * nu * cs));
-  H_clean = false;
-  // invariant of the full grid: rows outside the u band are zero
-  Layout lay{nu, nv, P, cs};
-  if (!(lay == fwd_layout)) {
-    CK(cudaMemsetAsync(full, 0, nu * P * nv * cs, stream));
-    fwd_layout = lay;
-    fwd_L = 0;
-  }
-  const size_t L = gp.band_full ? nu / 2 : gp.Lu;
-  if (!gp.band_full && fwd_L > L) {
-    const size_t rowb = P * nv * cs;
-    CK(cudaMemsetAsync(full + (L + 1) * rowb, 0, (fwd_L - L) * rowb, stream));
-    CK(cudaMemsetAsync(full + (nu - fwd_L) * rowb, 0, (fwd_L - L) * rowb, stream));
-  }
-  fwd_L = gp.band_full ? nu / 2 : L;
-
+  char *H = reinterpret_cast<char *>(b_H.ensure(P * gp.ny * gp.nx * cs));
+  const void *tw = upload_twiddles(gp, dbl);
+  ColArgs ca = make_col(gp, P, tw, band, H);
   const TileLayout tl = make_layout(gp.T, gp.kernel.W);
   const size_t smem = GridKernels<R>::smem_bytes(tl, gp.kernel.W, true);
   int *counter = reinterpret_cast<int *>(reinterpret_cast<char *>(b_small.p) + 2048);
@@ -626,28 +746,13 @@ void Context::grid_core(const wsg_args &a, const Staged &s, double *img, bool ac
     ga.pb1 = int(pb0 + npl);
     GridKernels<R>::dispatch(gp.kernel.W, true, num_sms, smem, stream, ga, g, kc);
     CK(cudaEventRecord(ev[3], stream));
-    // pass 1: along v over the band rows (out of place into the full grid)
-    if (gp.band_full) {
-      cufftHandle h = fft_plan(int(nv), 1, int(nv), 1, int(nv), int(nu * P), dbl);
-      fft_exec(h, band, full, dir, dbl);
-    } else {
-      const size_t rowb = P * nv * cs;
-      cufftHandle hlo = fft_plan(int(nv), 1, int(nv), 1, int(nv), int((L + 1) * P), dbl);
-      fft_exec(hlo, band, full, dir, dbl);
-      cufftHandle hhi = fft_plan(int(nv), 1, int(nv), 1, int(nv), int(L * P), dbl);
-      fft_exec(hhi, band + (L + 1) * rowb, full + (nu - L) * rowb, dir, dbl);
-    }
-    // pass 2: along u over the image columns, into H[p][j][u]
+    // transform along v: every (band row, plane) is a contiguous row of nv
     {
-      const int half = int(gp.ny / 2);
-      cufftHandle h2 = fft_plan(int(nu), int(P * nv), 1, 1, int(nu), half, dbl);
-      for (size_t p = 0; p < npl; ++p) {
-        // grid columns [0, ny/2) are image columns [ny/2, ny)
-        fft_exec(h2, full + (p * nv) * cs, H + (p * gp.ny + half) * nu * cs, dir, dbl);
-        // grid columns [nv-ny/2, nv) are image columns [0, ny/2)
-        fft_exec(h2, full + (p * nv + nv - half) * cs, H + (p * gp.ny) * nu * cs, dir, dbl);
-      }
+      cufftHandle h = fft_plan(int(nv), 1, int(nv), 1, int(nv), int(gp.band_rows * P), dbl);
+      fft_exec(h, band, band, dir, dbl);
     }
+    // pruned transform along u: band rows of the image columns -> image rows
+    ColKernels<R>::run(gp.logM, true, ca, int(npl), stream);
     CK(cudaEventRecord(ev[4], stream));
     ScreenArgs sa = make_screen(gp, reinterpret_cast<const double *>(b_cf.p), cc, P);
     sa.pb0 = int(pb0);
@@ -674,7 +779,9 @@ void Context::grid_core(const wsg_args &a, const Staged &s, double *img, bool ac
   stats.ms_grid = t_grid;
   stats.ms_fft = t_fft;
   stats.ms_screen = t_screen;
+  mark("passes-done");
   if (verbosity > 0) print_report(gp, true, P);
+  print_marks("ms2dirty");
 }
 
 template <typename R>
@@ -703,26 +810,15 @@ void Context::degrid_core(const wsg_args &a, const Staged &s, const double *img,
   ChebCorr cc = upload_corrections(gp);
   DevGeom g = make_geom(gp);
   DevKernel<R> kc = make_kernel<R>(gp.poly);
+  mark("corrections");
   const size_t P = choose_planes(gp, false);
+  mark("choose_planes");
   const size_t cs = 2 * sizeof(R);
-  const size_t nv = gp.nv, nu = gp.nu;
+  const size_t nv = gp.nv;
   char *band = reinterpret_cast<char *>(b_band.ensure(gp.band_rows * P * nv * cs));
-  char *full = reinterpret_cast<char *>(b_full_adj.ensure(nu * P * nv * cs));
-  char *H = reinterpret_cast<char *>(b_H.ensure(P * gp.ny * nu * cs));
-  // invariant of the adjoint full grid ([P][nv][nu]): rows v outside the
-  // image columns are zero (never written)
-  Layout lay{nu, nv, P, cs};
-  if (!(lay == adj_layout)) {
-    CK(cudaMemsetAsync(full, 0, nu * P * nv * cs, stream));
-    adj_layout = lay;
-  }
-  // H entries outside the image rows must be zero
-  if (!H_clean || !(lay == H_layout)) {
-    const size_t nxh = gp.nx / 2;
-    CK(cudaMemset2DAsync(H + nxh * cs, nu * cs, 0, (nu - gp.nx) * cs, P * gp.ny, stream));
-    H_clean = true;
-    H_layout = lay;
-  }
+  char *H = reinterpret_cast<char *>(b_H.ensure(P * gp.ny * gp.nx * cs));
+  const void *tw = upload_twiddles(gp, dbl);
+  ColArgs ca = make_col(gp, P, tw, band, H);
   const TileLayout tl = make_layout(gp.T, gp.kernel.W);
   const size_t smem = GridKernels<R>::smem_bytes(tl, gp.kernel.W, false);
   int *counter = reinterpret_cast<int *>(reinterpret_cast<char *>(b_small.p) + 2048);
@@ -743,10 +839,11 @@ void Context::degrid_core(const wsg_args &a, const Staged &s, const double *img,
   ga.vis_out = vis_out;
   ga.vis_double = a.vis_type == WSG_C128;
   const bool multi = P < gp.nplanes;
-  ga.acc = multi ? b_acc.ensure(gp.nvis * cs) : nullptr;
+  const bool need_acc = multi || GridKernels<R>::groups(gp.kernel.W) > 1;
+  ga.acc = need_acc ? b_acc.ensure(gp.nvis * cs) : nullptr;
+  if (need_acc) CK(cudaMemsetAsync(ga.acc, 0, gp.nvis * cs, stream));
 
   const int dir = CUFFT_FORWARD;
-  const size_t L = gp.band_full ? nu / 2 : gp.Lu;
   float t_grid = 0, t_fft = 0, t_screen = 0;
   for (size_t pb0 = 0; pb0 < gp.nplanes; pb0 += P) {
     const size_t npl = std::min(P, gp.nplanes - pb0);
@@ -759,35 +856,14 @@ void Context::degrid_core(const wsg_args &a, const Staged &s, const double *img,
     cuda_check(cudaGetLastError(), "k_screen_put launch");
   g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     CK(cudaEventRecord(ev[3], stream));
-    // pass 2 (transposed): along u, H[p][j][u] -> rows of the adjoint full
-    // grid, laid out [P][nv][nu] so that this pass writes contiguously
+    // pruned transform along u (transposed): image rows -> band rows of the
+    // image columns; the other columns of the band grid stay zero
+    CK(cudaMemsetAsync(band, 0, gp.band_rows * P * nv * cs, stream));
+    ColKernels<R>::run(gp.logM, false, ca, int(npl), stream);
+    // transform along v
     {
-      const int half = int(gp.ny / 2);
-      cufftHandle h2 = fft_plan(int(nu), 1, int(nu), 1, int(nu), half, dbl);
-      for (size_t p = 0; p < npl; ++p) {
-        // image columns [ny/2, ny) are grid columns [0, ny/2)
-        fft_exec(h2, H + (p * gp.ny + half) * nu * cs, full + (p * nv) * nu * cs, dir, dbl);
-        // image columns [0, ny/2) are grid columns [nv-ny/2, nv)
-        fft_exec(h2, H + (p * gp.ny) * nu * cs, full + (p * nv + nv - half) * nu * cs, dir, dbl);
-      }
-    }
-    // pass 1 (transposed): along v (stride nu) for the band rows u, into the
-    // band grid [band_rows][P][nv]
-    {
-      const int pnv = int(P * nv);
-      for (size_t p = 0; p < npl; ++p) {
-        char *src = full + p * nv * nu * cs;
-        char *dst = band + p * nv * cs;
-        if (gp.band_full) {
-          cufftHandle h = fft_plan(int(nv), int(nu), 1, 1, pnv, int(nu), dbl);
-          fft_exec(h, src, dst, dir, dbl);
-        } else {
-          cufftHandle hlo = fft_plan(int(nv), int(nu), 1, 1, pnv, int(L + 1), dbl);
-          fft_exec(hlo, src, dst, dir, dbl);
-          cufftHandle hhi = fft_plan(int(nv), int(nu), 1, 1, pnv, int(L), dbl);
-          fft_exec(hhi, src + (nu - L) * cs, dst + (L + 1) * P * nv * cs, dir, dbl);
-        }
-      }
+      cufftHandle h = fft_plan(int(nv), 1, int(nv), 1, int(nv), int(gp.band_rows * P), dbl);
+      fft_exec(h, band, band, dir, dbl);
     }
     CK(cudaEventRecord(ev[4], stream));
     CK(cudaMemsetAsync(counter, 0, sizeof(int), stream));
@@ -806,6 +882,12 @@ void Context::degrid_core(const wsg_args &a, const Staged &s, const double *img,
     CK(cudaEventElapsedTime(&t, ev[4], ev[5]));
     t_grid += t;
   }
+  if (need_acc) {
+    k_finalize<R><<<launch_blocks(gp.nvis, 256), 256, 0, stream>>>(int(gp.nvis), b_rec.p, ga.acc,
+                                                                  vis_out, ga.vis_double);
+    cuda_check(cudaGetLastError(), "k_finalize launch");
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+  }
   check_device_error(d_err);
   float t_prep;
   CK(cudaEventElapsedTime(&t_prep, ev[0], ev[1]));
@@ -814,7 +896,9 @@ void Context::degrid_core(const wsg_args &a, const Staged &s, const double *img,
   stats.ms_grid = t_grid;
   stats.ms_fft = t_fft;
   stats.ms_screen = t_screen;
+  mark("passes-done");
   if (verbosity > 0) print_report(gp, false, P);
+  print_marks("dirty2ms");
 }
 
 void Context::check_device_error(const int *d_err) {

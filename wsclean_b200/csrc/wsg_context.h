@@ -4,7 +4,9 @@
 #include <cuda_runtime.h>
 #include <cufft.h>
 
+#include <chrono>
 #include <map>
+#include <utility>
 #include <tuple>
 #include <vector>
 
@@ -72,27 +74,30 @@ class Context {
   // buffers
   DevBuf b_uvw, b_fovc, b_vis, b_wgt, b_mask;
   DevBuf b_keys_a, b_keys_b, b_vals_a, b_vals_b, b_cub, b_rec, b_chunks, b_small;
-  DevBuf b_band, b_full_fwd, b_full_adj, b_H;
-  DevBuf b_img, b_img2, b_acc, b_cf, b_fftwork, b_out;
+  DevBuf b_band, b_H;
+  DevBuf b_img, b_img2, b_acc, b_cf, b_tw, b_fftwork, b_out;
 
  private:
   std::vector<DevBuf *> all_buffers();
   template <typename R>
   bool prepare(const wsg_args &a, const Staged &s, bool gridding, void *vis_out_dev, GridPlan &gp);
   ChebCorr upload_corrections(const GridPlan &g);
+  const void *upload_twiddles(const GridPlan &g, bool dbl);
   size_t choose_planes(const GridPlan &g, bool gridding);
   cufftHandle fft_plan(int n, int istride, int idist, int ostride, int odist, int batch, bool dbl);
   void fft_exec(cufftHandle h, void *in, void *out, int dir, bool dbl);
   void record_stats(const GridPlan &g, bool gridding, size_t P);
   void check_device_error(const int *d_err);
   void print_report(const GridPlan &g, bool gridding, size_t P);
+  void mark(const char *what);
+  void print_marks(const char *title);
+  std::vector<std::pair<const char *, std::chrono::steady_clock::time_point>> marks;
 
   cudaEvent_t ev[8];
   std::map<std::tuple<int, int, int, int, int, int, int>, cufftHandle> fft_plans;
   size_t fft_work_need = 0;
-  Layout fwd_layout, adj_layout, H_layout;
-  size_t fwd_L = 0;
-  bool H_clean = false;
+  std::tuple<size_t, size_t, int> tw_key;
+  bool tw_valid = false;
   // correction-table cache
   std::tuple<int, double, double, size_t, size_t, size_t, size_t, double> corr_key;
   ChebCorr corr_cc;

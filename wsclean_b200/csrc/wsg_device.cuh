@@ -337,216 +337,149 @@ __device__ __forceinline__ int band_index(const DevGeom &g, int u) {
   return -1;
 }
 
+// ------------------------------------------------- per-warp record staging
+//
+// A warp works through its slice of a chunk 32 records at a time: lane l
+// loads record l of the batch (coalesced), evaluates its 3W kernel values --
+// W pieces per axis by Horner's rule of fixed degree W+4 with the
+// coefficients as compile-time constant-bank operands (the host pads
+// lower-degree fits with zero leading coefficients) -- and stages them in a
+// per-warp shared-memory block; the warp then consumes the batch record by
+// record with broadcast reads.
+template <int W> struct KDeg { static constexpr int value = W + 4; };
+template <typename R, int W> struct KStride {
+  // row of 3W values, padded to a 16-byte multiple
+  static constexpr int value = sizeof(R) == 4 ? ((3 * W + 3) & ~3) : ((3 * W + 1) & ~1);
+};
+template <typename R, int W> struct WarpStage {
+  static constexpr int KST = KStride<R, W>::value;
+  static constexpr size_t bytes = sizeof(R) * (32 * KST + 64) + 128;  // kv, (vr,vi), luv
+};
+
+template <int W, typename R>
+__device__ __forceinline__ void eval_const(const DevKernel<R> &k, R x, R *out) {
+  constexpr int DEG = KDeg<W>::value;
+#pragma unroll
+  for (int i = 0; i < W; ++i) {
+    R v = k.c[DEG][i];
+#pragma unroll
+    for (int j = DEG - 1; j >= 0; --j) v = fma(v, x, k.c[j][i]);
+    out[i] = v;
+  }
+}
+
+// Stages records [b0, b0+nb) of the warp's slice; returns via luv the packed
+// in-tile origin (or kSkip).  Lanes >= nb do nothing.
+template <typename R, int W, typename Rec>
+__device__ __forceinline__ void stage_batch(const Rec *recs, int b0, int nb, int lane, int tu,
+                                            int tv, int mp, const DevGeom &g,
+                                            const DevKernel<R> &kc, R *kv, R *vv, uint32_t *luv,
+                                            int *err, int &bb0, int &bb1, int &bb2, int &bb3) {
+  constexpr int KST = KStride<R, W>::value;
+  if (lane < nb) {
+    const Rec rr = recs[b0 + lane];
+    const int lu = int(rr.iuv >> 16) - tu * g.T;
+    const int lv = int(rr.iuv & 0xffffu) - tv * g.T;
+    if (lu < 0 || lu >= g.T || lv < 0 || lv >= g.T || int(rr.mp) != mp) {
+      atomicOr(err, 1);
+      luv[lane] = kSkip;
+    } else {
+      luv[lane] = (uint32_t(lu) << 16) | uint32_t(lv);
+      bb0 = min(bb0, lu); bb1 = max(bb1, lu);
+      bb2 = min(bb2, lv); bb3 = max(bb3, lv);
+      R vals[W];
+      R *row = kv + lane * KST;
+      eval_const<W>(kc, rr.xu, vals);
+#pragma unroll
+      for (int i = 0; i < W; ++i) row[i] = vals[i];
+      eval_const<W>(kc, rr.xv, vals);
+#pragma unroll
+      for (int i = 0; i < W; ++i) row[W + i] = vals[i];
+      if (g.do_w) {
+        eval_const<W>(kc, rr.xw, vals);
+#pragma unroll
+        for (int i = 0; i < W; ++i) row[2 * W + i] = vals[i];
+      } else {
+#pragma unroll
+        for (int i = 0; i < W; ++i) row[2 * W + i] = R(i == 0);
+      }
+      vv[2 * lane] = rr.vr;
+      vv[2 * lane + 1] = rr.vi;
+    }
+  }
+}
+
+__device__ __forceinline__ void warp_minmax(int &bb0, int &bb1, int &bb2, int &bb3) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    bb0 = min(bb0, __shfl_xor_sync(0xffffffffu, bb0, o));
+    bb1 = max(bb1, __shfl_xor_sync(0xffffffffu, bb1, o));
+    bb2 = min(bb2, __shfl_xor_sync(0xffffffffu, bb2, o));
+    bb3 = max(bb3, __shfl_xor_sync(0xffffffffu, bb3, o));
+  }
+}
+
 // ------------------------------------------------------------- k_spread
 //
-// One CTA drains chunks; all records of a chunk share one (tile, minplane)
-// bin, so the CTA owns a W-plane shared-memory tile (structure of arrays:
-// real parts then imaginary parts) for the chunk.  Warps take contiguous
-// slices of each sub-batch; lane q of a warp owns PPL (plane, u-row) pairs of
-// the footprint and W cells along v for each, accumulating in registers while
-// consecutive records share the footprint origin.
+// Persistent CTAs drain chunks; all records of a chunk share one
+// (tile, minplane) bin, so the CTA owns a W-plane shared-memory tile
+// (structure of arrays: real parts, then imaginary parts) for the chunk.  Each
+// warp takes a contiguous slice of the chunk; lane q owns PPL (plane, u-row)
+// pairs of the footprint and the W cells along v of each, accumulating in
+// registers while consecutive records share the footprint origin (records are
+// sorted by position inside the tile), then commits with shared-memory
+// atomics.  At the end of the chunk the touched region is added to the u-band
+// grid with vector atomics.
+// Atomically reads a shared-memory cell and leaves zero in it.
+__device__ __forceinline__ float take_zero(float *p) { return atomicExch(p, 0.0f); }
+__device__ __forceinline__ double take_zero(double *p) {
+  return __longlong_as_double(
+      (long long)atomicExch(reinterpret_cast<unsigned long long *>(p), 0ull));
+}
+
+// Chunks touching few distinct footprint origins are flushed / staged
+// footprint by footprint instead of over their bounding box.
+constexpr int kMaxOrig = 64;
+
 template <typename R, int W, int PPL, int NWARP>
 __global__ void __launch_bounds__(NWARP * 32)
 k_spread(GridArgs a, DevGeom g, DevKernel<R> kc) {
   using Rec = typename RecOf<R>::type;
+  using C = typename Cplx<R>::type;
   constexpr int NG = (W * W + 32 * PPL - 1) / (32 * PPL);  // warps per record
   constexpr int NSL = NWARP / NG;                          // record slices
-  constexpr int KST = 3 * W + 1;                           // kernel values per record
+  constexpr int KST = KStride<R, W>::value;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const TileLayout tl = a.tl;
   R *tre = reinterpret_cast<R *>(smem_raw);
   R *tim = tre + W * tl.PS;
-  R *kv_s = tim + W * tl.PS;             // [sb][KST]
-  R *vv_s = kv_s + a.sb * KST;           // [sb][2]
-  uint32_t *luv_s = reinterpret_cast<uint32_t *>(vv_s + 2 * a.sb);  // [sb]
-  __shared__ int sh_chunk, sh_bb[4];
+  __shared__ int sh_chunk, sh_bb[4], sh_norig;
+  __shared__ uint32_t sh_orig[kMaxOrig];
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int grp = warp % NG, slice = warp / NG;
+  unsigned char *wbase = smem_raw + size_t(2 * W * tl.PS) * sizeof(R) + warp * WarpStage<R, W>::bytes;
+  R *kv = reinterpret_cast<R *>(wbase);
+  R *vv = kv + 32 * KST;
+  uint32_t *luvs = reinterpret_cast<uint32_t *>(vv + 64);
   const Rec *recs = reinterpret_cast<const Rec *>(a.rec);
-  using C = typename Cplx<R>::type;
   C *grid = reinterpret_cast<C *>(a.grid);
 
   for (int i = tid; i < 2 * W * tl.PS; i += blockDim.x) tre[i] = R(0);
-  __syncthreads();
-
-  for (;;) {
-    if (tid == 0) {
-      sh_chunk = atomicAdd(a.counter, 1);
-      sh_bb[0] = 1 << 30; sh_bb[1] = -1; sh_bb[2] = 1 << 30; sh_bb[3] = -1;
-    }
-    __syncthreads();
-    const int ch = sh_chunk;
-    if (ch >= *a.nchunks) break;
-    const int s0 = a.chunk_start[ch];
-    const int s1 = (ch + 1 < *a.nchunks) ? a.chunk_start[ch + 1] : a.nvis;
-    const Rec r0 = recs[s0];
-    const int a0 = int(r0.iuv >> 16), b0 = int(r0.iuv & 0xffffu);
-    const int tu = a0 / g.T, tv = b0 / g.T;
-    const int mp = int(r0.mp);
-    const bool any_plane = (mp < a.pb1) && (mp + W > a.pb0);
-
-    if (any_plane) {
-      for (int sb0 = s0; sb0 < s1; sb0 += a.sb) {
-        const int n = min(a.sb, s1 - sb0);
-        // kernel values: one (record, axis) per thread
-        for (int t = tid; t < 3 * n; t += blockDim.x) {
-          const int j = t / 3, ax = t - 3 * j;
-          const Rec rr = recs[sb0 + j];
-          R vals[W];
-          R x = ax == 0 ? rr.xu : (ax == 1 ? rr.xv : rr.xw);
-          if (ax < 2 || g.do_w) {
-            eval_pieces<W, R>(kc, x, vals);
-          } else {
+  int pp[PPL], cu[PPL];
 #pragma unroll
-            for (int i = 0; i < W; ++i) vals[i] = R(i == 0);
-          }
-#pragma unroll
-          for (int i = 0; i < W; ++i) kv_s[j * KST + ax * W + i] = vals[i];
-          if (ax == 0) {
-            vv_s[2 * j] = rr.vr;
-            vv_s[2 * j + 1] = rr.vi;
-            const int lu = int(rr.iuv >> 16) - tu * g.T;
-            const int lv = int(rr.iuv & 0xffffu) - tv * g.T;
-            if (lu < 0 || lu >= g.T || lv < 0 || lv >= g.T || int(rr.mp) != mp) {
-              atomicOr(a.err, 1);
-              luv_s[j] = kSkip;
-            } else {
-              luv_s[j] = (uint32_t(lu) << 16) | uint32_t(lv);
-              atomicMin(&sh_bb[0], lu); atomicMax(&sh_bb[1], lu);
-              atomicMin(&sh_bb[2], lv); atomicMax(&sh_bb[3], lv);
-            }
-          }
-        }
-        __syncthreads();
-        if (slice < NSL) {
-          const int j0 = (n * slice) / NSL, j1 = (n * (slice + 1)) / NSL;
-          R accr[PPL][W], acci[PPL][W];
-          int pp[PPL], cu[PPL];
-          bool ok[PPL];
-#pragma unroll
-          for (int k = 0; k < PPL; ++k) {
-            const int q = grp * 32 * PPL + lane + 32 * k;
-            pp[k] = q / W;
-            cu[k] = q - pp[k] * W;
-            ok[k] = (q < W * W) && (mp + pp[k] >= a.pb0) && (mp + pp[k] < a.pb1);
-#pragma unroll
-            for (int c = 0; c < W; ++c) accr[k][c] = acci[k][c] = R(0);
-          }
-          uint32_t cur = 0xffffffffu;
-          auto commit = [&]() {
-            if (cur == 0xffffffffu) return;
-            const int lu = int(cur >> 16), lv = int(cur & 0xffffu);
-#pragma unroll
-            for (int k = 0; k < PPL; ++k) {
-              if (!ok[k]) continue;
-              const int base = pp[k] * tl.PS + (lu + cu[k]) * tl.RS + lv;
-#pragma unroll
-              for (int c = 0; c < W; ++c) {
-                atomicAdd(&tre[base + c], accr[k][c]);
-                atomicAdd(&tim[base + c], acci[k][c]);
-                accr[k][c] = acci[k][c] = R(0);
-              }
-            }
-          };
-          for (int j = j0; j < j1; ++j) {
-            const uint32_t luv = luv_s[j];
-            if (luv == kSkip) continue;
-            if (luv != cur) {
-              commit();
-              cur = luv;
-            }
-            const R vr = vv_s[2 * j], vi = vv_s[2 * j + 1];
-            const R *kj = kv_s + j * KST;
-            R kvv[W];
-#pragma unroll
-            for (int c = 0; c < W; ++c) kvv[c] = kj[W + c];
-#pragma unroll
-            for (int k = 0; k < PPL; ++k) {
-              const int pk = ok[k] ? pp[k] : 0, ck = ok[k] ? cu[k] : 0;
-              const R f = kj[2 * W + pk] * kj[ck];
-              const R ar = vr * f, ai = vi * f;
-#pragma unroll
-              for (int c = 0; c < W; ++c) {
-                accr[k][c] = fma(ar, kvv[c], accr[k][c]);
-                acci[k][c] = fma(ai, kvv[c], acci[k][c]);
-              }
-            }
-          }
-          commit();
-        }
-        __syncthreads();
-      }
-      // flush the touched region of the tile to the band grid
-      const int lu0 = sh_bb[0], lu1 = sh_bb[1] + W, lv0 = sh_bb[2], lv1 = sh_bb[3] + W;
-      const int nbu = max(lu1 - lu0, 0), nbv = max(lv1 - lv0, 0);
-      const int ucorner = tu * g.T - g.nsafe, vcorner = tv * g.T - g.nsafe;
-      const int ncell = W * nbu * nbv;
-      for (int t = tid; t < ncell; t += blockDim.x) {
-        const int p = t / (nbu * nbv);
-        const int rem = t - p * nbu * nbv;
-        const int ia = lu0 + rem / nbv, ib = lv0 + rem % nbv;
-        const int sidx = p * tl.PS + ia * tl.RS + ib;
-        const R xr = tre[sidx], xi = tim[sidx];
-        const int plane = mp + p;
-        if ((xr != R(0) || xi != R(0)) && plane >= a.pb0 && plane < a.pb1) {
-          int u = ucorner + ia;
-          u += (u < 0) ? g.nu : 0;
-          u -= (u >= g.nu) ? g.nu : 0;
-          int v = vcorner + ib;
-          v += (v < 0) ? g.nv : 0;
-          v -= (v >= g.nv) ? g.nv : 0;
-          const int bi = band_index(g, u);
-          if (bi >= 0) {
-            C *dst = grid + (size_t(bi) * a.P + (plane - a.pb0)) * size_t(g.nv) + v;
-            if constexpr (sizeof(R) == 4) {
-              atomicAdd(reinterpret_cast<float2 *>(dst), make_float2(xr, xi));
-            } else {
-              atomicAdd(&dst->x, xr);
-              atomicAdd(&dst->y, xi);
-            }
-          }
-        }
-        tre[sidx] = R(0);
-        tim[sidx] = R(0);
-      }
-    }
-    __syncthreads();
+  for (int k = 0; k < PPL; ++k) {
+    const int q = grp * 32 * PPL + lane + 32 * k;
+    pp[k] = q / W;
+    cu[k] = q - pp[k] * W;
   }
-}
-
-// ------------------------------------------------------------- k_interp
-//
-// Degridding, the exact transpose of k_spread: the chunk's tile region is
-// staged from the band grid into shared memory, each lane caches its
-// (plane, u-row) x W cells in registers while the footprint origin repeats,
-// and the kernel-weighted sum is reduced across the warp.
-template <typename R, int W, int PPL, int NWARP>
-__global__ void __launch_bounds__(NWARP * 32)
-k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
-  using Rec = typename RecOf<R>::type;
-  using C = typename Cplx<R>::type;
-  constexpr int NG = (W * W + 32 * PPL - 1) / (32 * PPL);
-  constexpr int NSL = NWARP / NG;
-  constexpr int KST = 3 * W + 1;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const TileLayout tl = a.tl;
-  R *tre = reinterpret_cast<R *>(smem_raw);
-  R *tim = tre + W * tl.PS;
-  R *kv_s = tim + W * tl.PS;
-  R *res_s = kv_s + a.sb * KST;                                     // [sb][2]
-  uint32_t *luv_s = reinterpret_cast<uint32_t *>(res_s + 2 * a.sb);  // [sb]
-  __shared__ int sh_chunk, sh_bb[4];
-
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int grp = warp % NG, slice = warp / NG;
-  const Rec *recs = reinterpret_cast<const Rec *>(a.rec);
-  const C *grid = reinterpret_cast<const C *>(a.grid);
 
   for (;;) {
+    __syncthreads();
     if (tid == 0) {
       sh_chunk = atomicAdd(a.counter, 1);
       sh_bb[0] = 1 << 30; sh_bb[1] = -1; sh_bb[2] = 1 << 30; sh_bb[3] = -1;
+      sh_norig = 0;
     }
     __syncthreads();
     const int ch = sh_chunk;
@@ -556,29 +489,118 @@ k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
     const Rec r0 = recs[s0];
     const int tu = int(r0.iuv >> 16) / g.T, tv = int(r0.iuv & 0xffffu) / g.T;
     const int mp = int(r0.mp);
-    const bool any_plane = (mp < a.pb1) && (mp + W > a.pb0);
-    // bounding box of the chunk's footprints
-    for (int s = s0 + tid; s < s1; s += blockDim.x) {
-      const uint32_t iuv = recs[s].iuv;
-      const int lu = int(iuv >> 16) - tu * g.T, lv = int(iuv & 0xffffu) - tv * g.T;
-      if (lu < 0 || lu >= g.T || lv < 0 || lv >= g.T) continue;
-      atomicMin(&sh_bb[0], lu); atomicMax(&sh_bb[1], lu);
-      atomicMin(&sh_bb[2], lv); atomicMax(&sh_bb[3], lv);
+    if (!((mp < a.pb1) && (mp + W > a.pb0))) continue;
+
+    if (slice < NSL) {
+      const int n = s1 - s0;
+      const int j0 = s0 + (n * slice) / NSL, j1 = s0 + (n * (slice + 1)) / NSL;
+      bool ok[PPL];
+#pragma unroll
+      for (int k = 0; k < PPL; ++k)
+        ok[k] = (pp[k] < W) && (mp + pp[k] >= a.pb0) && (mp + pp[k] < a.pb1);
+      R accr[PPL][W], acci[PPL][W];
+#pragma unroll
+      for (int k = 0; k < PPL; ++k)
+#pragma unroll
+        for (int c = 0; c < W; ++c) accr[k][c] = acci[k][c] = R(0);
+      uint32_t cur = 0xffffffffu;
+      int bb0 = 1 << 30, bb1 = -1, bb2 = 1 << 30, bb3 = -1;
+      auto commit = [&]() {
+        if (cur == 0xffffffffu) return;
+        const int lu = int(cur >> 16), lv = int(cur & 0xffffu);
+#pragma unroll
+        for (int k = 0; k < PPL; ++k) {
+          if (!ok[k]) continue;
+          const int base = pp[k] * tl.PS + (lu + cu[k]) * tl.RS + lv;
+#pragma unroll
+          for (int c = 0; c < W; ++c) {
+            atomicAdd(&tre[base + c], accr[k][c]);
+            atomicAdd(&tim[base + c], acci[k][c]);
+            accr[k][c] = acci[k][c] = R(0);
+          }
+        }
+      };
+      for (int b0 = j0; b0 < j1; b0 += 32) {
+        const int nb = min(32, j1 - b0);
+        stage_batch<R, W>(recs, b0, nb, lane, tu, tv, mp, g, kc, kv, vv, luvs, a.err, bb0, bb1,
+                          bb2, bb3);
+        __syncwarp();
+        for (int jj = 0; jj < nb; ++jj) {
+          const uint32_t luv = luvs[jj];
+          if (luv == kSkip) continue;
+          if (luv != cur) {
+            commit();
+            cur = luv;
+            if (lane == 0 && grp == 0) {
+              const int k = atomicAdd(&sh_norig, 1);
+              if (k < kMaxOrig) sh_orig[k] = luv;
+            }
+          }
+          const R *kb = kv + jj * KST;
+          R kvv[W];
+#pragma unroll
+          for (int c = 0; c < W; ++c) kvv[c] = kb[W + c];
+          const R vr = vv[2 * jj], vi = vv[2 * jj + 1];
+#pragma unroll
+          for (int k = 0; k < PPL; ++k) {
+            const R f = kb[2 * W + (ok[k] ? pp[k] : 0)] * kb[ok[k] ? cu[k] : 0];
+            const R ar = vr * f, ai = vi * f;
+#pragma unroll
+            for (int c = 0; c < W; ++c) {
+              accr[k][c] = fma(ar, kvv[c], accr[k][c]);
+              acci[k][c] = fma(ai, kvv[c], acci[k][c]);
+            }
+          }
+        }
+        __syncwarp();
+      }
+      commit();
+      warp_minmax(bb0, bb1, bb2, bb3);
+      if (lane == 0 && bb1 >= 0) {
+        atomicMin(&sh_bb[0], bb0); atomicMax(&sh_bb[1], bb1);
+        atomicMin(&sh_bb[2], bb2); atomicMax(&sh_bb[3], bb3);
+      }
     }
     __syncthreads();
+    // flush the touched cells of the tile to the band grid: footprint by
+    // footprint when few origins were used (a cell shared by two footprints
+    // is taken by atomic exchange, so it is added once), else the bounding box
     const int lu0 = sh_bb[0], lv0 = sh_bb[2];
     const int nbu = max(sh_bb[1] + W - lu0, 0), nbv = max(sh_bb[3] + W - lv0, 0);
     const int ucorner = tu * g.T - g.nsafe, vcorner = tv * g.T - g.nsafe;
-    const int ncell = W * nbu * nbv;
-    for (int t = tid; t < ncell; t += blockDim.x) {
-      const int p = t / (nbu * nbv);
-      const int rem = t - p * nbu * nbv;
-      const int ia = lu0 + rem / nbv, ib = lv0 + rem % nbv;
+    const int norig = sh_norig;
+    const bool by_list = norig <= kMaxOrig && norig * W * W < nbu * nbv;
+    // one (plane, row) line per warp-iteration, lanes along v (no divisions)
+    const int nline = by_list ? norig * W * W : W * nbu;
+    const int linelen = by_list ? W : nbv;
+    for (int line = warp; line < nline; line += NWARP) {
+      int p, ia, ib0;
+      if (by_list) {
+        const int o = line / (W * W), pr = line - o * W * W;
+        p = pr / W;
+        const uint32_t luv = sh_orig[o];
+        ia = int(luv >> 16) + (pr - p * W);
+        ib0 = int(luv & 0xffffu);
+      } else {
+        p = line / nbu;
+        ia = lu0 + (line - p * nbu);
+        ib0 = lv0;
+      }
+      for (int c = lane; c < linelen; c += 32) {
+      const int ib = ib0 + c;
+      const int sidx = p * tl.PS + ia * tl.RS + ib;
+      R xr, xi;
+      if (by_list) {
+        xr = take_zero(&tre[sidx]);
+        xi = take_zero(&tim[sidx]);
+      } else {
+        xr = tre[sidx];
+        xi = tim[sidx];
+        tre[sidx] = R(0);
+        tim[sidx] = R(0);
+      }
       const int plane = mp + p;
-      C val;
-      val.x = R(0);
-      val.y = R(0);
-      if (any_plane && plane >= a.pb0 && plane < a.pb1) {
+      if ((xr != R(0) || xi != R(0)) && plane >= a.pb0 && plane < a.pb1) {
         int u = ucorner + ia;
         u += (u < 0) ? g.nu : 0;
         u -= (u >= g.nu) ? g.nu : 0;
@@ -586,58 +608,165 @@ k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
         v += (v < 0) ? g.nv : 0;
         v -= (v >= g.nv) ? g.nv : 0;
         const int bi = band_index(g, u);
-        if (bi >= 0) val = grid[(size_t(bi) * a.P + (plane - a.pb0)) * size_t(g.nv) + v];
-      }
-      const int sidx = p * tl.PS + ia * tl.RS + ib;
-      tre[sidx] = val.x;
-      tim[sidx] = val.y;
-    }
-    __syncthreads();
-
-    for (int sb0 = s0; sb0 < s1; sb0 += a.sb) {
-      const int n = min(a.sb, s1 - sb0);
-      for (int t = tid; t < 3 * n; t += blockDim.x) {
-        const int j = t / 3, ax = t - 3 * j;
-        const Rec rr = recs[sb0 + j];
-        R vals[W];
-        R x = ax == 0 ? rr.xu : (ax == 1 ? rr.xv : rr.xw);
-        if (ax < 2 || g.do_w) {
-          eval_pieces<W, R>(kc, x, vals);
-        } else {
-#pragma unroll
-          for (int i = 0; i < W; ++i) vals[i] = R(i == 0);
-        }
-#pragma unroll
-        for (int i = 0; i < W; ++i) kv_s[j * KST + ax * W + i] = vals[i];
-        if (ax == 0) {
-          res_s[2 * j] = R(0);
-          res_s[2 * j + 1] = R(0);
-          const int lu = int(rr.iuv >> 16) - tu * g.T;
-          const int lv = int(rr.iuv & 0xffffu) - tv * g.T;
-          if (lu < 0 || lu >= g.T || lv < 0 || lv >= g.T || int(rr.mp) != mp) {
-            atomicOr(a.err, 1);
-            luv_s[j] = kSkip;
+        if (bi >= 0) {
+          C *dst = grid + (size_t(bi) * a.P + (plane - a.pb0)) * size_t(g.nv) + v;
+          if constexpr (sizeof(R) == 4) {
+            atomicAdd(reinterpret_cast<float2 *>(dst), make_float2(xr, xi));
           } else {
-            luv_s[j] = (uint32_t(lu) << 16) | uint32_t(lv);
+            atomicAdd(&dst->x, xr);
+            atomicAdd(&dst->y, xi);
           }
         }
       }
-      __syncthreads();
-      if (slice < NSL && any_plane) {
-        const int j0 = (n * slice) / NSL, j1 = (n * (slice + 1)) / NSL;
-        R cr[PPL][W], ci[PPL][W];
-        int pp[PPL], cu[PPL];
-        bool ok[PPL];
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------- k_interp
+//
+// Degridding, the exact transpose of k_spread: the chunk's tile region is
+// staged from the band grid into shared memory, each lane caches its
+// (plane, u-row) x W cells in registers while the footprint origin repeats,
+// and the kernel-weighted sum is reduced across the warp.  With one warp per
+// record and a single plane pass the result is finalised in place
+// (conjugation, conjugate shift phasor and weight); otherwise partial sums
+// go to a per-record accumulator finalised by k_finalize.
+template <typename R, int W, int PPL, int NWARP>
+__global__ void __launch_bounds__(NWARP * 32)
+k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
+  using Rec = typename RecOf<R>::type;
+  using C = typename Cplx<R>::type;
+  constexpr int NG = (W * W + 32 * PPL - 1) / (32 * PPL);
+  constexpr int NSL = NWARP / NG;
+  constexpr int KST = KStride<R, W>::value;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const TileLayout tl = a.tl;
+  R *tre = reinterpret_cast<R *>(smem_raw);
+  R *tim = tre + W * tl.PS;
+  __shared__ int sh_chunk, sh_bb[4], sh_norig;
+  __shared__ uint32_t sh_orig[kMaxOrig];
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int grp = warp % NG, slice = warp / NG;
+  unsigned char *wbase = smem_raw + size_t(2 * W * tl.PS) * sizeof(R) + warp * WarpStage<R, W>::bytes;
+  R *kv = reinterpret_cast<R *>(wbase);
+  R *vv = kv + 32 * KST;
+  uint32_t *luvs = reinterpret_cast<uint32_t *>(vv + 64);
+  const Rec *recs = reinterpret_cast<const Rec *>(a.rec);
+  const C *grid = reinterpret_cast<const C *>(a.grid);
+  const bool direct = a.last_pass && a.first_pass && NG == 1;
+
+  int pp[PPL], cu[PPL];
+  bool ok[PPL];
 #pragma unroll
-        for (int k = 0; k < PPL; ++k) {
-          const int q = grp * 32 * PPL + lane + 32 * k;
-          pp[k] = q / W;
-          cu[k] = q - pp[k] * W;
-          ok[k] = (q < W * W);
+  for (int k = 0; k < PPL; ++k) {
+    const int q = grp * 32 * PPL + lane + 32 * k;
+    pp[k] = q / W;
+    cu[k] = q - pp[k] * W;
+    ok[k] = q < W * W;
+  }
+
+  for (;;) {
+    __syncthreads();
+    if (tid == 0) {
+      sh_chunk = atomicAdd(a.counter, 1);
+      sh_bb[0] = 1 << 30; sh_bb[1] = -1; sh_bb[2] = 1 << 30; sh_bb[3] = -1;
+      sh_norig = 0;
+    }
+    __syncthreads();
+    const int ch = sh_chunk;
+    if (ch >= *a.nchunks) break;
+    const int s0 = a.chunk_start[ch];
+    const int s1 = (ch + 1 < *a.nchunks) ? a.chunk_start[ch + 1] : a.nvis;
+    const Rec r0 = recs[s0];
+    const int tu = int(r0.iuv >> 16) / g.T, tv = int(r0.iuv & 0xffffu) / g.T;
+    const int mp = int(r0.mp);
+    if (!((mp < a.pb1) && (mp + W > a.pb0))) continue;  // contributes nothing this pass
+    // bounding box and distinct footprint origins of the chunk
+    for (int s = s0 + tid; s < s1; s += blockDim.x) {
+      const uint32_t iuv = recs[s].iuv;
+      const int lu = int(iuv >> 16) - tu * g.T, lv = int(iuv & 0xffffu) - tv * g.T;
+      if (lu < 0 || lu >= g.T || lv < 0 || lv >= g.T) continue;
+      atomicMin(&sh_bb[0], lu); atomicMax(&sh_bb[1], lu);
+      atomicMin(&sh_bb[2], lv); atomicMax(&sh_bb[3], lv);
+      if (s == s0 || recs[s - 1].iuv != iuv) {
+        const int k = atomicAdd(&sh_norig, 1);
+        if (k < kMaxOrig) sh_orig[k] = (uint32_t(lu) << 16) | uint32_t(lv);
+      }
+    }
+    __syncthreads();
+    {
+      // stage the cells the chunk reads: footprint by footprint when few
+      // origins are used (cells shared by footprints are written twice with
+      // the same value), else the bounding box; four loads in flight
+      const int lu0 = sh_bb[0], lv0 = sh_bb[2];
+      const int nbu = max(sh_bb[1] + W - lu0, 0), nbv = max(sh_bb[3] + W - lv0, 0);
+      const int ucorner = tu * g.T - g.nsafe, vcorner = tv * g.T - g.nsafe;
+      const int norig = sh_norig;
+      const bool by_list = norig <= kMaxOrig && norig * W * W < nbu * nbv;
+      // (plane, row) lines over warps, lanes along v, four lines in flight
+      const int nline = by_list ? norig * W * W : W * nbu;
+      const int linelen = by_list ? W : nbv;
+      for (int l0 = warp; l0 < nline; l0 += 4 * NWARP) {
+        C val[4];
+        int sidx[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int line = l0 + q * NWARP;
+          val[q].x = R(0);
+          val[q].y = R(0);
+          sidx[q] = -1;
+          if (line < nline && lane < linelen) {
+            int p, ia, ib;
+            if (by_list) {
+              const int o = line / (W * W), pr = line - o * W * W;
+              p = pr / W;
+              const uint32_t luv = sh_orig[o];
+              ia = int(luv >> 16) + (pr - p * W);
+              ib = int(luv & 0xffffu) + lane;
+            } else {
+              p = line / nbu;
+              ia = lu0 + (line - p * nbu);
+              ib = lv0 + lane;
+            }
+            sidx[q] = p * tl.PS + ia * tl.RS + ib;
+            const int plane = mp + p;
+            if (plane >= a.pb0 && plane < a.pb1) {
+              int u = ucorner + ia;
+              u += (u < 0) ? g.nu : 0;
+              u -= (u >= g.nu) ? g.nu : 0;
+              int v = vcorner + ib;
+              v += (v < 0) ? g.nv : 0;
+              v -= (v >= g.nv) ? g.nv : 0;
+              const int bi = band_index(g, u);
+              if (bi >= 0) val[q] = grid[(size_t(bi) * a.P + (plane - a.pb0)) * size_t(g.nv) + v];
+            }
+          }
         }
-        uint32_t cur = 0xffffffffu;
-        for (int j = j0; j < j1; ++j) {
-          const uint32_t luv = luv_s[j];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          if (sidx[q] >= 0) {
+            tre[sidx[q]] = val[q].x;
+            tim[sidx[q]] = val[q].y;
+          }
+        }
+      }
+    }
+    __syncthreads();
+    if (slice < NSL) {
+      const int n = s1 - s0;
+      const int j0 = s0 + (n * slice) / NSL, j1 = s0 + (n * (slice + 1)) / NSL;
+      R cr[PPL][W], ci[PPL][W];
+      uint32_t cur = 0xffffffffu;
+      int bb0 = 0, bb1 = 0, bb2 = 0, bb3 = 0;
+      for (int b0 = j0; b0 < j1; b0 += 32) {
+        const int nb = min(32, j1 - b0);
+        stage_batch<R, W>(recs, b0, nb, lane, tu, tv, mp, g, kc, kv, vv, luvs, a.err, bb0, bb1,
+                          bb2, bb3);
+        __syncwarp();
+        for (int jj = 0; jj < nb; ++jj) {
+          const uint32_t luv = luvs[jj];
           if (luv == kSkip) continue;
           if (luv != cur) {
             cur = luv;
@@ -652,10 +781,10 @@ k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
               }
             }
           }
-          const R *kj = kv_s + j * KST;
+          const R *kb = kv + jj * KST;
           R kvv[W];
 #pragma unroll
-          for (int c = 0; c < W; ++c) kvv[c] = kj[W + c];
+          for (int c = 0; c < W; ++c) kvv[c] = kb[W + c];
           R sr = R(0), si = R(0);
 #pragma unroll
           for (int k = 0; k < PPL; ++k) {
@@ -665,53 +794,389 @@ k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
               tr = fma(cr[k][c], kvv[c], tr);
               ti = fma(ci[k][c], kvv[c], ti);
             }
-            const int pk = ok[k] ? pp[k] : 0, ck = ok[k] ? cu[k] : 0;
-            const R f = ok[k] ? kj[2 * W + pk] * kj[ck] : R(0);
+            const R f = ok[k] ? kb[2 * W + pp[k]] * kb[cu[k]] : R(0);
             sr = fma(tr, f, sr);
             si = fma(ti, f, si);
           }
           sr = warp_sum(sr);
           si = warp_sum(si);
           if (lane == 0) {
-            if (NG == 1) {
-              res_s[2 * j] = sr;
-              res_s[2 * j + 1] = si;
+            const int s = b0 + jj;
+            if (direct) {
+              const Rec rr = recs[s];
+              const uint32_t idx = rr.idx & 0x7fffffffu;
+              if (rr.idx & 0x80000000u) si = -si;
+              const double orr = double(rr.vr) * double(sr) - double(rr.vi) * double(si);
+              const double oi = double(rr.vr) * double(si) + double(rr.vi) * double(sr);
+              if (a.vis_double)
+                reinterpret_cast<double2 *>(a.vis_out)[idx] = make_double2(orr, oi);
+              else
+                reinterpret_cast<float2 *>(a.vis_out)[idx] = make_float2(float(orr), float(oi));
             } else {
-              atomicAdd(&res_s[2 * j], sr);
-              atomicAdd(&res_s[2 * j + 1], si);
+              C *accp = reinterpret_cast<C *>(a.acc) + s;
+              atomicAdd(&accp->x, sr);
+              atomicAdd(&accp->y, si);
             }
           }
         }
+        __syncwarp();
+      }
+    }
+  }
+}
+
+// Finalises degridded visibilities accumulated over plane passes or warp
+// groups: out[idx] = P * (flip ? conj(acc) : acc).
+template <typename R>
+__global__ void k_finalize(int nvis, const void *recv, const void *accv, void *vis_out,
+                           int vis_double) {
+  using Rec = typename RecOf<R>::type;
+  using C = typename Cplx<R>::type;
+  const Rec *recs = reinterpret_cast<const Rec *>(recv);
+  const C *acc = reinterpret_cast<const C *>(accv);
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nvis; s += gridDim.x * blockDim.x) {
+    const Rec rr = recs[s];
+    double sr = double(acc[s].x), si = double(acc[s].y);
+    if (rr.idx & 0x80000000u) si = -si;
+    const uint32_t idx = rr.idx & 0x7fffffffu;
+    const double orr = double(rr.vr) * sr - double(rr.vi) * si;
+    const double oi = double(rr.vr) * si + double(rr.vi) * sr;
+    if (vis_double)
+      reinterpret_cast<double2 *>(vis_out)[idx] = make_double2(orr, oi);
+    else
+      reinterpret_cast<float2 *>(vis_out)[idx] = make_float2(float(orr), float(oi));
+  }
+}
+
+// ------------------------------------------------ shared-memory FFTs
+//
+// The transform along u of one image column is pruned on both sides: only
+// the occupied u band [-L, L] holds data and only the nx image rows are
+// needed.  With nu = K*M, M = 2^m >= 2L+1, the length-nu DFT splits into K
+// length-M DFTs of the band data twisted by exp(+-2 pi i u k2 / nu):
+//     F(K k1 + k2) = sum_u [g(u) e^{2 pi i u k2/nu}] e^{2 pi i u k1/M}.
+// Each is a radix-16 Stockham FFT in shared memory by M/16 threads holding 16
+// values each; twiddles come from FP64-computed tables.
+
+__host__ __device__ constexpr double cos16(int e) {
+  return e == 0 ? 1.0 : e == 1 ? 0.92387953251128673848 : e == 2 ? 0.70710678118654752440
+       : e == 3 ? 0.38268343236508977173 : e == 4 ? 0.0 : e == 5 ? -0.38268343236508977173
+       : e == 6 ? -0.70710678118654752440 : e == 7 ? -0.92387953251128673848 : -1.0;
+}
+__host__ __device__ constexpr double sin16(int e) {
+  return e == 0 ? 0.0 : e == 1 ? 0.38268343236508977173 : e == 2 ? 0.70710678118654752440
+       : e == 3 ? 0.92387953251128673848 : e == 4 ? 1.0 : e == 5 ? 0.92387953251128673848
+       : e == 6 ? 0.70710678118654752440 : e == 7 ? 0.38268343236508977173 : 0.0;
+}
+template <int N>
+__host__ __device__ constexpr int bitrev(int i) {
+  int r = 0;
+  for (int b = 1; b < N; b <<= 1) {
+    r = (r << 1) | (i & 1);
+    i >>= 1;
+  }
+  return r;
+}
+
+template <typename C>
+__device__ __forceinline__ C cmul(C a, C b) {
+  C r;
+  r.x = a.x * b.x - a.y * b.y;
+  r.y = a.x * b.y + a.y * b.x;
+  return r;
+}
+
+// In-register DFT of N <= 16 points (radix-2, decimation in time):
+// v[q] <- sum_r v[r] exp(sign 2 pi i r q / N).
+template <int N, typename C>
+__device__ __forceinline__ void dft_reg(C *v, int sign) {
+  using R = decltype(v[0].x);
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    const int j = bitrev<N>(i);
+    if (j > i) {
+      C t = v[i];
+      v[i] = v[j];
+      v[j] = t;
+    }
+  }
+#pragma unroll
+  for (int len = 2; len <= N; len <<= 1) {
+#pragma unroll
+    for (int i = 0; i < N; i += len) {
+#pragma unroll
+      for (int k = 0; k < len / 2; ++k) {
+        C a = v[i + k], b = v[i + k + len / 2];
+        const int e = k * (16 / len);
+        if (e == 4) {  // w = sign * i
+          const R bx = b.x;
+          b.x = sign > 0 ? -b.y : b.y;
+          b.y = sign > 0 ? bx : -bx;
+        } else if (e == 2 || e == 6) {  // w = (+-1 + sign i) / sqrt(2)
+          const R h = R(0.70710678118654752440);
+          const R c = (e == 2) ? h : -h, sn = sign > 0 ? h : -h;
+          const R bx = b.x;
+          b.x = c * bx - sn * b.y;
+          b.y = c * b.y + sn * bx;
+        } else if (e != 0) {
+          C w;
+          w.x = R(cos16(e));
+          w.y = R(sign * sin16(e));
+          b = cmul(b, w);
+        }
+        v[i + k].x = a.x + b.x;
+        v[i + k].y = a.y + b.y;
+        v[i + k + len / 2].x = a.x - b.x;
+        v[i + k + len / 2].y = a.y - b.y;
+      }
+    }
+  }
+}
+
+// Buffer index with one padding slot per 16 elements: the first radix-16
+// stage writes at a stride of 16 elements, which without padding puts every
+// lane of a warp on the same shared-memory banks.
+__device__ __forceinline__ int fpad(int i) { return i + (i >> 4); }
+template <int M> struct FftBuf { static constexpr int value = M + M / 16; };
+
+// Per-stage twiddle tables: the stage with stride NS > 1 and radix R needs
+// exp(+2 pi i r k / (NS R)) for r in [1, R), k in [0, NS); stored [r-1][k]
+// (consecutive lanes read consecutive k), concatenated in stage order.
+// (every stage before the last has radix 16, so the stage with stride NS
+// starts after the tables of strides 16, 256, ..., NS/16).
+template <int NS>
+struct TwOffset {
+  static constexpr int value = (NS <= 16) ? 0 : TwOffset<NS / 16>::value + 15 * (NS / 16);
+};
+template <>
+struct TwOffset<1> {
+  static constexpr int value = 0;
+};
+
+// Stockham autosort stages on buf (in place: each stage reads all its inputs
+// before a barrier, then writes).  tw: the per-stage tables above.
+template <typename C, int M, int NS, int TPF>
+struct FftStages {
+  static __device__ __forceinline__ void run(C *buf, const C *tw, int t, int sign) {
+    if constexpr (NS < M) {
+      constexpr int R = (M / NS >= 16) ? 16 : M / NS;
+      constexpr int ITEMS = (M / R) / TPF;
+      C v[ITEMS][R];
+#pragma unroll
+      for (int it = 0; it < ITEMS; ++it) {
+        const int j = t + TPF * it;
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[it][r] = buf[fpad(j + r * (M / R))];
       }
       __syncthreads();
-      // finalize this sub-batch's records
-      for (int j = tid; j < n; j += blockDim.x) {
-        const int s = sb0 + j;
-        R sr = res_s[2 * j], si = res_s[2 * j + 1];
-        C *accp = reinterpret_cast<C *>(a.acc);
-        if (!a.first_pass) {
-          sr += accp[s].x;
-          si += accp[s].y;
-        }
-        if (a.last_pass) {
-          const Rec rr = recs[s];
-          const uint32_t idx = rr.idx & 0x7fffffffu;
-          if (rr.idx & 0x80000000u) si = -si;
-          const double orr = double(rr.vr) * double(sr) - double(rr.vi) * double(si);
-          const double oi = double(rr.vr) * double(si) + double(rr.vi) * double(sr);
-          if (a.vis_double) {
-            reinterpret_cast<double2 *>(a.vis_out)[idx] = make_double2(orr, oi);
-          } else {
-            reinterpret_cast<float2 *>(a.vis_out)[idx] = make_float2(float(orr), float(oi));
+#pragma unroll
+      for (int it = 0; it < ITEMS; ++it) {
+        const int j = t + TPF * it;
+        const int k = j & (NS - 1);
+        if constexpr (NS > 1) {
+          constexpr int off = TwOffset<NS>::value;
+#pragma unroll
+          for (int r = 1; r < R; ++r) {
+            C w = tw[off + (r - 1) * NS + k];
+            if (sign < 0) w.y = -w.y;
+            v[it][r] = cmul(v[it][r], w);
           }
-        } else {
-          C o;
-          o.x = sr;
-          o.y = si;
-          accp[s] = o;
         }
+        dft_reg<R>(v[it], sign);
+        const int d = (j / NS) * NS * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) buf[fpad(d + r * NS)] = v[it][r];
       }
       __syncthreads();
+      FftStages<C, M, NS * R, TPF>::run(buf, tw, t, sign);
+    }
+  }
+};
+
+struct ColArgs {
+  int nx, ny, nu, nv;
+  int P, npl;           // planes in the band layout, planes in this pass
+  int L, band_rows, band_full, K;
+  const void *twM;      // exp(+2 pi i t / M), M entries
+  const void *twnu;     // exp(+2 pi i t / nu), nu entries
+  void *band;           // [band_rows][P][nv] complex
+  void *H;              // [P][ny][nx] complex: u-transformed image columns
+};
+
+// u of buffer slot b (b in [0, M)), or a value > nu if the slot is empty.
+__device__ __forceinline__ int slot_u(const ColArgs &a, int b, int M) {
+  if (a.band_full) return b;           // K == 1, M == nu: every row
+  if (b <= a.L) return b;
+  if (b >= M - a.L) return b - M;      // negative u
+  return 1 << 30;
+}
+__device__ __forceinline__ int slot_bi(const ColArgs &a, int u) {
+  return (a.band_full || u >= 0) ? u : u + a.band_rows;
+}
+
+// Columns per CTA (NB) and threads: M/16 threads per column, up to 512
+// threads per CTA in mixed precision and 256 in FP64 (register budget).
+template <typename R, int M>
+struct ColCfg {
+  static constexpr int TPF = M / 16;
+  static constexpr int MAXT = 256;
+  static constexpr int NB = (MAXT / TPF) > 8 ? 8 : ((MAXT / TPF) < 1 ? 1 : MAXT / TPF);
+  static constexpr int THREADS = NB * TPF;
+};
+
+// Shared memory of a column CTA: NB padded buffers, then the M twiddles.
+template <typename R, int M>
+struct ColSmem {
+  static constexpr size_t bytes() {
+    return (size_t(ColCfg<R, M>::NB) * FftBuf<M>::value + M) * 2 * sizeof(R);
+  }
+};
+
+// (u k2) mod nu for u in the band: |u| <= L < M/2 = nu/(2K) and k2 < K give
+// |u k2| < nu/2, so one conditional add replaces the modulo.
+__device__ __forceinline__ int twist_index(int u, int k2, int nu) {
+  const int e = u * k2;
+  return e < 0 ? e + nu : e;
+}
+
+// ms2dirty direction: band rows (after the v transform) -> H image rows,
+// backward (+) transform along u.
+template <typename R, int LOGM>
+__global__ void __launch_bounds__(ColCfg<R, (1 << LOGM)>::THREADS) k_ucol_bwd(ColArgs a) {
+  using C = typename Cplx<R>::type;
+  constexpr int M = 1 << LOGM, TPF = ColCfg<R, M>::TPF, NB = ColCfg<R, M>::NB;
+  constexpr int BL = FftBuf<M>::value;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *bufall = reinterpret_cast<C *>(smem_raw);
+  C *tws = bufall + NB * BL;
+  const int grp = threadIdx.x / TPF, t = threadIdx.x - grp * TPF;
+  C *buf = bufall + grp * BL;
+  const int lp = blockIdx.y;
+  const int j = blockIdx.x * NB + grp;
+  const bool jv = j < a.ny;
+  const C *band = reinterpret_cast<const C *>(a.band);
+  const C *twnu = reinterpret_cast<const C *>(a.twnu);
+  C *H = reinterpret_cast<C *>(a.H);
+  for (int i = threadIdx.x; i < M; i += blockDim.x) tws[i] = reinterpret_cast<const C *>(a.twM)[i];
+  // coalesced load (slot-major, adjacent image columns innermost), eight
+  // loads in flight per thread before the shared-memory stores
+  constexpr int ITEMS = NB * M / ColCfg<R, M>::THREADS;  // 16 per thread
+  static_assert(ITEMS % 8 == 0, "load batching");
+#pragma unroll 1
+  for (int i0 = 0; i0 < ITEMS; i0 += 8) {
+    C val[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int item = threadIdx.x + (i0 + q) * blockDim.x;
+      const int c = item % NB, b = item / NB;
+      const int jj = blockIdx.x * NB + c;
+      val[q].x = R(0);
+      val[q].y = R(0);
+      const int u = slot_u(a, b, M);
+      if (jj < a.ny && u < (1 << 29)) {
+        int jx = jj + a.nv - a.ny / 2;
+        jx -= (jx >= a.nv) ? a.nv : 0;
+        val[q] = band[(size_t(slot_bi(a, u)) * a.P + lp) * a.nv + jx];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int item = threadIdx.x + (i0 + q) * blockDim.x;
+      bufall[(item % NB) * BL + fpad(item / NB)] = val[q];
+    }
+  }
+  __syncthreads();
+  C g[16];
+#pragma unroll
+  for (int r = 0; r < 16; ++r) g[r] = buf[fpad(t + TPF * r)];
+  __syncthreads();
+  for (int k2 = 0; k2 < a.K; ++k2) {
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+      const int b = t + TPF * r;
+      const int u = slot_u(a, b, M);
+      C val = g[r];
+      if (k2 != 0 && u < (1 << 29)) val = cmul(val, twnu[twist_index(u, k2, a.nu)]);
+      buf[fpad(b)] = val;
+    }
+    __syncthreads();
+    FftStages<C, M, 1, TPF>::run(buf, tws, t, +1);
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+      const int k1 = t + TPF * r;
+      const int k = a.K * k1 + k2;
+      const int ks = (k < a.nu / 2) ? k : k - a.nu;
+      const int i = ks + a.nx / 2;
+      if (jv && i >= 0 && i < a.nx) H[(size_t(lp) * a.ny + j) * a.nx + i] = buf[fpad(k1)];
+    }
+    __syncthreads();
+  }
+}
+
+// dirty2ms direction, the exact transpose: H image rows -> band rows of the
+// image columns, forward (-) transform along u.  Band entries of other
+// columns are left untouched (zeroed by the caller).
+template <typename R, int LOGM>
+__global__ void __launch_bounds__(ColCfg<R, (1 << LOGM)>::THREADS) k_ucol_fwd(ColArgs a) {
+  using C = typename Cplx<R>::type;
+  constexpr int M = 1 << LOGM, TPF = ColCfg<R, M>::TPF, NB = ColCfg<R, M>::NB;
+  constexpr int BL = FftBuf<M>::value;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *bufall = reinterpret_cast<C *>(smem_raw);
+  C *tws = bufall + NB * BL;
+  const int grp = threadIdx.x / TPF, t = threadIdx.x - grp * TPF;
+  C *buf = bufall + grp * BL;
+  const int lp = blockIdx.y;
+  const int j = blockIdx.x * NB + grp;
+  const bool jv = j < a.ny;
+  C *band = reinterpret_cast<C *>(a.band);
+  const C *twnu = reinterpret_cast<const C *>(a.twnu);
+  const C *H = reinterpret_cast<const C *>(a.H);
+  for (int i = threadIdx.x; i < M; i += blockDim.x) tws[i] = reinterpret_cast<const C *>(a.twM)[i];
+  C acc[16];
+#pragma unroll
+  for (int r = 0; r < 16; ++r) acc[r].x = acc[r].y = R(0);
+  for (int k2 = 0; k2 < a.K; ++k2) {
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+      const int k1 = t + TPF * r;
+      const int k = a.K * k1 + k2;
+      const int ks = (k < a.nu / 2) ? k : k - a.nu;
+      const int i = ks + a.nx / 2;
+      C val;
+      val.x = R(0);
+      val.y = R(0);
+      if (jv && i >= 0 && i < a.nx) val = H[(size_t(lp) * a.ny + j) * a.nx + i];
+      buf[fpad(k1)] = val;
+    }
+    __syncthreads();
+    FftStages<C, M, 1, TPF>::run(buf, tws, t, -1);
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+      const int b = t + TPF * r;
+      const int u = slot_u(a, b, M);
+      C val = buf[fpad(b)];
+      if (k2 != 0 && u < (1 << 29)) {
+        C w = twnu[twist_index(u, k2, a.nu)];
+        w.y = -w.y;
+        val = cmul(val, w);
+      }
+      acc[r].x += val.x;
+      acc[r].y += val.y;
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int r = 0; r < 16; ++r) buf[fpad(t + TPF * r)] = acc[r];
+  __syncthreads();
+  for (int item = threadIdx.x; item < NB * M; item += blockDim.x) {
+    const int c = item % NB, b = item / NB;
+    const int jj = blockIdx.x * NB + c;
+    const int u = slot_u(a, b, M);
+    if (jj < a.ny && u < (1 << 29)) {
+      int jx = jj + a.nv - a.ny / 2;
+      jx -= (jx >= a.nv) ? a.nv : 0;
+      band[(size_t(slot_bi(a, u)) * a.P + lp) * a.nv + jx] = bufall[c * BL + fpad(b)];
     }
   }
 }
@@ -763,8 +1228,8 @@ __device__ __forceinline__ void pixel_terms(const ScreenArgs &s, int i, int j,
   q = nm1 + s.nshift;
 }
 
-// ms2dirty: img(i,j) += corr(i,j) * sum_p Re(H[p][j][ix] * exp(-2 pi i w_p q))
-// H holds the u-transformed image columns, [P][ny][nu].
+// ms2dirty: img(i,j) += corr(i,j) * sum_p Re(H[p][j][i] * exp(-2 pi i w_p q)),
+// FP64 phases (recurrence over planes) and FP64 accumulation.
 template <typename R>
 __global__ void __launch_bounds__(256) k_screen_add(ScreenArgs s, const void *Hv, double *img) {
   using C = typename Cplx<R>::type;
@@ -780,22 +1245,22 @@ __global__ void __launch_bounds__(256) k_screen_add(ScreenArgs s, const void *Hv
       double corr, q;
       bool inside;
       pixel_terms(s, i, j, corr, q, inside);
-      int ix = s.nu - s.nx / 2 + i;
-      if (ix >= s.nu) ix -= s.nu;
       double acc = 0;
+      const C *hp = H + size_t(j) * s.nx + i;
+      const size_t pstride = size_t(s.ny) * s.nx;
       if (s.do_w && inside) {
         const double w0 = s.wmin + s.pb0 * s.dw;
         double2 sc = cexp_turns(-w0 * q);
         const double2 st = cexp_turns(-s.dw * q);
         for (int p = 0; p < s.npl; ++p) {
-          const C h = H[(size_t(p) * s.ny + j) * s.nu + ix];
+          const C h = hp[p * pstride];
           acc += double(h.x) * sc.x - double(h.y) * sc.y;
           const double nr = sc.x * st.x - sc.y * st.y;
           sc.y = sc.x * st.y + sc.y * st.x;
           sc.x = nr;
         }
       } else {
-        for (int p = 0; p < s.npl; ++p) acc += double(H[(size_t(p) * s.ny + j) * s.nu + ix].x);
+        for (int p = 0; p < s.npl; ++p) acc += double(hp[p * pstride].x);
       }
       val = acc * corr;
     }
@@ -808,7 +1273,7 @@ __global__ void __launch_bounds__(256) k_screen_add(ScreenArgs s, const void *Hv
   }
 }
 
-// dirty2ms: H[p][j][ix] = dirty(i,j) * corr(i,j) * exp(+2 pi i w_p q)
+// dirty2ms: H[p][j][i] = dirty(i,j) * corr(i,j) * exp(+2 pi i w_p q)
 template <typename R>
 __global__ void __launch_bounds__(256) k_screen_put(ScreenArgs s, const double *img, void *Hv) {
   using C = typename Cplx<R>::type;
@@ -822,6 +1287,7 @@ __global__ void __launch_bounds__(256) k_screen_put(ScreenArgs s, const double *
   }
   __syncthreads();
   const int i = i0 + tx;
+  const size_t pstride = size_t(s.ny) * s.nx;
   for (int k = 0; k < 4; ++k) {
     const int j = j0 + ty + 8 * k;
     if (i >= s.nx || j >= s.ny) continue;
@@ -829,8 +1295,7 @@ __global__ void __launch_bounds__(256) k_screen_put(ScreenArgs s, const double *
     bool inside;
     pixel_terms(s, i, j, corr, q, inside);
     const double val = tile[ty + 8 * k][tx] * corr;
-    int ix = s.nu - s.nx / 2 + i;
-    if (ix >= s.nu) ix -= s.nu;
+    C *hp = H + size_t(j) * s.nx + i;
     if (s.do_w && inside) {
       const double w0 = s.wmin + s.pb0 * s.dw;
       double2 sc = cexp_turns(w0 * q);
@@ -839,7 +1304,7 @@ __global__ void __launch_bounds__(256) k_screen_put(ScreenArgs s, const double *
         C o;
         o.x = R(val * sc.x);
         o.y = R(val * sc.y);
-        H[(size_t(p) * s.ny + j) * s.nu + ix] = o;
+        hp[p * pstride] = o;
         const double nr = sc.x * st.x - sc.y * st.y;
         sc.y = sc.x * st.y + sc.y * st.x;
         sc.x = nr;
@@ -849,7 +1314,7 @@ __global__ void __launch_bounds__(256) k_screen_put(ScreenArgs s, const double *
         C o;
         o.x = R(val);
         o.y = R(0);
-        H[(size_t(p) * s.ny + j) * s.nu + ix] = o;
+        hp[p * pstride] = o;
       }
     }
   }

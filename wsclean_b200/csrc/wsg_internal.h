@@ -116,6 +116,9 @@ struct GridPlan {
   // occupied u band: rows [0, Lu] and [nu-Lu, nu), or all rows
   size_t Lu = 0, band_rows = 0;
   bool band_full = false;
+  // nu = K * 2^logM with 2^logM >= band_rows: the u transform of an image
+  // column is K pruned FFTs of length 2^logM
+  int logM = 0, K = 1;
   // bins and sort keys
   int T = 16;
   int ntu = 0, ntv = 0, nwmin = 1;
