@@ -110,6 +110,27 @@ int wsg_ms2dirty(wsg_ctx *ctx, const wsg_args *a, const void *vis, void *dirty,
 /* Replaces ducc0::dirty2ms (wgridder.h:1712-1729), the exact adjoint. */
 int wsg_dirty2ms(wsg_ctx *ctx, const wsg_args *a, const void *dirty, void *vis);
 
+/* Allocation-free variant of wsg_ms2dirty, for callers that cannot allocate
+ * device memory while they grid -- for example code recording a CUDA graph,
+ * where cudaMalloc is not allowed, or a process whose device memory is owned
+ * by another framework's pool.  It calls no cudaMalloc, cudaFree or
+ * allocating library routine (no cuFFT plans; its own FFT kernels instead):
+ * all scratch comes from one static device array of 96 MiB that every GPU
+ * loading the library holds until the process exits.  This entry point has no
+ * counterpart in the reference.
+ *
+ * Limits: mixed precision only; uvw, freq, vis, dirty (and wgt/mask when
+ * given) must be device memory; the whole problem's scratch (about 40 bytes
+ * per visibility plus the FP64 image plus at least one w plane of the band
+ * grid and of the transformed columns) must fit in the 96 MiB, otherwise
+ * WSG_ERR_INVALID with a message.  nv is a power of two here, so the grid
+ * can differ from wsg_ms2dirty's; results agree within epsilon.
+ * The first call on a device looks up the array's device address and should
+ * come before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU race and must be serialised by the caller.  stream may
+ * be NULL (the legacy default stream).  The image is overwritten. */
+int wsg_ms2dirty_noalloc(const wsg_args *a, const void *vis, void *dirty, void *stream);
+
 /* -------------------------------------- WGriddingGridder_Simple replacement */
 
 typedef struct {

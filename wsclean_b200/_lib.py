@@ -27,7 +27,7 @@ EXPORTED = [
     "wsg_gridder_finalize_image", "wsg_gridder_real_image",
     "wsg_gridder_initialize_prediction", "wsg_gridder_predict_visibilities",
     "wsg_gridder_ctx", "wsg_get_stats", "wsg_last_error", "wsg_abi_version",
-    "wsg_plan_grid",
+    "wsg_plan_grid", "wsg_ms2dirty_noalloc",
 ]
 
 c_size_t, c_double, c_int, c_void_p = ctypes.c_size_t, ctypes.c_double, ctypes.c_int, ctypes.c_void_p
@@ -124,6 +124,7 @@ def lib():
         L.wsg_gridder_ctx.argtypes = [vp]
         L.wsg_gridder_ctx.restype = vp
         L.wsg_get_stats.argtypes = [vp, P(WsgStats)]
+        L.wsg_ms2dirty_noalloc.argtypes = [P(WsgArgs), vp, vp, vp]
         L.wsg_plan_grid.argtypes = [P(WsgArgs), c_size_t, c_double, c_double, c_double,
                                     c_double, P(WsgStats)]
         L.wsg_last_error.restype = ctypes.c_char_p

@@ -313,7 +313,7 @@ bool pick_nu(double n0, double umax_px, int W, bool fp32, size_t &nu, int &logM,
   return best != ~size_t(0);
 }
 
-void choose_grid(GridPlan &g, double sigma_min, double sigma_max, int tile) {
+void choose_grid(GridPlan &g, double sigma_min, double sigma_max, int tile, bool pow2_v) {
   require(g.nx % 2 == 0, "nx_dirty must be even");
   require(g.ny % 2 == 0, "ny_dirty must be even");
   require(g.eps > 0, "epsilon must be positive");
@@ -359,6 +359,11 @@ void choose_grid(GridPlan &g, double sigma_min, double sigma_max, int tile) {
     t.kernel = k;
     if (!pick_nu(g.nx * k.sigma, umax_px, k.W, g.fp32, t.nu, t.logM, t.K)) continue;
     t.nv = 2 * good_size_cufft(size_t(g.ny * k.sigma * 0.5) + 1);
+    if (pow2_v) {
+      size_t p2 = 256;
+      while (p2 < size_t(g.ny * k.sigma) + 2) p2 *= 2;
+      t.nv = p2;
+    }
     set_band(t);
     double planes = 1;
     if (g.do_w) {

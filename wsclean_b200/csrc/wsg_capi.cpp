@@ -192,6 +192,13 @@ int wsg_gridder_predict_visibilities(wsg_gridder *g, size_t nrows, size_t nchan,
 
 wsg_ctx *wsg_gridder_ctx(wsg_gridder *g) { return g ? &g->view : nullptr; }
 
+int wsg_ms2dirty_noalloc(const wsg_args *a, const void *vis, void *dirty, void *stream) {
+  return guarded([&] {
+    wsg::require(a != nullptr, "args are required");
+    wsg::ms2dirty_noalloc(*a, vis, dirty, reinterpret_cast<cudaStream_t>(stream));
+  });
+}
+
 int wsg_plan_grid(const wsg_args *a, size_t nvis, double wmin, double wmax, double umax,
                   double vmax, wsg_stats *out) {
   return guarded([&] {

@@ -104,6 +104,9 @@ class Context {
   bool corr_valid = false;
 };
 
+// Allocation-free mixed-precision ms2dirty (scratch in a static device array).
+void ms2dirty_noalloc(const wsg_args &a, const void *vis, void *dirty, cudaStream_t stream);
+
 // WGriddingGridder_Simple replacement (wgridder/wgriddinggridder_simple.h:34-144).
 class Gridder {
  public:

@@ -1181,6 +1181,37 @@ __global__ void __launch_bounds__(ColCfg<R, (1 << LOGM)>::THREADS) k_ucol_fwd(Co
   }
 }
 
+// In-place FFT of `rows` contiguous rows of length M = 2^LOGM in global
+// memory (the transform along v when cuFFT cannot be used), sign +1 backward.
+template <typename R, int LOGM>
+__global__ void __launch_bounds__(ColCfg<R, (1 << LOGM)>::THREADS)
+k_row_fft(void *data, long long rows, const void *twv, int sign) {
+  using C = typename Cplx<R>::type;
+  constexpr int M = 1 << LOGM, TPF = ColCfg<R, M>::TPF, NB = ColCfg<R, M>::NB;
+  constexpr int BL = FftBuf<M>::value;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *bufall = reinterpret_cast<C *>(smem_raw);
+  C *tws = bufall + NB * BL;
+  const int grp = threadIdx.x / TPF, t = threadIdx.x - grp * TPF;
+  C *d = reinterpret_cast<C *>(data);
+  for (int i = threadIdx.x; i < M; i += blockDim.x) tws[i] = reinterpret_cast<const C *>(twv)[i];
+  const long long row = (long long)blockIdx.x * NB + grp;
+  const bool rv = row < rows;
+#pragma unroll
+  for (int r = 0; r < 16; ++r) {
+    C v;
+    v.x = R(0);
+    v.y = R(0);
+    if (rv) v = d[row * M + t + TPF * r];
+    bufall[grp * BL + fpad(t + TPF * r)] = v;
+  }
+  __syncthreads();
+  FftStages<C, M, 1, TPF>::run(bufall + grp * BL, tws, t, sign);
+#pragma unroll
+  for (int r = 0; r < 16; ++r)
+    if (rv) d[row * M + t + TPF * r] = bufall[grp * BL + fpad(t + TPF * r)];
+}
+
 // ------------------------------------------------------------- screens
 
 struct ScreenArgs {

@@ -129,7 +129,9 @@ struct GridPlan {
 // Parameter choice (the analogue of ducc0 Params::getNuNv, wgridder.h:1503-1576,
 // and the w-plane placement of countRanges, wgridder.h:690-699).  The cost
 // model is this implementation's own, calibrated for the B200 kernels.
-void choose_grid(GridPlan &g, double sigma_min, double sigma_max, int tile);
+// pow2_v: restrict nv to a power of two (for the FFT along v by the
+// library's own shared-memory kernel instead of cuFFT).
+void choose_grid(GridPlan &g, double sigma_min, double sigma_max, int tile, bool pow2_v = false);
 
 // Nominal device bytes for one pass with `planes` planes resident.
 size_t plan_bytes(const GridPlan &g, size_t planes, bool gridding);
