@@ -121,3 +121,11 @@ def test_kernel_table_consistent():
         assert all(b < a for a, b in zip(errs, errs[1:]))
     e, b, e0 = tab[(6, 1.5)]
     assert kernel_db.err1d(6, 1.5, b, e0) == pytest.approx(e, rel=1e-6)
+
+
+def test_cpp_adapter_compiles(tmp_path):
+    """The WGriddingGridderBase adapter builds against include/wsg.h alone."""
+    host = os.path.join(ROOT, "wsclean_b200", "host")
+    subprocess.run(["g++", "-std=c++17", "-c", "-I", host, "-I", os.path.join(ROOT, "include"),
+                    os.path.join(host, "wgriddinggridder_b200.cpp"), "-o",
+                    str(tmp_path / "adapter.o")], check=True)

@@ -155,3 +155,28 @@ def config1(scale=1.0, npix=1024):
                                  np.linspace(150e6, 151.5e6, 4), seed=1, ntimes=nt)
     return dict(uvw=uvw, freq=freq, rng=rng, npix_x=npix, npix_y=npix,
                 pixsize=10.0 * ARCSEC, nsrc=20)
+
+
+def briggs_weights(uvw, freq, nx, ny, px, py, robust=0.0, noise_weights=None):
+    """Briggs imaging weights with WSClean's ImageWeights semantics
+    (structures/imageweights.cpp:113-143, cell lookup imageweights.h:73-80):
+    the weights are summed on a half-plane (v >= 0) grid of nx x ny/2 cells of
+    1/(n*pixelscale) wavelengths, and each visibility gets
+    1 / (1 + W_cell * s^2) with s^2 = (5*10^-robust)^2 / (sum W^2 / sum W)."""
+    nrows, nchan = uvw.shape[0], len(freq)
+    w = np.ones((nrows, nchan)) if noise_weights is None else np.asarray(noise_weights, float)
+    u = uvw[:, 0:1] * (np.asarray(freq)[None, :] / C_LIGHT)
+    v = uvw[:, 1:2] * (np.asarray(freq)[None, :] / C_LIGHT)
+    flip = v < 0
+    u = np.where(flip, -u, u)
+    v = np.where(flip, -v, v)
+    x = np.floor(u * nx * px + nx // 2).astype(np.int64)
+    y = np.floor(v * ny * py).astype(np.int64)
+    ok = (x >= 0) & (x < nx) & (y < ny // 2)
+    grid = np.zeros(nx * (ny // 2))
+    np.add.at(grid, (x[ok] + y[ok] * nx), w[ok])
+    total = w[ok].sum()
+    avg = np.sum(grid * grid) / total
+    s2 = (5.0 * np.exp(-np.log(10.0) * robust)) ** 2 / avg
+    cell = np.where(ok, grid[np.where(ok, x + y * nx, 0)], 0.0)
+    return np.where(ok, 1.0 / (1.0 + cell * s2), 0.0)
