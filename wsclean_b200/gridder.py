@@ -81,6 +81,14 @@ class Context:
     def release_buffers(self):
         L.check(L.lib().wsg_ctx_release_buffers(self._h))
 
+    def _bind_stream(self, *tensors):
+        """Run the call on torch's current stream of the tensors' device when
+        any operand is a CUDA tensor, so that it is ordered after the torch
+        work that produced its inputs (the context's own stream otherwise)."""
+        dev = next((t.device for t in tensors if _is_torch(t) and t.is_cuda), None)
+        s = torch.cuda.current_stream(dev).cuda_stream if dev is not None else None
+        L.check(L.lib().wsg_ctx_set_stream(self._h, s))
+
     def stats(self):
         s = L.WsgStats()
         L.check(L.lib().wsg_get_stats(self._h, ctypes.byref(s)))
@@ -142,6 +150,7 @@ class Context:
         a = self._args(uvw, freq, nrows, nchan, wgt, mask, npix_x, npix_y, pixsize_x, pixsize_y,
                        epsilon, do_wgridding, negate_v, divide_by_n, sigma_min, sigma_max,
                        center_x, center_y, precision, _NP_C[vdt], _NP_F[ddt], keep)
+        self._bind_stream(v, d, *keep)
         L.check(L.lib().wsg_ms2dirty(self._h, ctypes.byref(a), vp, dp, int(bool(accumulate))))
         return d
 
@@ -167,6 +176,7 @@ class Context:
         a = self._args(uvw, freq, nrows, nchan, wgt, mask, npix_x, npix_y, pixsize_x, pixsize_y,
                        epsilon, do_wgridding, negate_v, divide_by_n, sigma_min, sigma_max,
                        center_x, center_y, precision, _NP_C[vdt], _NP_F[ddt], keep)
+        self._bind_stream(d, v, *keep)
         L.check(L.lib().wsg_dirty2ms(self._h, ctypes.byref(a), dp, vp))
         return v
 
