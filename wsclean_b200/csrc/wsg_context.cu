@@ -247,6 +247,24 @@ int launch_blocks(size_t n, int threads) {
   return int(std::min<size_t>(std::max<size_t>(b, 1), 65535 * 8));
 }
 
+// Dynamic shared-memory limit of a kernel, set once per (kernel, device):
+// every driver call on the launch path costs host time that the GPU waits
+// through.
+template <typename F>
+void smem_attr(F *fn, size_t smem) {
+  static std::mutex mu;
+  static std::map<std::pair<const void *, int>, size_t> done;
+  int dev = 0;
+  cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+  std::lock_guard<std::mutex> lk(mu);
+  auto key = std::make_pair(reinterpret_cast<const void *>(fn), dev);
+  auto it = done.find(key);
+  if (it != done.end() && it->second >= smem) return;
+  cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+             "smem attribute");
+  done[key] = smem;
+}
+
 }  // namespace
 
 // Kernel template dispatch over the support W.
@@ -278,13 +296,11 @@ struct GridKernels {
     constexpr int P = ppl<W>();
     if (spread) {
       auto fn = k_spread<R, W, P, NWARP>;
-      cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
-                 "smem attribute");
+      smem_attr(fn, smem);
       fn<<<grid, NWARP * 32, smem, st>>>(a, g, kc);
     } else {
       auto fn = k_interp<R, W, P, NWARP>;
-      cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
-                 "smem attribute");
+      smem_attr(fn, smem);
       fn<<<grid, NWARP * 32, smem, st>>>(a, g, kc);
     }
     cuda_check(cudaGetLastError(), spread ? "k_spread launch" : "k_interp launch");
@@ -310,13 +326,9 @@ struct GridKernels {
         // set the smem attribute before asking for the occupancy
         constexpr int P = ppl<WW>();
         if (spread)
-          cuda_check(cudaFuncSetAttribute(k_spread<R, WW, P, NWARP>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
-                     "smem attribute");
+          smem_attr(k_spread<R, WW, P, NWARP>, smem);
         else
-          cuda_check(cudaFuncSetAttribute(k_interp<R, WW, P, NWARP>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
-                     "smem attribute");
+          smem_attr(k_interp<R, WW, P, NWARP>, smem);
         int occ = occupancy<WW>(spread, smem);
         dim3 grid(nsm * occ);
         run<WW>(spread, grid, smem, st, a, g, kc);
@@ -348,17 +360,13 @@ struct ColKernels {
   static void run1(bool bwd, const ColArgs &a, int npl, cudaStream_t st) {
     constexpr int M = 1 << LOGM;
     using Cfg = ColCfg<R, M>;
-    const size_t smem = ColSmem<R, M>::bytes();
+    const size_t smem = ColSmem2<R, M>::bytes();
     dim3 grid((a.ny + Cfg::NB - 1) / Cfg::NB, npl);
     if (bwd) {
-      cuda_check(cudaFuncSetAttribute(k_ucol_bwd<R, LOGM>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
-                 "smem attribute");
+      smem_attr(k_ucol_bwd<R, LOGM>, smem);
       k_ucol_bwd<R, LOGM><<<grid, Cfg::THREADS, smem, st>>>(a);
     } else {
-      cuda_check(cudaFuncSetAttribute(k_ucol_fwd<R, LOGM>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
-                 "smem attribute");
+      smem_attr(k_ucol_fwd<R, LOGM>, smem);
       k_ucol_fwd<R, LOGM><<<grid, Cfg::THREADS, smem, st>>>(a);
     }
     cuda_check(cudaGetLastError(), bwd ? "k_ucol_bwd launch" : "k_ucol_fwd launch");
@@ -582,8 +590,10 @@ ColArgs make_col(const GridPlan &g, size_t P, const void *tw, void *band, void *
   c.band_full = g.band_full;
   c.K = g.K;
   const size_t cs = g.fp32 ? 8 : 16;
+  const size_t M = size_t(1) << g.logM;
   c.twM = tw;
-  c.twnu = reinterpret_cast<const char *>(tw) + (size_t(1) << g.logM) * cs;
+  c.twB = reinterpret_cast<const char *>(tw) + M * cs;
+  c.twQ = reinterpret_cast<const char *>(tw) + (M + size_t(g.K) * (M / 16)) * cs;
   c.band = band;
   c.H = H;
   return c;
@@ -627,35 +637,50 @@ ChebCorr Context::upload_corrections(const GridPlan &g) {
 // FP64-computed twiddle tables: the per-stage tables of the length-M
 // shared-memory FFT (M entries) and exp(+2 pi i t / nu) for the twist (nu
 // entries), stored in the arithmetic type, cached per (M, nu, type).
+// Twiddle tables of the pruned u transform (nu = K M), as interleaved
+// (re, im) doubles: the per-stage FFT tables exp(+2 pi i r k / (NS R)),
+// [r-1][k] in stage order (M entries); the twist bases exp(+2 pi i t k2 / nu),
+// [k2][t] for t < M/16; and the per-slot factors exp(+2 pi i (M/16 q - neg M)
+// k2 / nu), [k2][q][neg].  Angles are reduced exactly in integers before the
+// FP64 sin/cos.
+static std::vector<double> col_twiddle_table(size_t M, size_t nu, size_t K) {
+  const size_t TPF = M / 16;
+  std::vector<double> h(2 * (M + K * TPF + 32 * K), 0.0);
+  auto put = [&](size_t idx, long long num, long long den) {
+    long long r = num % den;
+    if (r < 0) r += den;
+    double f = double(r) / double(den);
+    if (f > 0.5) f -= 1.0;
+    h[2 * idx] = std::cos(2.0 * M_PI * f);
+    h[2 * idx + 1] = std::sin(2.0 * M_PI * f);
+  };
+  size_t off = 0;
+  for (size_t NS = 1; NS < M;) {
+    const size_t R = (M / NS >= 16) ? 16 : M / NS;
+    if (NS > 1) {
+      for (size_t r = 1; r < R; ++r)
+        for (size_t k = 0; k < NS; ++k) put(off + (r - 1) * NS + k, (long long)(r * k), (long long)(NS * R));
+      off += (R - 1) * NS;
+    }
+    NS *= R;
+  }
+  for (size_t k2 = 0; k2 < K; ++k2)
+    for (size_t t = 0; t < TPF; ++t) put(M + k2 * TPF + t, (long long)(t * k2), (long long)nu);
+  for (size_t k2 = 0; k2 < K; ++k2)
+    for (size_t q = 0; q < 16; ++q)
+      for (int neg = 0; neg < 2; ++neg)
+        put(M + K * TPF + (k2 * 16 + q) * 2 + neg,
+            ((long long)(TPF * q) - (neg ? (long long)M : 0)) * (long long)k2, (long long)nu);
+  return h;
+}
+
 const void *Context::upload_twiddles(const GridPlan &g, bool dbl) {
   const size_t M = size_t(1) << g.logM;
   auto key = std::make_tuple(M, g.nu, int(dbl));
   const size_t cs = dbl ? 16 : 8;
   if (!(tw_valid && key == tw_key)) {
-    std::vector<double> h(2 * (M + g.nu), 0.0);
-    // per-stage FFT twiddles exp(+2 pi i r k / (NS R)), [r-1][k], stage order
-    size_t off = 0;
-    for (size_t NS = 1; NS < M;) {
-      const size_t R = (M / NS >= 16) ? 16 : M / NS;
-      if (NS > 1) {
-        for (size_t r = 1; r < R; ++r)
-          for (size_t k = 0; k < NS; ++k) {
-            const double f = double(r * k) / double(NS * R);
-            h[2 * (off + (r - 1) * NS + k)] = std::cos(2.0 * M_PI * f);
-            h[2 * (off + (r - 1) * NS + k) + 1] = std::sin(2.0 * M_PI * f);
-          }
-        off += (R - 1) * NS;
-      }
-      NS *= R;
-    }
-    for (size_t t = 0; t < g.nu; ++t) {
-      // reduce t/nu to [-1/2, 1/2] turns before the FP64 sin/cos
-      double f = double(t) / double(g.nu);
-      if (f > 0.5) f -= 1.0;
-      h[2 * (M + t)] = std::cos(2.0 * M_PI * f);
-      h[2 * (M + t) + 1] = std::sin(2.0 * M_PI * f);
-    }
-    void *d = b_tw.ensure((M + g.nu) * cs);
+    const std::vector<double> h = col_twiddle_table(M, g.nu, size_t(g.K));
+    void *d = b_tw.ensure(h.size() / 2 * cs);
     if (dbl) {
       CK(cudaMemcpy(d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
     } else {
@@ -668,17 +693,28 @@ const void *Context::upload_twiddles(const GridPlan &g, bool dbl) {
   return b_tw.p;
 }
 
+// Planes resident per pass: as many as fit in 55% of the device memory and
+// in what is free (plus what this context already holds).  cudaMemGetInfo is
+// a slow driver query (milliseconds, and tens of them when other processes
+// query the GPU), so a repeated plan whose buffers are still held reuses the
+// previous answer.
 size_t Context::choose_planes(const GridPlan &g, bool gridding) {
+  const size_t per = plan_bytes(g, 1, gridding);
+  const size_t held = b_band.n + b_H.n;
+  const auto key = std::make_tuple(per, g.nplanes, int(gridding));
+  if (planes_valid && key == planes_key && held >= planes_last * per) return planes_last;
   size_t total = 0, freeb = 0;
   CK(cudaMemGetInfo(&freeb, &total));
-  size_t held = b_band.n + b_H.n;
   double budget = 0.55 * double(total);
   size_t avail = size_t(std::min<double>(budget, double(freeb + held) - 2e9));
-  size_t per = plan_bytes(g, 1, gridding);
   size_t P = std::max<size_t>(1, std::min<size_t>(g.nplanes, per ? avail / per : g.nplanes));
   int lim = env_int("WSG_MAX_PLANES", 0);
   if (lim > 0) P = std::min<size_t>(P, size_t(lim));
-  return std::min(P, g.nplanes);
+  P = std::min(P, g.nplanes);
+  planes_key = key;
+  planes_last = P;
+  planes_valid = true;
+  return P;
 }
 
 template <typename R>
@@ -1253,9 +1289,7 @@ void row_fft_f(int logM, void *data, long long rows, const void *tw, int sign, c
     constexpr int M = 1 << LOGM;
     using Cfg = ColCfg<float, M>;
     const size_t smem = ColSmem<float, M>::bytes();
-    cuda_check(cudaFuncSetAttribute(k_row_fft<float, LOGM>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
-               "smem attribute");
+    smem_attr(k_row_fft<float, LOGM>, smem);
     const long long nblk = (rows + Cfg::NB - 1) / Cfg::NB;
     k_row_fft<float, LOGM><<<unsigned(nblk), Cfg::THREADS, smem, st>>>(data, rows, tw, sign);
     cuda_check(cudaGetLastError(), "k_row_fft launch");
@@ -1416,14 +1450,8 @@ void ms2dirty_noalloc(const wsg_args &a, const void *vis, void *dirty, cudaStrea
     cuda_check(cudaMemcpyAsync(d_cf, cf.data(), cf.size() * sizeof(double), cudaMemcpyHostToDevice,
                                stream), "cf H2D");
     const size_t Mu = size_t(1) << gp.logM, Mv = gp.nv;
-    std::vector<float> htw = stage_twiddles_f(Mu);
-    htw.resize(2 * (Mu + gp.nu));
-    for (size_t t = 0; t < gp.nu; ++t) {
-      double f = double(t) / double(gp.nu);
-      if (f > 0.5) f -= 1.0;
-      htw[2 * (Mu + t)] = float(std::cos(2.0 * M_PI * f));
-      htw[2 * (Mu + t) + 1] = float(std::sin(2.0 * M_PI * f));
-    }
+    const std::vector<double> htwd = col_twiddle_table(Mu, gp.nu, size_t(gp.K));
+    const std::vector<float> htw(htwd.begin(), htwd.end());
     const std::vector<float> htwv = stage_twiddles_f(Mv);
     float *d_tw = reinterpret_cast<float *>(ar.take(htw.size() * sizeof(float)));
     float *d_twv = reinterpret_cast<float *>(ar.take(htwv.size() * sizeof(float)));

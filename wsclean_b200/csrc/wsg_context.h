@@ -98,6 +98,10 @@ class Context {
   size_t fft_work_need = 0;
   std::tuple<size_t, size_t, int> tw_key;
   bool tw_valid = false;
+  // last plane-batch choice (choose_planes)
+  std::tuple<size_t, size_t, int> planes_key;
+  size_t planes_last = 0;
+  bool planes_valid = false;
   // correction-table cache
   std::tuple<int, double, double, size_t, size_t, size_t, size_t, double> corr_key;
   ChebCorr corr_cc;

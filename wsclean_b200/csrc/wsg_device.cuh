@@ -868,16 +868,6 @@ __host__ __device__ constexpr double sin16(int e) {
        : e == 3 ? 0.92387953251128673848 : e == 4 ? 1.0 : e == 5 ? 0.92387953251128673848
        : e == 6 ? 0.70710678118654752440 : e == 7 ? 0.38268343236508977173 : 0.0;
 }
-template <int N>
-__host__ __device__ constexpr int bitrev(int i) {
-  int r = 0;
-  for (int b = 1; b < N; b <<= 1) {
-    r = (r << 1) | (i & 1);
-    i >>= 1;
-  }
-  return r;
-}
-
 template <typename C>
 __device__ __forceinline__ C cmul(C a, C b) {
   C r;
@@ -886,50 +876,48 @@ __device__ __forceinline__ C cmul(C a, C b) {
   return r;
 }
 
-// In-register DFT of N <= 16 points (radix-2, decimation in time):
-// v[q] <- sum_r v[r] exp(sign 2 pi i r q / N).
+// In-register DFT of N <= 16 points: v[q] <- sum_r v[r] exp(sign 2 pi i r q / N),
+// as radix-2 Stockham stages (natural order in and out, so every register
+// index is a compile-time constant once the loops are unrolled).
 template <int N, typename C>
 __device__ __forceinline__ void dft_reg(C *v, int sign) {
   using R = decltype(v[0].x);
+  constexpr int LOG = N == 2 ? 1 : N == 4 ? 2 : N == 8 ? 3 : 4;
+  static_assert((1 << LOG) == N, "dft_reg: N must be 2, 4, 8 or 16");
 #pragma unroll
-  for (int i = 0; i < N; ++i) {
-    const int j = bitrev<N>(i);
-    if (j > i) {
-      C t = v[i];
-      v[i] = v[j];
-      v[j] = t;
-    }
-  }
+  for (int s = 0; s < LOG; ++s) {
+    const int NS = 1 << s;
+    C y[N];
 #pragma unroll
-  for (int len = 2; len <= N; len <<= 1) {
-#pragma unroll
-    for (int i = 0; i < N; i += len) {
-#pragma unroll
-      for (int k = 0; k < len / 2; ++k) {
-        C a = v[i + k], b = v[i + k + len / 2];
-        const int e = k * (16 / len);
-        if (e == 4) {  // w = sign * i
-          const R bx = b.x;
-          b.x = sign > 0 ? -b.y : b.y;
-          b.y = sign > 0 ? bx : -bx;
-        } else if (e == 2 || e == 6) {  // w = (+-1 + sign i) / sqrt(2)
-          const R h = R(0.70710678118654752440);
-          const R c = (e == 2) ? h : -h, sn = sign > 0 ? h : -h;
-          const R bx = b.x;
-          b.x = c * bx - sn * b.y;
-          b.y = c * b.y + sn * bx;
-        } else if (e != 0) {
-          C w;
-          w.x = R(cos16(e));
-          w.y = R(sign * sin16(e));
-          b = cmul(b, w);
-        }
-        v[i + k].x = a.x + b.x;
-        v[i + k].y = a.y + b.y;
-        v[i + k + len / 2].x = a.x - b.x;
-        v[i + k + len / 2].y = a.y - b.y;
+    for (int j = 0; j < N / 2; ++j) {
+      const int k = j & (NS - 1);
+      const C a = v[j];
+      C b = v[j + N / 2];
+      const int e = k * (8 / NS);  // twiddle exp(sign 2 pi i k / (2 NS)) in 16ths of a turn
+      if (e == 4) {  // w = sign * i
+        const R bx = b.x;
+        b.x = sign > 0 ? -b.y : b.y;
+        b.y = sign > 0 ? bx : -bx;
+      } else if (e == 2 || e == 6) {  // w = (+-1 + sign i) / sqrt(2)
+        const R h = R(0.70710678118654752440);
+        const R c = (e == 2) ? h : -h, sn = sign > 0 ? h : -h;
+        const R bx = b.x;
+        b.x = c * bx - sn * b.y;
+        b.y = c * b.y + sn * bx;
+      } else if (e != 0) {
+        C w;
+        w.x = R(cos16(e));
+        w.y = R(sign * sin16(e));
+        b = cmul(b, w);
       }
+      const int d = (j / NS) * 2 * NS + k;
+      y[d].x = a.x + b.x;
+      y[d].y = a.y + b.y;
+      y[d + NS].x = a.x - b.x;
+      y[d + NS].y = a.y - b.y;
     }
+#pragma unroll
+    for (int j = 0; j < N; ++j) v[j] = y[j];
   }
 }
 
@@ -997,8 +985,9 @@ struct ColArgs {
   int nx, ny, nu, nv;
   int P, npl;           // planes in the band layout, planes in this pass
   int L, band_rows, band_full, K;
-  const void *twM;      // exp(+2 pi i t / M), M entries
-  const void *twnu;     // exp(+2 pi i t / nu), nu entries
+  const void *twM;      // per-stage FFT twiddles, M entries
+  const void *twB;      // exp(+2 pi i t k2 / nu), [k2][t], K x M/16 entries
+  const void *twQ;      // exp(+2 pi i (M/16 q - neg M) k2 / nu), [k2][q][neg], K x 32
   void *band;           // [band_rows][P][nv] complex
   void *H;              // [P][ny][nx] complex: u-transformed image columns
 };
@@ -1022,6 +1011,9 @@ struct ColCfg {
   static constexpr int MAXT = 256;
   static constexpr int NB = (MAXT / TPF) > 8 ? 8 : ((MAXT / TPF) < 1 ? 1 : MAXT / TPF);
   static constexpr int THREADS = NB * TPF;
+  // resident CTAs asked of the register allocator (128 registers a thread
+  // for FP32 at 256 threads)
+  static constexpr int MINB = (sizeof(R) == 4 && THREADS <= 256) ? 2 : 1;
 };
 
 // Shared memory of a column CTA: NB padded buffers, then the M twiddles.
@@ -1032,42 +1024,134 @@ struct ColSmem {
   }
 };
 
-// (u k2) mod nu for u in the band: |u| <= L < M/2 = nu/(2K) and k2 < K give
-// |u k2| < nu/2, so one conditional add replaces the modulo.
-__device__ __forceinline__ int twist_index(int u, int k2, int nu) {
-  const int e = u * k2;
-  return e < 0 ? e + nu : e;
+// ---- column transforms with register-resident first and last stages ----
+//
+// The M-point transform runs as Stockham stages (radix 16, the last one of
+// radix M/NS) but keeps the first stage's inputs and the last stage's outputs
+// in registers: thread t of a column group holds positions t + TPF q
+// (q = 0..15) on both ends, which are exactly the first radix-16 stage's
+// inputs and (for every power-of-two M) the last stage's outputs.  Only the
+// exchanges between stages go through shared memory, ping-ponging between two
+// buffers so that each stage needs one barrier.
+
+// Stages after the first, from stride NS on: `cur` holds the data; middle
+// stages write `oth` and swap.  The last stage leaves its outputs in o[q] =
+// X[t + TPF q].
+template <typename C, int M, int NS, int TPF, int SIGN>
+__device__ __forceinline__ void col_tail(C *cur, C *oth, const C *tw, int t, C (&o)[16]) {
+  if constexpr (M / NS > 16) {
+    C v[16];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r] = cur[fpad(t + r * TPF)];
+    const int k = t & (NS - 1);
+    constexpr int off = TwOffset<NS>::value;
+#pragma unroll
+    for (int r = 1; r < 16; ++r) {
+      C w = tw[off + (r - 1) * NS + k];
+      if (SIGN < 0) w.y = -w.y;
+      v[r] = cmul(v[r], w);
+    }
+    dft_reg<16>(v, SIGN);
+    const int d = (t / NS) * NS * 16 + k;
+#pragma unroll
+    for (int r = 0; r < 16; ++r) oth[fpad(d + r * NS)] = v[r];
+    __syncthreads();
+    col_tail<C, M, NS * 16, TPF, SIGN>(oth, cur, tw, t, o);
+  } else {
+    constexpr int RL = M / NS, IT = 16 / RL;
+    constexpr int off = TwOffset<NS>::value;
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+      const int j = t + TPF * it;  // < NS: the stage's k is j itself
+      C v[RL];
+#pragma unroll
+      for (int r = 0; r < RL; ++r) v[r] = cur[fpad(j + r * NS)];
+#pragma unroll
+      for (int r = 1; r < RL; ++r) {
+        C w = tw[off + (r - 1) * NS + j];
+        if (SIGN < 0) w.y = -w.y;
+        v[r] = cmul(v[r], w);
+      }
+      dft_reg<RL>(v, SIGN);
+#pragma unroll
+      for (int r = 0; r < RL; ++r) o[it + r * IT] = v[r];
+    }
+  }
 }
 
+// Number of middle (radix-16, not last) stages of an M-point transform.
+template <int M>
+struct ColMid {
+  static constexpr int count() {
+    int n = 0;
+    for (int NS = 16; M / NS > 16; NS *= 16) ++n;
+    return n;
+  }
+  static constexpr int value = count();
+};
+
+// v[q] = x[t + TPF q] -> o[q] = X[t + TPF q].  S and O are the group's two
+// buffers; with an even number of middle stages the last stage reads S, so
+// the caller alternates S between consecutive transforms.
+template <typename C, int M, int TPF, int SIGN>
+__device__ __forceinline__ void col_fft(C (&v)[16], C *S, C *O, const C *tw, int t, C (&o)[16]) {
+  dft_reg<16>(v, SIGN);
+#pragma unroll
+  for (int r = 0; r < 16; ++r) S[fpad(16 * t + r)] = v[r];
+  __syncthreads();
+  col_tail<C, M, 16, TPF, SIGN>(S, O, tw, t, o);
+}
+
+// Twist factor exp(+2 pi i u k2 / nu) of slot b = t + TPF q, u = b or b - M
+// (the negative half of the band), as base(k2, t) * tq(k2, q, neg); both
+// tables are exact FP64 values rounded to R.
+template <typename C, int TPF>
+__device__ __forceinline__ C col_twist(const ColArgs &a, const C *twB, const C *twQ, int k2,
+                                       int t, int q, int M, C base) {
+  const int b = t + TPF * q;
+  const int neg = (!a.band_full && b >= M - a.L) ? 1 : 0;
+  return cmul(__ldg(&twQ[(k2 * 16 + q) * 2 + neg]), base);
+}
+
+// Shared memory of a column CTA: two padded buffers per column, then the
+// M stage twiddles.
+template <typename R, int M>
+struct ColSmem2 {
+  static constexpr size_t bytes() {
+    return (size_t(2) * ColCfg<R, M>::NB * FftBuf<M>::value + M) * 2 * sizeof(R);
+  }
+};
+
 // ms2dirty direction: band rows (after the v transform) -> H image rows,
-// backward (+) transform along u.
+// backward (+) transform along u, for NB adjacent image columns j and plane lp.
 template <typename R, int LOGM>
-__global__ void __launch_bounds__(ColCfg<R, (1 << LOGM)>::THREADS) k_ucol_bwd(ColArgs a) {
+__global__ void __launch_bounds__(ColCfg<R, (1 << LOGM)>::THREADS, ColCfg<R, (1 << LOGM)>::MINB)
+k_ucol_bwd(ColArgs a) {
   using C = typename Cplx<R>::type;
   constexpr int M = 1 << LOGM, TPF = ColCfg<R, M>::TPF, NB = ColCfg<R, M>::NB;
   constexpr int BL = FftBuf<M>::value;
+  constexpr bool kFlip = (ColMid<M>::value % 2) == 0;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *bufall = reinterpret_cast<C *>(smem_raw);
-  C *tws = bufall + NB * BL;
+  C *tws = bufall + 2 * NB * BL;
   const int grp = threadIdx.x / TPF, t = threadIdx.x - grp * TPF;
-  C *buf = bufall + grp * BL;
+  C *A = bufall + 2 * grp * BL, *B = A + BL;
   const int lp = blockIdx.y;
   const int j = blockIdx.x * NB + grp;
   const bool jv = j < a.ny;
   const C *band = reinterpret_cast<const C *>(a.band);
-  const C *twnu = reinterpret_cast<const C *>(a.twnu);
+  const C *twB = reinterpret_cast<const C *>(a.twB);
+  const C *twQ = reinterpret_cast<const C *>(a.twQ);
   C *H = reinterpret_cast<C *>(a.H);
   for (int i = threadIdx.x; i < M; i += blockDim.x) tws[i] = reinterpret_cast<const C *>(a.twM)[i];
-  // coalesced load (slot-major, adjacent image columns innermost), eight
-  // loads in flight per thread before the shared-memory stores
-  constexpr int ITEMS = NB * M / ColCfg<R, M>::THREADS;  // 16 per thread
-  static_assert(ITEMS % 8 == 0, "load batching");
-#pragma unroll 1
-  for (int i0 = 0; i0 < ITEMS; i0 += 8) {
-    C val[8];
+  // coalesced load (slot-major, adjacent image columns innermost) into the
+  // A buffers, all sixteen loads of a thread in flight together
+  constexpr int ITEMS = NB * M / ColCfg<R, M>::THREADS;  // 16
+  {
+    C val[ITEMS];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const int item = threadIdx.x + (i0 + q) * blockDim.x;
+    for (int q = 0; q < ITEMS; ++q) {
+      const int item = threadIdx.x + q * blockDim.x;
       const int c = item % NB, b = item / NB;
       const int jj = blockIdx.x * NB + c;
       val[q].x = R(0);
@@ -1080,36 +1164,40 @@ __global__ void __launch_bounds__(ColCfg<R, (1 << LOGM)>::THREADS) k_ucol_bwd(Co
       }
     }
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const int item = threadIdx.x + (i0 + q) * blockDim.x;
-      bufall[(item % NB) * BL + fpad(item / NB)] = val[q];
+    for (int q = 0; q < ITEMS; ++q) {
+      const int item = threadIdx.x + q * blockDim.x;
+      bufall[(item % NB) * 2 * BL + fpad(item / NB)] = val[q];
     }
   }
   __syncthreads();
   C g[16];
 #pragma unroll
-  for (int r = 0; r < 16; ++r) g[r] = buf[fpad(t + TPF * r)];
+  for (int q = 0; q < 16; ++q) g[q] = A[fpad(t + TPF * q)];
   __syncthreads();
+  C *rowp = H + (size_t(lp) * a.ny + j) * a.nx;
+  const int half_nu = a.nu / 2, half_nx = a.nx / 2;
   for (int k2 = 0; k2 < a.K; ++k2) {
+    C v[16];
+    if (k2 == 0) {
 #pragma unroll
-    for (int r = 0; r < 16; ++r) {
-      const int b = t + TPF * r;
-      const int u = slot_u(a, b, M);
-      C val = g[r];
-      if (k2 != 0 && u < (1 << 29)) val = cmul(val, twnu[twist_index(u, k2, a.nu)]);
-      buf[fpad(b)] = val;
-    }
-    __syncthreads();
-    FftStages<C, M, 1, TPF>::run(buf, tws, t, +1);
+      for (int q = 0; q < 16; ++q) v[q] = g[q];
+    } else {
+      const C base = __ldg(&twB[k2 * TPF + t]);
 #pragma unroll
-    for (int r = 0; r < 16; ++r) {
-      const int k1 = t + TPF * r;
-      const int k = a.K * k1 + k2;
-      const int ks = (k < a.nu / 2) ? k : k - a.nu;
-      const int i = ks + a.nx / 2;
-      if (jv && i >= 0 && i < a.nx) H[(size_t(lp) * a.ny + j) * a.nx + i] = buf[fpad(k1)];
+      for (int q = 0; q < 16; ++q) v[q] = cmul(g[q], col_twist<C, TPF>(a, twB, twQ, k2, t, q, M, base));
     }
-    __syncthreads();
+    C *S = (kFlip && (k2 & 1)) ? B : A;
+    C *O = (kFlip && (k2 & 1)) ? A : B;
+    C o[16];
+    col_fft<C, M, TPF, +1>(v, S, O, tws, t, o);
+    if (jv) {
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const int k = a.K * (t + TPF * q) + k2;
+        const int i = (k < half_nu ? k : k - a.nu) + half_nx;
+        if (i >= 0 && i < a.nx) rowp[i] = o[q];
+      }
+    }
   }
 }
 
@@ -1117,57 +1205,65 @@ __global__ void __launch_bounds__(ColCfg<R, (1 << LOGM)>::THREADS) k_ucol_bwd(Co
 // image columns, forward (-) transform along u.  Band entries of other
 // columns are left untouched (zeroed by the caller).
 template <typename R, int LOGM>
-__global__ void __launch_bounds__(ColCfg<R, (1 << LOGM)>::THREADS) k_ucol_fwd(ColArgs a) {
+__global__ void __launch_bounds__(ColCfg<R, (1 << LOGM)>::THREADS, ColCfg<R, (1 << LOGM)>::MINB)
+k_ucol_fwd(ColArgs a) {
   using C = typename Cplx<R>::type;
   constexpr int M = 1 << LOGM, TPF = ColCfg<R, M>::TPF, NB = ColCfg<R, M>::NB;
   constexpr int BL = FftBuf<M>::value;
+  constexpr bool kFlip = (ColMid<M>::value % 2) == 0;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *bufall = reinterpret_cast<C *>(smem_raw);
-  C *tws = bufall + NB * BL;
+  C *tws = bufall + 2 * NB * BL;
   const int grp = threadIdx.x / TPF, t = threadIdx.x - grp * TPF;
-  C *buf = bufall + grp * BL;
+  C *A = bufall + 2 * grp * BL, *B = A + BL;
   const int lp = blockIdx.y;
   const int j = blockIdx.x * NB + grp;
   const bool jv = j < a.ny;
   C *band = reinterpret_cast<C *>(a.band);
-  const C *twnu = reinterpret_cast<const C *>(a.twnu);
-  const C *H = reinterpret_cast<const C *>(a.H);
+  const C *twB = reinterpret_cast<const C *>(a.twB);
+  const C *twQ = reinterpret_cast<const C *>(a.twQ);
+  const C *rowp = reinterpret_cast<const C *>(a.H) + (size_t(lp) * a.ny + (jv ? j : 0)) * a.nx;
   for (int i = threadIdx.x; i < M; i += blockDim.x) tws[i] = reinterpret_cast<const C *>(a.twM)[i];
+  const int half_nu = a.nu / 2, half_nx = a.nx / 2;
   C acc[16];
 #pragma unroll
-  for (int r = 0; r < 16; ++r) acc[r].x = acc[r].y = R(0);
+  for (int q = 0; q < 16; ++q) acc[q].x = acc[q].y = R(0);
   for (int k2 = 0; k2 < a.K; ++k2) {
+    C v[16];
 #pragma unroll
-    for (int r = 0; r < 16; ++r) {
-      const int k1 = t + TPF * r;
-      const int k = a.K * k1 + k2;
-      const int ks = (k < a.nu / 2) ? k : k - a.nu;
-      const int i = ks + a.nx / 2;
-      C val;
-      val.x = R(0);
-      val.y = R(0);
-      if (jv && i >= 0 && i < a.nx) val = H[(size_t(lp) * a.ny + j) * a.nx + i];
-      buf[fpad(k1)] = val;
+    for (int q = 0; q < 16; ++q) {
+      const int k = a.K * (t + TPF * q) + k2;
+      const int i = (k < half_nu ? k : k - a.nu) + half_nx;
+      v[q].x = R(0);
+      v[q].y = R(0);
+      if (jv && i >= 0 && i < a.nx) v[q] = rowp[i];
     }
-    __syncthreads();
-    FftStages<C, M, 1, TPF>::run(buf, tws, t, -1);
+    C *S = (kFlip && (k2 & 1)) ? B : A;
+    C *O = (kFlip && (k2 & 1)) ? A : B;
+    if (k2 == 0) __syncthreads();  // the stage table is in place
+    C o[16];
+    col_fft<C, M, TPF, -1>(v, S, O, tws, t, o);
+    if (k2 == 0) {
 #pragma unroll
-    for (int r = 0; r < 16; ++r) {
-      const int b = t + TPF * r;
-      const int u = slot_u(a, b, M);
-      C val = buf[fpad(b)];
-      if (k2 != 0 && u < (1 << 29)) {
-        C w = twnu[twist_index(u, k2, a.nu)];
-        w.y = -w.y;
-        val = cmul(val, w);
+      for (int q = 0; q < 16; ++q) {
+        acc[q].x += o[q].x;
+        acc[q].y += o[q].y;
       }
-      acc[r].x += val.x;
-      acc[r].y += val.y;
-    }
-    __syncthreads();
-  }
+    } else {
+      const C base = __ldg(&twB[k2 * TPF + t]);
 #pragma unroll
-  for (int r = 0; r < 16; ++r) buf[fpad(t + TPF * r)] = acc[r];
+      for (int q = 0; q < 16; ++q) {
+        C w = col_twist<C, TPF>(a, twB, twQ, k2, t, q, M, base);
+        w.y = -w.y;
+        const C val = cmul(o[q], w);
+        acc[q].x += val.x;
+        acc[q].y += val.y;
+      }
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < 16; ++q) A[fpad(t + TPF * q)] = acc[q];
   __syncthreads();
   for (int item = threadIdx.x; item < NB * M; item += blockDim.x) {
     const int c = item % NB, b = item / NB;
@@ -1176,7 +1272,7 @@ __global__ void __launch_bounds__(ColCfg<R, (1 << LOGM)>::THREADS) k_ucol_fwd(Co
     if (jj < a.ny && u < (1 << 29)) {
       int jx = jj + a.nv - a.ny / 2;
       jx -= (jx >= a.nv) ? a.nv : 0;
-      band[(size_t(slot_bi(a, u)) * a.P + lp) * a.nv + jx] = bufall[c * BL + fpad(b)];
+      band[(size_t(slot_bi(a, u)) * a.P + lp) * a.nv + jx] = bufall[c * 2 * BL + fpad(b)];
     }
   }
 }
