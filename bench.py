@@ -58,7 +58,56 @@ def parse_args():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-clocks", action="store_true",
                     help="do not sample nvidia-smi during the timed region")
+    ap.add_argument("--timed-only", action="store_true",
+                    help="stop after the timed region (for profiler launch lists)")
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="fraction of the 997 timesteps (small cases for ncu captures)")
+    ap.add_argument("--launch-summary", metavar="CSV",
+                    help="summarise an ncu launch list (gpu__time_duration.sum) of a "
+                         "--timed-only run: per kernel launches, time and share over the "
+                         "last --steps steps, then exit")
     return ap.parse_args()
+
+
+def launch_summary(path, steps):
+    """Per-kernel totals of the last `steps` steps (two gridder calls each,
+    each starting with k_scan) of an ncu --csv launch list."""
+    import collections
+    import csv
+    rows = list(csv.reader(open(path)))
+    hi = next(i for i, r in enumerate(rows) if "Kernel Name" in r)
+    h = rows[hi]
+    ki, vi, ui = h.index("Kernel Name"), h.index("Metric Value"), h.index("Metric Unit")
+    scale = {"nsecond": 1e-6, "usecond": 1e-3, "msecond": 1.0, "second": 1e3}
+    launches = [(r[ki], float(r[vi].replace(",", "")) * scale.get(r[ui], 1e-6))
+                for r in rows[hi + 1:] if len(r) > vi and r[vi]]
+    starts = [i for i, (k, _) in enumerate(launches) if "k_scan" in k]
+    seg = launches[starts[-2 * steps]:] if len(starts) >= 2 * steps else launches
+    tot = collections.OrderedDict()
+    for k, ms in seg:
+        name = k.split("(")[0].replace("void ", "")
+        c = tot.setdefault(name, [0, 0.0])
+        c[0] += 1
+        c[1] += ms
+    T = sum(v for _, v in tot.values())
+    print(f"{'kernel':72s} {'launches':>8s} {'ms':>8s} {'share':>6s}")
+    for k, (n, ms) in sorted(tot.items(), key=lambda x: -x[1][1]):
+        print(f"{k[:72]:72s} {n:8d} {ms:8.3f} {100 * ms / T:5.1f}%")
+    print(f"total {T:.3f} ms over {sum(n for n, _ in tot.values())} launches in {steps} step(s)")
+
+
+def profiled_traffic():
+    """DRAM bytes per step (read + write, all kernels of one ms2dirty +
+    dirty2ms) from the committed ncu summary, or None."""
+    path = os.path.join(HERE, "profiles", "pipeline_traffic_config2.txt")
+    try:
+        with open(path) as fh:
+            for line in fh:
+                if line.startswith("traffic_bytes_per_step:"):
+                    return int(line.split(":", 1)[1].strip())
+    except OSError:
+        pass
+    return None
 
 
 def algorithmic_bytes(nvis, nrows, nx, ny, grid, s_vis, s_grid):
@@ -122,9 +171,9 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def workload():
+def workload(scale=1.0):
     from wsclean_b200 import synth
-    c = synth.config2()
+    c = synth.config2(scale=scale)
     rng = np.random.default_rng(12)
     nx = c["npix_x"]
     ix, iy, flux = synth.point_sky(c["nsrc"], nx, nx, rng)
@@ -153,7 +202,7 @@ def run_reference(args, world, rank):
     if not O.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "compiled reference (oracle/_ref) missing"}))
         return
-    c, ix, iy, flux = workload()
+    c, ix, iy, flux = workload(args.scale)
     from wsclean_b200 import synth
     uvw, freq, nx, px = c["uvw"], c["freq"], c["npix_x"], c["pixsize"]
     nvis = uvw.shape[0] * len(freq)
@@ -224,7 +273,7 @@ def run_ours(args, world, rank, local, pg):
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    c, ix, iy, flux = workload()
+    c, ix, iy, flux = workload(args.scale)
     uvw, freq, nx, px = c["uvw"], c["freq"], c["npix_x"], c["pixsize"]
     nrows, nchan = uvw.shape[0], len(freq)
     nvis = nrows * nchan
@@ -272,6 +321,7 @@ def run_ours(args, world, rank, local, pg):
         phases = {}
         l0 = ctx.stats()["kernel_launches"]
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        step_ms = []
         for _ in range(steps):
             # the library runs on its own stream and synchronises before
             # returning, so events on the current stream bracket each call
@@ -288,6 +338,7 @@ def run_ours(args, world, rank, local, pg):
             torch.cuda.synchronize(dev)
             t_ms += ev[0].elapsed_time(ev[1])
             t_dm += ev[1].elapsed_time(ev[2])
+            step_ms.append(round(ev[0].elapsed_time(ev[2]), 3))
             for k in ("ms_prep", "ms_grid", "ms_fft", "ms_screen", "ms_total"):
                 phases.setdefault("ms2dirty_" + k, []).append(st1[k])
                 phases.setdefault("dirty2ms_" + k, []).append(st2[k])
@@ -297,24 +348,35 @@ def run_ours(args, world, rank, local, pg):
         if pg is not None:
             pg.all_reduce(tt, op=pg.ReduceOp.MAX)
         t_ms, t_dm = float(tt[0]), float(tt[1])
-        return t_ms, t_dm, {k: statistics.median(v) for k, v in phases.items()}, launches, st1, st2
+        phases = {k: statistics.median(v) for k, v in phases.items()}
+        return t_ms, t_dm, phases, launches, st1, st2, step_ms
 
     # ---- timed region (mixed, the headline)
     sampler = ClockSampler(local)
     if not args.no_clocks:
         sampler.start()
-    t_ms, t_dm, phases, launches, st1, st2 = timed("mixed", args.steps, args.warmup)
+    t_ms, t_dm, phases, launches, st1, st2, step_ms = timed("mixed", args.steps, args.warmup)
     clocks = sampler.stop()
     ms_per_step = (t_ms + t_dm) / args.steps
     value = world * nvis * args.steps / ((t_ms + t_dm) / 1e3) / 1e6
     grid_info = {"nu": st1["nu"], "nv": st1["nv"], "nplanes": st1["nplanes"], "W": st1["supp"],
                  "sigma": round(st1["sigma"], 4), "u_band_rows": st1["band_rows"]}
 
+    if args.timed_only:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                              "steps": args.steps, "warmup": args.warmup,
+                              "ms_per_step": ms_per_step, "step_ms": step_ms,
+                              "timed_only": True, "scale": args.scale, "grid": grid_info,
+                              "phases_ms": phases, "gpu_launches": launches}))
+        ctx.close()
+        return
+
     # ---- FP64 plain form (same workload)
     fp64 = None
     if not args.no_fp64:
         k64 = max(2, args.steps // 3)
-        t64_ms, t64_dm, ph64, _, s64, _ = timed("fp64", k64, 1)
+        t64_ms, t64_dm, ph64, _, s64, _, _ = timed("fp64", k64, 1)
         fp64 = {"value": world * nvis * k64 / ((t64_ms + t64_dm) / 1e3) / 1e6,
                 "ms2dirty_mvis_s": world * nvis * k64 / (t64_ms / 1e3) / 1e6,
                 "dirty2ms_mvis_s": world * nvis * k64 / (t64_dm / 1e3) / 1e6,
@@ -426,11 +488,12 @@ def run_ours(args, world, rank, local, pg):
             "mixed_over_fp64": (value / fp64["value"]) if fp64 else None,
             "accuracy": acc,
             "phases_ms": phases,
+            "step_ms": step_ms,
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "roofline": {"bound": "hbm", "kernel": "ms2dirty+dirty2ms pipeline",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak, "traffic": profiled_traffic(),
                          "peak_source": peak_src,
                          "bytes_per_step": B},
             "cpu_baseline": cpu,
@@ -443,6 +506,9 @@ def run_ours(args, world, rank, local, pg):
 
 def main():
     args = parse_args()
+    if args.launch_summary:
+        launch_summary(args.launch_summary, args.steps)
+        return
     world, rank, local, pg = dist_setup(args)
     try:
         if args.impl == "reference":

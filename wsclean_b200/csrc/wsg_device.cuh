@@ -13,8 +13,10 @@
 //               footprint origin repeats, commit to a shared-memory tile, and
 //               flush the tile to the u-band grid with vector atomics
 //                                                             (x2grid_c_helper/HelperX2g2, wgridder.h:934-1031,1142-1236)
-//   cuFFT       pruned 2-D backward FFT per plane (band rows along v, image
-//               columns along u)                              (grid2dirty_c_overwrite_wscreen_add, :496-534)
+//   cuFFT       backward FFT along v of the occupied u band (all planes of a pass)
+//   k_ucol_bwd  pruned backward FFT along u of the image columns only: nu = K M,
+//               K twisted M-point FFTs per column, band in, image rows out
+//                                                             (grid2dirty_c_overwrite_wscreen_add, :496-534)
 //   k_screen    sum over planes of Re(grid * w-screen), FP64, times the grid
 //               correction, added into the FP64 image         (grid2dirty_post2 :428-484, apply_global_corrections :1348-1400)
 #pragma once
