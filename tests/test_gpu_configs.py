@@ -1,0 +1,151 @@
+"""Parity on the geometries of the four other benchmark configurations (the
+headline bench runs config 2):
+
+* config 1 at full size: 2.9M complex128 visibilities, 1024^2 at 10",
+  epsilon 1e-12, FP64 -- against the FP64 DFT and the reference w-gridder;
+* config 3 at full size: the chi^2 gradient at 2048^2 / 8" with Briggs
+  (robust 0) x U[0.5, 2] noise weights and a 5%-perturbed model, against
+  central finite differences (h = 1e-3 Jy, 64 pixels, tolerance 1e-4) and
+  the gradient computed with the reference w-gridder;
+* config 4: facets of the seeded Voronoi tessellation (512^2 .. 2048^2 boxes,
+  phase centre at the box centre) on output channels of 8 input channels,
+  over a quarter of the observation;
+* config 5: the 8192^2 / 2" wide-field geometry with |w| up to 40% of
+  max|uv| on a 2% time subsample (10.4M visibilities), against the DFT on
+  64 pixels and on a 20k-visibility subsample."""
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+KW = dict(negate_v=True, divide_by_n=False, sigma_min=1.1, sigma_max=2.0)
+
+
+@pytest.fixture(scope="module")
+def G():
+    from wsclean_b200 import gridder
+    return gridder
+
+
+def test_config1_fp64_full(G):
+    from wsclean_b200 import synth
+    c = synth.config1()
+    uvw, freq, nx, px = c["uvw"], c["freq"], c["npix_x"], c["pixsize"]
+    rng = np.random.default_rng(1)
+    ix, iy, flux = synth.point_sky(c["nsrc"], nx, nx, rng)
+    vis = synth.predict_vis(uvw, freq, nx, nx, px, px, ix, iy, flux, device="cuda:0")
+    vis = vis + 0.1 * (rng.normal(size=vis.shape) + 1j * rng.normal(size=vis.shape))
+    assert vis.size == 2_903_040 and vis.dtype == np.complex128
+    d = G.ms2dirty(uvw, freq, vis, nx, nx, px, px, 1e-12, precision="fp64",
+                   dirty_dtype=np.float64, **KW)
+    pix = rng.integers(0, nx * nx, 64)
+    ref = O.dft_ms2dirty(uvw, freq, vis, nx, nx, px, px, pixels=pix, negate_v=True,
+                         divide_by_n=False)
+    assert O.rel_rms(d.ravel()[pix], ref) < 1e-11
+    if O.ref_available():
+        dr = O.ref_ms2dirty(uvw, freq, vis, nx, nx, px, px, 1e-12, prec="double")
+        assert O.rel_rms(d, dr) < 1e-11
+    model = synth.sky_image(nx, nx, ix, iy, flux)
+    v = G.dirty2ms(uvw, freq, model, px, px, 1e-12, precision="fp64", vis_dtype=np.complex128,
+                   **KW)
+    sel = rng.choice(vis.size, 10000, replace=False)
+    vref = O.dft_dirty2ms(uvw, freq, model, px, px, negate_v=True, divide_by_n=False, select=sel)
+    assert O.rel_rms(v.ravel()[sel], vref) < 1e-11
+
+
+def test_config3_gradient_full(G):
+    from wsclean_b200 import synth
+    from wsclean_b200.interface import ImagingParameters, Operator, chi2
+    c = synth.config3()
+    uvw, freq, nx, px = c["uvw"], c["freq"], c["npix_x"], c["pixsize"]
+    rng = np.random.default_rng(3)
+    ix, iy, flux = synth.point_sky(c["nsrc"], nx, nx, rng)
+    vis = synth.predict_vis(uvw, freq, nx, nx, px, px, ix, iy, flux, device="cuda:0")
+    noise = rng.uniform(0.5, 2.0, vis.shape)
+    w = noise * synth.briggs_weights(uvw, freq, nx, nx, px, px, robust=0.0, noise_weights=noise)
+    sky = synth.sky_image(nx, nx, ix, iy, flux)
+    model = sky * (1 + 0.05 * rng.normal(size=sky.shape))
+    p = ImagingParameters(uvw, freq, nx, nx, px, px, epsilon=1e-10, precision="fp64")
+    dev = torch.device("cuda", 0)
+    V, Wt = torch.as_tensor(vis, device=dev), torch.as_tensor(w, device=dev)
+    h = 1e-3
+    with Operator(p) as op:
+        x = torch.as_tensor(model, device=dev).requires_grad_(True)
+        chi2(op, x, V, Wt).backward()
+        grad = x.grad.cpu().numpy()
+        # half the pixels at sources (large gradients), half at random
+        src = np.flatnonzero(sky.ravel())
+        pix = np.concatenate([rng.choice(src, 32, replace=False), rng.integers(0, nx * nx, 32)])
+        fd = []
+        for k in pix:
+            e = torch.zeros(nx * nx, dtype=torch.float64, device=dev)
+            e[k] = h
+            e = e.reshape(nx, nx)
+            with torch.no_grad():
+                fd.append((chi2(op, x + e, V, Wt).item() - chi2(op, x - e, V, Wt).item()) / (2 * h))
+    fd = np.array(fd)
+    g = grad.ravel()[pix]
+    assert np.max(np.abs(g - fd)) / np.max(np.abs(fd)) < 1e-4
+    if O.ref_available():
+        kw = dict(KW, prec="double")
+        Ax = O.ref_dirty2ms(uvw, freq, model, px, px, 1e-10, vis_dtype=np.complex128, **kw)
+        gref = -2.0 * O.ref_ms2dirty(uvw, freq, w * (vis - Ax), nx, nx, px, px, 1e-10, **kw)
+        assert O.rel_rms(grad, gref) < 1e-7
+
+
+@pytest.mark.parametrize("prec,eps,tol", [("mixed", 1e-5, 1e-5), ("fp64", 1e-10, 1e-9)])
+def test_config4_facets(G, prec, eps, tol):
+    from wsclean_b200 import synth
+    c = synth.config4(scale=0.25)
+    uvw, freq, px = c["uvw"], c["freq"], c["pixsize"]
+    facets = synth.facets4()
+    sizes = [f["nx"] * f["ny"] for f in facets]
+    pick = [int(np.argmin(sizes)), int(np.argmax(sizes)), 5]
+    rng = np.random.default_rng(44)
+    for oc in (0, 7):
+        fr = freq[8 * oc:8 * oc + 8]
+        vis = (rng.normal(size=(len(uvw), 8)) + 1j * rng.normal(size=(len(uvw), 8)))
+        vis = vis.astype(np.complex64 if prec == "mixed" else np.complex128)
+        for fi in pick:
+            f = facets[fi]
+            cx, cy = f["dx"] * px, f["dy"] * px
+            d = G.ms2dirty(uvw, fr, vis, f["nx"], f["ny"], px, px, eps, precision=prec,
+                           center_x=cx, center_y=cy, dirty_dtype=np.float64, **KW)
+            pix = rng.integers(0, f["nx"] * f["ny"], 48)
+            ref = O.dft_ms2dirty(uvw, fr, vis, f["nx"], f["ny"], px, px, pixels=pix,
+                                 negate_v=True, divide_by_n=False, center_x=cx, center_y=cy)
+            assert O.rel_rms(d.ravel()[pix], ref) < tol, (oc, fi)
+            model = np.zeros((f["nx"], f["ny"]))
+            model[rng.integers(0, f["nx"], 30), rng.integers(0, f["ny"], 30)] = rng.uniform(0.1, 5, 30)
+            v = G.dirty2ms(uvw, fr, model, px, px, eps, precision=prec, center_x=cx, center_y=cy,
+                           vis_dtype=np.complex128, **KW)
+            sel = rng.choice(v.size, 5000, replace=False)
+            vref = O.dft_dirty2ms(uvw, fr, model, px, px, negate_v=True, divide_by_n=False,
+                                  center_x=cx, center_y=cy, select=sel)
+            assert O.rel_rms(v.ravel()[sel], vref) < tol, (oc, fi)
+
+
+def test_config5_widefield_subsample(G):
+    from wsclean_b200 import synth
+    c = synth.config5(scale=0.02)
+    uvw, freq, nx, px = c["uvw"], c["freq"], c["npix_x"], c["pixsize"]
+    rng = np.random.default_rng(5)
+    nvis = uvw.shape[0] * len(freq)
+    assert nvis > 10_000_000
+    dev = torch.device("cuda", 0)
+    vis = torch.complex(torch.randn(uvw.shape[0], len(freq), device=dev),
+                        torch.randn(uvw.shape[0], len(freq), device=dev))
+    d = G.ms2dirty(uvw, freq, vis, nx, nx, px, px, 1e-5, dirty_dtype=np.float64, **KW)
+    pix = rng.integers(0, nx * nx, 64)
+    ref = O.dft_ms2dirty(uvw, freq, vis.cpu().numpy(), nx, nx, px, px, pixels=pix,
+                         negate_v=True, divide_by_n=False)
+    assert O.rel_rms(d.cpu().numpy().ravel()[pix], ref) < 1e-5
+    ix, iy, flux = synth.point_sky(c["nsrc"], nx, nx, rng)
+    model = synth.sky_image(nx, nx, ix, iy, flux) + synth.gaussian_blobs(nx, nx, c["ngauss"], rng)
+    v = G.dirty2ms(uvw, freq, torch.as_tensor(model, device=dev), px, px, 1e-5,
+                   vis_dtype=np.complex128, **KW)
+    sel = rng.choice(nvis, 20000, replace=False)
+    vref = O.dft_dirty2ms(uvw, freq, model, px, px, negate_v=True, divide_by_n=False, select=sel)
+    assert O.rel_rms(v.cpu().numpy().ravel()[sel], vref) < 1e-5

@@ -157,6 +157,77 @@ def config1(scale=1.0, npix=1024):
                 pixsize=10.0 * ARCSEC, nsrc=20)
 
 
+def config3(scale=1.0, npix=2048, pixsize_arcsec=8.0):
+    """The config-2 array and sky imaged at 2048^2 and 8" pixels (the
+    chi^2-gradient configuration); Briggs weights come from briggs_weights."""
+    return config2(scale=scale, npix=npix, pixsize_arcsec=pixsize_arcsec)
+
+
+def config4(scale=1.0):
+    """96 antennas within 10 km, 1 h at 10 s (360 timesteps), 64 channels at
+    120-180 MHz, dec -30 deg; a 4096^2 field of 10" pixels cut into the 16
+    facets of facets4().  Each of the 8 output channels covers 8 input
+    channels."""
+    nt = max(2, int(round(360 * scale)))
+    freq = 120e6 + (np.arange(64) + 0.5) * (60e6 / 64)
+    uvw, freq, rng = observation(96, 10000.0, None, 10.0, -30.0, freq, seed=4, ntimes=nt)
+    return dict(uvw=uvw, freq=freq, rng=rng, npix_x=4096, npix_y=4096,
+                pixsize=10.0 * ARCSEC, nsrc=200, out_channels=8)
+
+
+def facets4(npix=4096, nfacets=16, seed=4, min_box=512, max_box=2048):
+    """Seeded Voronoi facets of an npix^2 field: for each site, the bounding
+    box of its Voronoi cell (on a coarse raster), its sides clamped to
+    [min_box, max_box] and made even.  Returns a list of dicts with the box
+    size (nx, ny) and its centre offset from the field centre in pixels
+    (dx, dy): the facet's phase centre is l = dx * pixsize, m = dy * pixsize."""
+    rng = np.random.default_rng(seed)
+    sites = rng.uniform(0, npix, (nfacets, 2))
+    step = 16
+    g = (np.arange(0, npix, step) + step / 2)
+    X, Y = np.meshgrid(g, g, indexing="ij")
+    d2 = (X[..., None] - sites[:, 0]) ** 2 + (Y[..., None] - sites[:, 1]) ** 2
+    owner = np.argmin(d2, axis=-1)
+    out = []
+    for f in range(nfacets):
+        xs, ys = X[owner == f], Y[owner == f]
+        x0, x1 = xs.min() - step / 2, xs.max() + step / 2
+        y0, y1 = ys.min() - step / 2, ys.max() + step / 2
+        nx = int(np.clip(x1 - x0, min_box, max_box)) // 2 * 2
+        ny = int(np.clip(y1 - y0, min_box, max_box)) // 2 * 2
+        cx, cy = 0.5 * (x0 + x1), 0.5 * (y0 + y1)
+        out.append(dict(nx=nx, ny=ny, dx=cx - npix / 2, dy=cy - npix / 2))
+    return out
+
+
+def config5(scale=1.0):
+    """256 antennas with log-radial radii out to 20 km, 1000 timesteps at 8 s,
+    16 channels at 140-190 MHz, dec -30 deg, |w| up to 40% of max|uv|;
+    8192^2 at 2" (about 522M visibilities at scale 1)."""
+    nt = max(2, int(round(1000 * scale)))
+    freq = np.linspace(140e6, 190e6, 16)
+    uvw, freq, rng = observation(256, 20000.0, None, 8.0, -30.0, freq, seed=5, wfrac=0.4,
+                                 log_radial=True, ntimes=nt)
+    return dict(uvw=uvw, freq=freq, rng=rng, npix_x=8192, npix_y=8192,
+                pixsize=2.0 * ARCSEC, nsrc=2000, ngauss=5)
+
+
+def gaussian_blobs(npix_x, npix_y, n, rng, sigma_px=(2.0, 8.0), flux=(0.5, 5.0)):
+    """n seeded Gaussian extended sources as a pixel image (each truncated
+    at 4 sigma)."""
+    img = np.zeros((npix_x, npix_y))
+    for _ in range(n):
+        s = rng.uniform(*sigma_px)
+        cx = rng.uniform(0.2, 0.8) * npix_x
+        cy = rng.uniform(0.2, 0.8) * npix_y
+        h = int(np.ceil(4 * s))
+        ix = np.arange(int(cx) - h, int(cx) + h + 1)
+        iy = np.arange(int(cy) - h, int(cy) + h + 1)
+        g = np.exp(-0.5 * (((ix[:, None] - cx) ** 2 + (iy[None, :] - cy) ** 2) / s ** 2))
+        img[np.ix_(ix, iy)] += rng.uniform(*flux) * g / g.sum()
+    return img
+
+
 def briggs_weights(uvw, freq, nx, ny, px, py, robust=0.0, noise_weights=None):
     """Briggs imaging weights with WSClean's ImageWeights semantics
     (structures/imageweights.cpp:113-143, cell lookup imageweights.h:73-80):
