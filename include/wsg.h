@@ -67,7 +67,9 @@ typedef struct wsg_gridder wsg_gridder;
  * cuFFT plans.  device < 0 selects the current device. */
 int wsg_ctx_create(int device, wsg_ctx **out);
 int wsg_ctx_destroy(wsg_ctx *ctx);
-/* Optional: run on a caller-provided cudaStream_t (passed as void*). */
+/* Optional: run on a caller-provided cudaStream_t (passed as void*); NULL
+ * returns to the context's own stream (pass cudaStreamLegacy for the legacy
+ * default stream).  Work on the stream before a call is ordered before it. */
 int wsg_ctx_set_stream(wsg_ctx *ctx, void *stream);
 /* Releases the cached device buffers and cuFFT plans (they regrow on demand). */
 int wsg_ctx_release_buffers(wsg_ctx *ctx);
@@ -208,6 +210,59 @@ int wsg_plan_grid(const wsg_args *a, size_t nvis, double wmin, double wmax, doub
 /* Message of the last failed call on this thread ("" if none). */
 const char *wsg_last_error(void);
 int wsg_abi_version(void);
+
+/* ------------------------------------------ reusable plans, batched jobs */
+
+/* A plan fixes everything that depends only on the coordinates -- uvw,
+ * freq, weights and mask -- for repeated ms2dirty / dirty2ms calls on new
+ * visibilities or images: the grid and kernel choice, the sort of the
+ * visibilities into uv-tile bins and the per-visibility records (pixel
+ * coordinates, shift phasor and weight).  This is WSClean's major cycle,
+ * which grids (Invert) and degrids (Predict) the same rows many times
+ * (wgridder/wgriddingmsgridder.cpp:135-137,179-181).
+ *
+ * A plan holds one or more jobs sharing the visibilities: facets (each with
+ * its own image size and phase centre, the per-facet direction-dependent
+ * shift of WSClean's faceting) times output channels (each gridding a range
+ * of the input channels).  All jobs share one kernel (W, sigma), chosen for
+ * the largest; their records are drained by a single persistent spread or
+ * interpolation launch, followed by each job's FFTs and w-screen.
+ *
+ * Execution enqueues work on the context's stream and returns without
+ * waiting (wsg_ctx_synchronize waits).  It performs no allocation and no
+ * host synchronisation, so it can be recorded into a CUDA graph by the
+ * caller; when the stream is not being captured, the plan records its own
+ * graph per set of pointers on the second call and replays it afterwards.
+ * vis, dirty and the outputs must be device memory.  A visibility whose
+ * weight or mask is zero contributes nothing (the active set of dirty2ms;
+ * zero-valued visibilities are gridded as zeros).  These entry points
+ * extend the reference's interface; ducc0 re-plans on every call. */
+typedef struct wsg_plan wsg_plan;
+
+typedef struct {
+  size_t npix_x, npix_y;      /* image (facet) size, both even */
+  double center_x, center_y;  /* phase centre of the image, as wsg_args */
+  size_t chan_begin, chan_end;/* input channels [chan_begin, chan_end) */
+} wsg_job;
+
+/* Builds a plan.  a: the common arguments (uvw, freq, nrows, nchan, wgt,
+ * mask, pixel sizes, epsilon, flags, sigma range, precision, vis_type,
+ * dirty_type).  jobs: njobs job descriptions, or NULL for one job over all
+ * channels with a->npix_x, npix_y, center_x, center_y.  The coordinate
+ * arrays are read during the call only. */
+int wsg_plan_create(wsg_ctx *ctx, const wsg_args *a, const wsg_job *jobs, size_t njobs,
+                    wsg_plan **out);
+int wsg_plan_destroy(wsg_plan *p);
+/* dirty[j] = image of job j (npix_x x npix_y of dirty_type, x-major), or
+ * dirty[j] += image when accumulate != 0.  vis: nrows x nchan of vis_type. */
+int wsg_plan_ms2dirty(wsg_plan *p, const void *vis, void *const *dirty, int accumulate);
+/* vis = sum over jobs of the prediction of dirty[j] (each job writes its
+ * channel range; facets of the same channels add up). */
+int wsg_plan_dirty2ms(wsg_plan *p, const void *const *dirty, void *vis);
+/* Grid, kernel and plane choice of job `job` (timings are zero). */
+int wsg_plan_get_stats(const wsg_plan *p, size_t job, wsg_stats *out);
+/* Waits for the work enqueued on the context's stream. */
+int wsg_ctx_synchronize(wsg_ctx *ctx);
 
 #ifdef __cplusplus
 }

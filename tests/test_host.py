@@ -39,8 +39,9 @@ def test_struct_layouts_match_binding(tmp_path):
 #include <stddef.h>
 #include "wsg.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu\n", sizeof(wsg_args), sizeof(wsg_stats), sizeof(wsg_gridder_params),
-         offsetof(wsg_args, dirty_type), offsetof(wsg_stats, kernel_launches));
+  printf("%zu %zu %zu %zu %zu %zu %zu\n", sizeof(wsg_args), sizeof(wsg_stats), sizeof(wsg_gridder_params),
+         offsetof(wsg_args, dirty_type), offsetof(wsg_stats, kernel_launches), sizeof(wsg_job),
+         offsetof(wsg_job, chan_end));
   return 0;
 }''')
     exe = tmp_path / "layout"
@@ -48,7 +49,8 @@ int main(void) {
     out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
     got = [int(x) for x in out]
     want = [ctypes.sizeof(L.WsgArgs), ctypes.sizeof(L.WsgStats), ctypes.sizeof(L.WsgGridderParams),
-            L.WsgArgs.dirty_type.offset, L.WsgStats.kernel_launches.offset]
+            L.WsgArgs.dirty_type.offset, L.WsgStats.kernel_launches.offset,
+            ctypes.sizeof(L.WsgJob), L.WsgJob.chan_end.offset]
     assert got == want
 
 

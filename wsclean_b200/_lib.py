@@ -28,6 +28,8 @@ EXPORTED = [
     "wsg_gridder_initialize_prediction", "wsg_gridder_predict_visibilities",
     "wsg_gridder_ctx", "wsg_get_stats", "wsg_last_error", "wsg_abi_version",
     "wsg_plan_grid", "wsg_ms2dirty_noalloc",
+    "wsg_plan_create", "wsg_plan_destroy", "wsg_plan_ms2dirty", "wsg_plan_dirty2ms",
+    "wsg_plan_get_stats", "wsg_ctx_synchronize",
 ]
 
 c_size_t, c_double, c_int, c_void_p = ctypes.c_size_t, ctypes.c_double, ctypes.c_int, ctypes.c_void_p
@@ -58,6 +60,14 @@ class WsgGridderParams(ctypes.Structure):
         ("nthreads", c_size_t), ("epsilon", c_double),
         ("verbosity", c_size_t), ("tuning", c_int),
         ("precision", c_int), ("device", c_int),
+    ]
+
+
+class WsgJob(ctypes.Structure):
+    _fields_ = [
+        ("npix_x", c_size_t), ("npix_y", c_size_t),
+        ("center_x", c_double), ("center_y", c_double),
+        ("chan_begin", c_size_t), ("chan_end", c_size_t),
     ]
 
 
@@ -127,6 +137,12 @@ def lib():
         L.wsg_ms2dirty_noalloc.argtypes = [P(WsgArgs), vp, vp, vp]
         L.wsg_plan_grid.argtypes = [P(WsgArgs), c_size_t, c_double, c_double, c_double,
                                     c_double, P(WsgStats)]
+        L.wsg_plan_create.argtypes = [vp, P(WsgArgs), P(WsgJob), c_size_t, P(vp)]
+        L.wsg_plan_destroy.argtypes = [vp]
+        L.wsg_plan_ms2dirty.argtypes = [vp, vp, P(vp), c_int]
+        L.wsg_plan_dirty2ms.argtypes = [vp, P(vp), vp]
+        L.wsg_plan_get_stats.argtypes = [vp, c_size_t, P(WsgStats)]
+        L.wsg_ctx_synchronize.argtypes = [vp]
         L.wsg_last_error.restype = ctypes.c_char_p
         L.wsg_abi_version.restype = c_int
         for name in EXPORTED:

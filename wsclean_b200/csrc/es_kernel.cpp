@@ -355,6 +355,7 @@ void choose_grid(GridPlan &g, double sigma_min, double sigma_max, int tile, bool
   size_t bnu = 0, bnv = 0;
   int blogM = 0, bK = 1;
   for (const auto &k : cands) {
+    if (g.force_W && (k.W != g.force_W || std::fabs(k.sigma - g.force_sigma) > 1e-12)) continue;
     GridPlan t = g;
     t.kernel = k;
     if (!pick_nu(g.nx * k.sigma, umax_px, k.W, g.fp32, t.nu, t.logM, t.K)) continue;

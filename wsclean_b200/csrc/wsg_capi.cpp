@@ -14,6 +14,11 @@
 struct wsg_ctx {
   std::unique_ptr<wsg::Context> own;
   wsg::Context *ctx = nullptr;
+  int plans = 0;  // live plans on this context (it must outlive them)
+};
+struct wsg_plan {
+  std::unique_ptr<wsg::Plan> impl;
+  wsg_ctx *ctx = nullptr;
 };
 struct wsg_gridder {
   wsg::Gridder impl;
@@ -87,6 +92,10 @@ int wsg_ctx_create(int device, wsg_ctx **out) {
 }
 
 int wsg_ctx_destroy(wsg_ctx *ctx) {
+  if (ctx && ctx->plans > 0) {
+    g_last_error = "destroy the context's plans first";
+    return WSG_ERR_STATE;
+  }
   return guarded([&] {
     wsg::require(ctx == nullptr || ctx->own != nullptr, "a gridder's context is destroyed with the gridder");
     delete ctx;
@@ -238,6 +247,59 @@ int wsg_plan_grid(const wsg_args *a, size_t nvis, double wmin, double wmax, doub
     out->dw = g.dw;
     out->nshift = g.nshift;
     out->precision = g.fp32 ? WSG_PREC_MIXED : WSG_PREC_FP64;
+  });
+}
+
+int wsg_plan_create(wsg_ctx *ctx, const wsg_args *a, const wsg_job *jobs, size_t njobs,
+                    wsg_plan **out) {
+  return guarded([&] {
+    wsg::require(ctx != nullptr && a != nullptr && out != nullptr, "ctx, args and out are required");
+    auto *h = new wsg_plan;
+    try {
+      h->impl.reset(new wsg::Plan(*ctx->ctx, *a, jobs, njobs));
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    h->ctx = ctx;
+    ++ctx->plans;
+    *out = h;
+  });
+}
+
+int wsg_plan_destroy(wsg_plan *p) {
+  return guarded([&] {
+    if (!p) return;
+    if (p->ctx) --p->ctx->plans;
+    delete p;
+  });
+}
+
+int wsg_plan_ms2dirty(wsg_plan *p, const void *vis, void *const *dirty, int accumulate) {
+  return guarded([&] {
+    wsg::require(p != nullptr, "plan is NULL");
+    p->impl->ms2dirty(vis, dirty, accumulate);
+  });
+}
+
+int wsg_plan_dirty2ms(wsg_plan *p, const void *const *dirty, void *vis) {
+  return guarded([&] {
+    wsg::require(p != nullptr, "plan is NULL");
+    p->impl->dirty2ms(dirty, vis);
+  });
+}
+
+int wsg_plan_get_stats(const wsg_plan *p, size_t job, wsg_stats *out) {
+  return guarded([&] {
+    wsg::require(p != nullptr && out != nullptr, "plan and out are required");
+    p->impl->stats(job, *out);
+  });
+}
+
+int wsg_ctx_synchronize(wsg_ctx *ctx) {
+  return guarded([&] {
+    wsg::require(ctx != nullptr, "ctx is NULL");
+    ctx->ctx->synchronize();
   });
 }
 

@@ -33,6 +33,8 @@ struct Layout {
   }
 };
 
+class Plan;
+
 // Device pointers of one call's inputs.
 struct Staged {
   const double *uvw = nullptr;
@@ -52,6 +54,7 @@ class Context {
   void ms2dirty(const wsg_args &a, const void *vis, void *dirty, int accumulate);
   void dirty2ms(const wsg_args &a, const void *dirty, void *vis);
   void release_buffers();
+  void synchronize();
   size_t device_bytes();
   void validate(const wsg_args &a);
 
@@ -78,6 +81,7 @@ class Context {
   DevBuf b_img, b_img2, b_acc, b_cf, b_tw, b_fftwork, b_out;
 
  private:
+  friend class Plan;
   std::vector<DevBuf *> all_buffers();
   template <typename R>
   bool prepare(const wsg_args &a, const Staged &s, bool gridding, void *vis_out_dev, GridPlan &gp);
@@ -106,6 +110,64 @@ class Context {
   std::tuple<int, double, double, size_t, size_t, size_t, size_t, double> corr_key;
   ChebCorr corr_cc;
   bool corr_valid = false;
+};
+
+// One job of a plan (see wsg_plan_create).
+struct PlanJob {
+  GridPlan gp;              // the job's grid (shared kernel)
+  size_t chan0 = 0, chan1 = 0;
+  size_t rec_off = 0, nrec = 0;
+  size_t band_off = 0, band_bytes = 0;  // bytes in the plan's band buffer
+  size_t cf_off = 0;        // doubles in the plan's correction buffer
+  size_t tw_off = 0;        // bytes in the plan's twiddle buffer
+  ChebCorr cc;
+  cufftHandle fft = 0;
+};
+
+// Reusable plan over one or more jobs sharing the visibilities.
+class Plan {
+ public:
+  Plan(Context &cx, const wsg_args &a, const wsg_job *jobs, size_t njobs);
+  ~Plan();
+  Plan(const Plan &) = delete;
+  Plan &operator=(const Plan &) = delete;
+  void ms2dirty(const void *vis, void *const *dirty, int accumulate);
+  void dirty2ms(const void *const *dirty, void *vis);
+  void stats(size_t job, wsg_stats &out) const;
+  size_t njobs() const { return jobs_.size(); }
+
+ private:
+  template <typename R>
+  void build(const std::vector<wsg_job> &jobs);
+  template <typename R>
+  void enqueue_grid(const void *vis, void *const *dirty, int accumulate);
+  template <typename R>
+  void enqueue_degrid(const void *const *dirty, void *vis);
+  void enqueue(int mode, const void *in, void *const *outs, const void *const *ins, void *out,
+               int accumulate);
+  void run(int mode, const void *in, void *const *outs, const void *const *ins, void *out,
+           int accumulate);
+
+  Context &cx_;
+  wsg_args a_;
+  bool dbl_ = false;
+  std::vector<PlanJob> jobs_;
+  DevBuf rec_, chunks_, chunk_job_, jobgeom_, band_, H_, img_, cf_, tw_, acc_, small_, fftwork_;
+  size_t nrec_ = 0, band_total_ = 0, max_npix_ = 0;
+  int nchunks_ = 0;
+  std::vector<unsigned char> kernel_;  // DevKernel<R> bytes
+  std::vector<unsigned char> geom_;    // DevGeom of the first job (kernel, tile: shared)
+  int W_ = 0, T_ = 0;
+  bool need_acc_ = false;
+  // graphs recorded per (mode, pointers, accumulate)
+  struct Graph {
+    int mode = 0, accumulate = 0;
+    std::vector<const void *> ptrs;
+    cudaGraphExec_t exec = nullptr;
+  };
+  std::vector<Graph> graphs_;
+  std::vector<std::pair<int, std::vector<const void *>>> eager_seen_;
+  bool use_graphs_ = true;
 };
 
 // Allocation-free mixed-precision ms2dirty (scratch in a static device array).

@@ -289,6 +289,29 @@ __global__ void k_records(size_t nvis, int nchan, const uint32_t *__restrict__ s
   }
 }
 
+// Batch plans: a job's records index its own channel range; make the index
+// flat over the full nrows x nchan_total array (the conjugation bit is kept).
+template <typename Rec>
+__global__ void k_plan_remap(size_t n, Rec *__restrict__ rec, uint32_t nch, uint32_t nch_total,
+                             uint32_t chan0) {
+  for (size_t s = blockIdx.x * size_t(blockDim.x) + threadIdx.x; s < n;
+       s += size_t(gridDim.x) * blockDim.x) {
+    const uint32_t id = rec[s].idx;
+    const uint32_t k = id & 0x7fffffffu, r = k / nch, c = k - r * nch;
+    rec[s].idx = (id & 0x80000000u) | (r * nch_total + chan0 + c);
+  }
+}
+
+// Batch plans: append a job's chunk starts (shifted by its record offset)
+// and tag the chunks with the job.
+__global__ void k_plan_chunks(int n, const int *__restrict__ in, int *__restrict__ out,
+                              int *__restrict__ job_of, int rec_off, int job) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    out[i] = in[i] + rec_off;
+    job_of[i] = job;
+  }
+}
+
 // ----------------------------------------------------- chunk boundaries
 
 // A chunk starts where the (tile, minplane) bin changes or at a multiple of
@@ -311,6 +334,15 @@ struct TileLayout {
   int PS;   // plane stride (elements)
 };
 
+// Grid geometry of one gridding job.  A call is one job; a batch plan runs
+// many jobs (facets x output channels) sharing one kernel, tile size and
+// record array through a single spread / interpolation launch.
+struct JobGeom {
+  int nu, nv, Lu, band_rows, band_full;
+  int P, pb0, pb1;   // planes in the band layout, planes of this pass [pb0, pb1)
+  void *grid;        // the job's u-band grid [band_rows][P][nv] complex
+};
+
 struct GridArgs {
   const void *rec;
   const int *chunk_start;
@@ -328,7 +360,40 @@ struct GridArgs {
   int vis_double;
   void *acc;         // per-record accumulator (multi-pass), complex R
   int first_pass, last_pass;
+  // batch plans: per-job geometry and the job of each chunk (jobs == null:
+  // one job, described by DevGeom and the fields above)
+  const JobGeom *jobs;
+  const int *chunk_job;
+  // plan execution (gridding): records hold the static factor c = weight *
+  // conj(shift phasor); the visibility is gathered at staging and the
+  // spread value is V conj(c), conjugated for flipped w
+  const void *vis_in;
+  int vis_in_double;
+  // degridding: add into vis_out (jobs that predict the same visibilities)
+  int vis_accumulate;
 };
+
+__device__ __forceinline__ JobGeom load_job(const GridArgs &a, const DevGeom &g, int ch) {
+  if (a.jobs) return a.jobs[a.chunk_job ? a.chunk_job[ch] : 0];
+  JobGeom j;
+  j.nu = g.nu;
+  j.nv = g.nv;
+  j.Lu = g.Lu;
+  j.band_rows = g.band_rows;
+  j.band_full = g.band_full;
+  j.P = a.P;
+  j.pb0 = a.pb0;
+  j.pb1 = a.pb1;
+  j.grid = a.grid;
+  return j;
+}
+
+__device__ __forceinline__ int band_index_j(const JobGeom &j, int u) {
+  if (j.band_full) return u;
+  if (u <= j.Lu) return u;
+  if (u >= j.nu - j.Lu) return u - (j.nu - j.band_rows);
+  return -1;
+}
 
 constexpr uint32_t kSkip = 0xfffffffeu;  // record marker: outside its chunk's tile
 
@@ -376,7 +441,8 @@ template <typename R, int W, typename Rec>
 __device__ __forceinline__ void stage_batch(const Rec *recs, int b0, int nb, int lane, int tu,
                                             int tv, int mp, const DevGeom &g,
                                             const DevKernel<R> &kc, R *kv, R *vv, uint32_t *luv,
-                                            int *err, int &bb0, int &bb1, int &bb2, int &bb3) {
+                                            int *err, int &bb0, int &bb1, int &bb2, int &bb3,
+                                            const void *vis_in, int vis_in_double) {
   constexpr int KST = KStride<R, W>::value;
   if (lane < nb) {
     const Rec rr = recs[b0 + lane];
@@ -405,8 +471,25 @@ __device__ __forceinline__ void stage_batch(const Rec *recs, int b0, int nb, int
 #pragma unroll
         for (int i = 0; i < W; ++i) row[2 * W + i] = R(i == 0);
       }
-      vv[2 * lane] = rr.vr;
-      vv[2 * lane + 1] = rr.vi;
+      R vr = rr.vr, vi = rr.vi;
+      if (vis_in) {
+        const uint32_t id = rr.idx & 0x7fffffffu;
+        R xr, xi;
+        if (vis_in_double) {
+          const double2 x = reinterpret_cast<const double2 *>(vis_in)[id];
+          xr = R(x.x);
+          xi = R(x.y);
+        } else {
+          const float2 x = reinterpret_cast<const float2 *>(vis_in)[id];
+          xr = R(x.x);
+          xi = R(x.y);
+        }
+        vr = xr * rr.vr + xi * rr.vi;
+        vi = xi * rr.vr - xr * rr.vi;
+        if (rr.idx & 0x80000000u) vi = -vi;
+      }
+      vv[2 * lane] = vr;
+      vv[2 * lane + 1] = vi;
     }
   }
 }
@@ -457,6 +540,7 @@ k_spread(GridArgs a, DevGeom g, DevKernel<R> kc) {
   R *tim = tre + W * tl.PS;
   __shared__ int sh_chunk, sh_bb[4], sh_norig;
   __shared__ uint32_t sh_orig[kMaxOrig];
+  __shared__ JobGeom sh_job;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int grp = warp % NG, slice = warp / NG;
@@ -465,7 +549,6 @@ k_spread(GridArgs a, DevGeom g, DevKernel<R> kc) {
   R *vv = kv + 32 * KST;
   uint32_t *luvs = reinterpret_cast<uint32_t *>(vv + 64);
   const Rec *recs = reinterpret_cast<const Rec *>(a.rec);
-  C *grid = reinterpret_cast<C *>(a.grid);
 
   for (int i = tid; i < 2 * W * tl.PS; i += blockDim.x) tre[i] = R(0);
   int pp[PPL], cu[PPL];
@@ -482,16 +565,18 @@ k_spread(GridArgs a, DevGeom g, DevKernel<R> kc) {
       sh_chunk = atomicAdd(a.counter, 1);
       sh_bb[0] = 1 << 30; sh_bb[1] = -1; sh_bb[2] = 1 << 30; sh_bb[3] = -1;
       sh_norig = 0;
+      if (sh_chunk < *a.nchunks) sh_job = load_job(a, g, sh_chunk);
     }
     __syncthreads();
     const int ch = sh_chunk;
     if (ch >= *a.nchunks) break;
+    const JobGeom jb = sh_job;
     const int s0 = a.chunk_start[ch];
     const int s1 = (ch + 1 < *a.nchunks) ? a.chunk_start[ch + 1] : a.nvis;
     const Rec r0 = recs[s0];
     const int tu = int(r0.iuv >> 16) / g.T, tv = int(r0.iuv & 0xffffu) / g.T;
     const int mp = int(r0.mp);
-    if (!((mp < a.pb1) && (mp + W > a.pb0))) continue;
+    if (!((mp < jb.pb1) && (mp + W > jb.pb0))) continue;
 
     if (slice < NSL) {
       const int n = s1 - s0;
@@ -499,7 +584,7 @@ k_spread(GridArgs a, DevGeom g, DevKernel<R> kc) {
       bool ok[PPL];
 #pragma unroll
       for (int k = 0; k < PPL; ++k)
-        ok[k] = (pp[k] < W) && (mp + pp[k] >= a.pb0) && (mp + pp[k] < a.pb1);
+        ok[k] = (pp[k] < W) && (mp + pp[k] >= jb.pb0) && (mp + pp[k] < jb.pb1);
       R accr[PPL][W], acci[PPL][W];
 #pragma unroll
       for (int k = 0; k < PPL; ++k)
@@ -525,7 +610,7 @@ k_spread(GridArgs a, DevGeom g, DevKernel<R> kc) {
       for (int b0 = j0; b0 < j1; b0 += 32) {
         const int nb = min(32, j1 - b0);
         stage_batch<R, W>(recs, b0, nb, lane, tu, tv, mp, g, kc, kv, vv, luvs, a.err, bb0, bb1,
-                          bb2, bb3);
+                          bb2, bb3, a.vis_in, a.vis_in_double);
         __syncwarp();
         for (int jj = 0; jj < nb; ++jj) {
           const uint32_t luv = luvs[jj];
@@ -602,16 +687,16 @@ k_spread(GridArgs a, DevGeom g, DevKernel<R> kc) {
         tim[sidx] = R(0);
       }
       const int plane = mp + p;
-      if ((xr != R(0) || xi != R(0)) && plane >= a.pb0 && plane < a.pb1) {
+      if ((xr != R(0) || xi != R(0)) && plane >= jb.pb0 && plane < jb.pb1) {
         int u = ucorner + ia;
-        u += (u < 0) ? g.nu : 0;
-        u -= (u >= g.nu) ? g.nu : 0;
+        u += (u < 0) ? jb.nu : 0;
+        u -= (u >= jb.nu) ? jb.nu : 0;
         int v = vcorner + ib;
-        v += (v < 0) ? g.nv : 0;
-        v -= (v >= g.nv) ? g.nv : 0;
-        const int bi = band_index(g, u);
+        v += (v < 0) ? jb.nv : 0;
+        v -= (v >= jb.nv) ? jb.nv : 0;
+        const int bi = band_index_j(jb, u);
         if (bi >= 0) {
-          C *dst = grid + (size_t(bi) * a.P + (plane - a.pb0)) * size_t(g.nv) + v;
+          C *dst = reinterpret_cast<C *>(jb.grid) + (size_t(bi) * jb.P + (plane - jb.pb0)) * size_t(jb.nv) + v;
           if constexpr (sizeof(R) == 4) {
             atomicAdd(reinterpret_cast<float2 *>(dst), make_float2(xr, xi));
           } else {
@@ -622,6 +707,26 @@ k_spread(GridArgs a, DevGeom g, DevKernel<R> kc) {
       }
       }
     }
+  }
+}
+
+// Writes (or, for batch plans, atomically adds) one degridded visibility.
+__device__ __forceinline__ void store_vis(void *out, int dbl, int accumulate, uint32_t idx,
+                                          double re, double im) {
+  if (dbl) {
+    double2 *p = reinterpret_cast<double2 *>(out) + idx;
+    if (accumulate) {
+      atomicAdd(&p->x, re);
+      atomicAdd(&p->y, im);
+    } else {
+      *p = make_double2(re, im);
+    }
+  } else {
+    float2 *p = reinterpret_cast<float2 *>(out) + idx;
+    if (accumulate)
+      atomicAdd(p, make_float2(float(re), float(im)));
+    else
+      *p = make_float2(float(re), float(im));
   }
 }
 
@@ -648,6 +753,7 @@ k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
   R *tim = tre + W * tl.PS;
   __shared__ int sh_chunk, sh_bb[4], sh_norig;
   __shared__ uint32_t sh_orig[kMaxOrig];
+  __shared__ JobGeom sh_job;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int grp = warp % NG, slice = warp / NG;
@@ -656,7 +762,6 @@ k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
   R *vv = kv + 32 * KST;
   uint32_t *luvs = reinterpret_cast<uint32_t *>(vv + 64);
   const Rec *recs = reinterpret_cast<const Rec *>(a.rec);
-  const C *grid = reinterpret_cast<const C *>(a.grid);
   const bool direct = a.last_pass && a.first_pass && NG == 1;
 
   int pp[PPL], cu[PPL];
@@ -675,16 +780,18 @@ k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
       sh_chunk = atomicAdd(a.counter, 1);
       sh_bb[0] = 1 << 30; sh_bb[1] = -1; sh_bb[2] = 1 << 30; sh_bb[3] = -1;
       sh_norig = 0;
+      if (sh_chunk < *a.nchunks) sh_job = load_job(a, g, sh_chunk);
     }
     __syncthreads();
     const int ch = sh_chunk;
     if (ch >= *a.nchunks) break;
+    const JobGeom jb = sh_job;
     const int s0 = a.chunk_start[ch];
     const int s1 = (ch + 1 < *a.nchunks) ? a.chunk_start[ch + 1] : a.nvis;
     const Rec r0 = recs[s0];
     const int tu = int(r0.iuv >> 16) / g.T, tv = int(r0.iuv & 0xffffu) / g.T;
     const int mp = int(r0.mp);
-    if (!((mp < a.pb1) && (mp + W > a.pb0))) continue;  // contributes nothing this pass
+    if (!((mp < jb.pb1) && (mp + W > jb.pb0))) continue;  // contributes nothing this pass
     // bounding box and distinct footprint origins of the chunk
     for (int s = s0 + tid; s < s1; s += blockDim.x) {
       const uint32_t iuv = recs[s].iuv;
@@ -734,15 +841,16 @@ k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
             }
             sidx[q] = p * tl.PS + ia * tl.RS + ib;
             const int plane = mp + p;
-            if (plane >= a.pb0 && plane < a.pb1) {
+            if (plane >= jb.pb0 && plane < jb.pb1) {
               int u = ucorner + ia;
-              u += (u < 0) ? g.nu : 0;
-              u -= (u >= g.nu) ? g.nu : 0;
+              u += (u < 0) ? jb.nu : 0;
+              u -= (u >= jb.nu) ? jb.nu : 0;
               int v = vcorner + ib;
-              v += (v < 0) ? g.nv : 0;
-              v -= (v >= g.nv) ? g.nv : 0;
-              const int bi = band_index(g, u);
-              if (bi >= 0) val[q] = grid[(size_t(bi) * a.P + (plane - a.pb0)) * size_t(g.nv) + v];
+              v += (v < 0) ? jb.nv : 0;
+              v -= (v >= jb.nv) ? jb.nv : 0;
+              const int bi = band_index_j(jb, u);
+              if (bi >= 0)
+                val[q] = reinterpret_cast<const C *>(jb.grid)[(size_t(bi) * jb.P + (plane - jb.pb0)) * size_t(jb.nv) + v];
             }
           }
         }
@@ -765,7 +873,7 @@ k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
       for (int b0 = j0; b0 < j1; b0 += 32) {
         const int nb = min(32, j1 - b0);
         stage_batch<R, W>(recs, b0, nb, lane, tu, tv, mp, g, kc, kv, vv, luvs, a.err, bb0, bb1,
-                          bb2, bb3);
+                          bb2, bb3, a.vis_in, a.vis_in_double);
         __syncwarp();
         for (int jj = 0; jj < nb; ++jj) {
           const uint32_t luv = luvs[jj];
@@ -810,10 +918,7 @@ k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
               if (rr.idx & 0x80000000u) si = -si;
               const double orr = double(rr.vr) * double(sr) - double(rr.vi) * double(si);
               const double oi = double(rr.vr) * double(si) + double(rr.vi) * double(sr);
-              if (a.vis_double)
-                reinterpret_cast<double2 *>(a.vis_out)[idx] = make_double2(orr, oi);
-              else
-                reinterpret_cast<float2 *>(a.vis_out)[idx] = make_float2(float(orr), float(oi));
+              store_vis(a.vis_out, a.vis_double, a.vis_accumulate, idx, orr, oi);
             } else {
               C *accp = reinterpret_cast<C *>(a.acc) + s;
               atomicAdd(&accp->x, sr);
@@ -828,10 +933,11 @@ k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
 }
 
 // Finalises degridded visibilities accumulated over plane passes or warp
-// groups: out[idx] = P * (flip ? conj(acc) : acc).
+// groups: out[idx] = P * (flip ? conj(acc) : acc) (added into out when
+// accumulating).
 template <typename R>
 __global__ void k_finalize(int nvis, const void *recv, const void *accv, void *vis_out,
-                           int vis_double) {
+                           int vis_double, int vis_accumulate) {
   using Rec = typename RecOf<R>::type;
   using C = typename Cplx<R>::type;
   const Rec *recs = reinterpret_cast<const Rec *>(recv);
@@ -843,10 +949,7 @@ __global__ void k_finalize(int nvis, const void *recv, const void *accv, void *v
     const uint32_t idx = rr.idx & 0x7fffffffu;
     const double orr = double(rr.vr) * sr - double(rr.vi) * si;
     const double oi = double(rr.vr) * si + double(rr.vi) * sr;
-    if (vis_double)
-      reinterpret_cast<double2 *>(vis_out)[idx] = make_double2(orr, oi);
-    else
-      reinterpret_cast<float2 *>(vis_out)[idx] = make_float2(float(orr), float(oi));
+    store_vis(vis_out, vis_double, vis_accumulate, idx, orr, oi);
   }
 }
 

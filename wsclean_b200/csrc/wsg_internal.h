@@ -124,6 +124,9 @@ struct GridPlan {
   int ntu = 0, ntv = 0, nwmin = 1;
   int lbits = 0;      // sort bits per axis for the position inside a tile
   int key_bits = 0;   // total key bits (<= 31)
+  // batch plans: every job uses the kernel (W, sigma) of the first one
+  int force_W = 0;
+  double force_sigma = 0;
 };
 
 // Parameter choice (the analogue of ducc0 Params::getNuNv, wgridder.h:1503-1576,

@@ -31,6 +31,11 @@ _NP_C = {np.dtype(np.complex64): L.WSG_C64, np.dtype(np.complex128): L.WSG_C128}
 _NP_F = {np.dtype(np.float32): L.WSG_F32, np.dtype(np.float64): L.WSG_F64}
 
 
+# cudaStreamLegacy: the handle of the legacy default stream (a NULL stream
+# argument would select the context's own stream instead)
+_CUDA_STREAM_LEGACY = 1
+
+
 def _is_torch(x):
     return torch is not None and isinstance(x, torch.Tensor)
 
@@ -87,6 +92,8 @@ class Context:
         work that produced its inputs (the context's own stream otherwise)."""
         dev = next((t.device for t in tensors if _is_torch(t) and t.is_cuda), None)
         s = torch.cuda.current_stream(dev).cuda_stream if dev is not None else None
+        if dev is not None and s == 0:
+            s = _CUDA_STREAM_LEGACY   # torch's default stream is the legacy NULL stream
         L.check(L.lib().wsg_ctx_set_stream(self._h, s))
 
     def stats(self):
@@ -319,3 +326,125 @@ def plan_grid(npix_x, npix_y, pixsize_x, pixsize_y, epsilon, nvis, wmin, wmax, u
                                   float(umax), float(umax if vmax is None else vmax),
                                   ctypes.byref(s)))
     return s.as_dict()
+
+
+class Plan:
+    """A reusable plan (``wsg_plan_create``): the grid choice, visibility sort
+    and per-visibility records for fixed uvw / freq / weights / mask, over one
+    job or a batch of jobs (facets x output channels) sharing the
+    visibilities.  ``jobs`` is a list of dicts with npix_x, npix_y and
+    optionally center_x, center_y (phase centre, radians) and chan_begin,
+    chan_end (input channel range); without it there is one job of
+    npix_x x npix_y over all channels.
+
+    Execution takes torch CUDA tensors, runs on torch's current stream and
+    returns without waiting, so a major cycle built from these calls can be
+    recorded with ``torch.cuda.graph``.  On a non-default stream the plan
+    records and replays its own graph from the second call with the same
+    tensors on."""
+
+    def __init__(self, uvw, freq, pixsize_x, pixsize_y, epsilon, npix_x=None, npix_y=None,
+                 jobs=None, wgt=None, mask=None, do_wgridding=True, negate_v=False,
+                 divide_by_n=True, sigma_min=1.1, sigma_max=2.6, center_x=0.0, center_y=0.0,
+                 precision="mixed", vis_dtype=np.complex64, dirty_dtype=None, context=None,
+                 device=-1):
+        self.ctx = context if context is not None else Context(device)
+        self._own_ctx = context is None
+        nrows, nchan = int(np.shape(uvw)[0]), int(np.shape(freq)[0])
+        self.nrows, self.nchan = nrows, nchan
+        self.vis_dtype = np.dtype(vis_dtype)
+        pr = _precision(precision)
+        self.dirty_dtype = np.dtype(dirty_dtype) if dirty_dtype is not None else (
+            np.dtype(np.float64) if pr == L.WSG_PREC_FP64 else np.dtype(np.float32))
+        keep = []
+        a = self.ctx._args(uvw, freq, nrows, nchan, wgt, mask, npix_x or 16, npix_y or 16,
+                           pixsize_x, pixsize_y, epsilon, do_wgridding, negate_v, divide_by_n,
+                           sigma_min, sigma_max, center_x, center_y, precision,
+                           _NP_C[self.vis_dtype], _NP_F[self.dirty_dtype], keep)
+        if jobs is None:
+            if npix_x is None or npix_y is None:
+                raise ValueError("npix_x and npix_y are required without jobs")
+            jobs = [dict(npix_x=npix_x, npix_y=npix_y, center_x=center_x, center_y=center_y)]
+        self.jobs = [dict(j) for j in jobs]
+        arr = (L.WsgJob * len(jobs))()
+        for k, j in enumerate(jobs):
+            arr[k].npix_x, arr[k].npix_y = int(j["npix_x"]), int(j["npix_y"])
+            arr[k].center_x = float(j.get("center_x", 0.0))
+            arr[k].center_y = float(j.get("center_y", 0.0))
+            arr[k].chan_begin = int(j.get("chan_begin", 0))
+            arr[k].chan_end = int(j.get("chan_end", nchan))
+        h = ctypes.c_void_p()
+        self.ctx._bind_stream(*[x for x in keep if _is_torch(x)])
+        L.check(L.lib().wsg_plan_create(self.ctx._h, ctypes.byref(a), arr, len(jobs),
+                                        ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            L.lib().wsg_plan_destroy(self._h)
+            self._h = None
+        if getattr(self, "_own_ctx", False) and self.ctx is not None:
+            self.ctx.close()
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _tensor(self, x, dtype, what):
+        if not (_is_torch(x) and x.is_cuda):
+            raise ValueError(f"plan execution takes CUDA tensors ({what})")
+        t, _, _, _ = _prep(x, dtype)
+        return t
+
+    def ms2dirty(self, vis, dirty=None, accumulate=False):
+        """Images of all jobs: list of (npix_x, npix_y) tensors."""
+        v = self._tensor(vis, self.vis_dtype, "vis")
+        if tuple(v.shape) != (self.nrows, self.nchan):
+            raise ValueError("vis must be nrows x nchan")
+        tdt = torch.float64 if self.dirty_dtype == np.float64 else torch.float32
+        if dirty is None:
+            dirty = [torch.zeros((j["npix_x"], j["npix_y"]), dtype=tdt, device=v.device)
+                     for j in self.jobs]
+        elif _is_torch(dirty):
+            dirty = [dirty]
+        outs = [self._tensor(d, self.dirty_dtype, "dirty") for d in dirty]
+        if any(o is not d for o, d in zip(outs, dirty)):
+            raise ValueError("dirty images must be contiguous tensors of the plan's dirty dtype")
+        ptrs = (ctypes.c_void_p * len(outs))(*[o.data_ptr() for o in outs])
+        self.ctx._bind_stream(v)
+        L.check(L.lib().wsg_plan_ms2dirty(self._h, v.data_ptr(), ptrs, int(bool(accumulate))))
+        self._keep = (v, outs)
+        return outs
+
+    def dirty2ms(self, dirty, vis=None):
+        """Sum over jobs of the predicted visibilities (nrows x nchan tensor)."""
+        if _is_torch(dirty):
+            dirty = [dirty]
+        ins = [self._tensor(d, self.dirty_dtype, "dirty") for d in dirty]
+        if len(ins) != len(self.jobs):
+            raise ValueError("one image per job is required")
+        tdt = torch.complex128 if self.vis_dtype == np.complex128 else torch.complex64
+        if vis is None:
+            vis = torch.empty((self.nrows, self.nchan), dtype=tdt, device=ins[0].device)
+        out = self._tensor(vis, self.vis_dtype, "vis")
+        if out is not vis:
+            raise ValueError("vis must be a contiguous tensor of the plan's vis dtype")
+        ptrs = (ctypes.c_void_p * len(ins))(*[d.data_ptr() for d in ins])
+        self.ctx._bind_stream(out)
+        L.check(L.lib().wsg_plan_dirty2ms(self._h, ptrs, out.data_ptr()))
+        self._keep = (ins, out)
+        return out
+
+    def stats(self, job=0):
+        s = L.WsgStats()
+        L.check(L.lib().wsg_plan_get_stats(self._h, int(job), ctypes.byref(s)))
+        return s.as_dict()
