@@ -58,6 +58,8 @@ def parse_args():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-clocks", action="store_true",
                     help="do not sample nvidia-smi during the timed region")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the config-4 batched-facets measurement")
     ap.add_argument("--timed-only", action="store_true",
                     help="stop after the timed region (for profiler launch lists)")
     ap.add_argument("--scale", type=float, default=1.0,
@@ -241,6 +243,82 @@ def run_reference(args, world, rank):
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out))
+
+
+def run_batched(dev, torch, ctx, args):
+    """Config 4: 16 Voronoi facets x 8 output channels (8 of 64 input
+    channels each) = 128 jobs over the same rows, gridded and degridded
+    through one reusable plan (one persistent spread / interpolation launch
+    per call, replayed as a CUDA graph), against the plain FP64 form run job
+    by job (timed on the first 16 jobs and scaled to all 128)."""
+    from wsclean_b200 import synth
+    from wsclean_b200 import gridder as G
+    c = synth.config4()
+    uvw, freq, px = c["uvw"], c["freq"], c["pixsize"]
+    nrows = uvw.shape[0]
+    jobs = [dict(npix_x=f["nx"], npix_y=f["ny"], center_x=f["dx"] * px, center_y=f["dy"] * px,
+                 chan_begin=8 * oc, chan_end=8 * oc + 8)
+            for oc in range(8) for f in synth.facets4()]
+    kw = dict(negate_v=True, divide_by_n=False, sigma_min=1.1, sigma_max=2.0)
+    g = torch.Generator(device=dev).manual_seed(7)
+    vis = torch.complex(torch.randn(nrows, 64, device=dev, generator=g),
+                        torch.randn(nrows, 64, device=dev, generator=g))
+    jv = nrows * 8 * len(jobs)
+    t0 = time.perf_counter()
+    plan = G.Plan(uvw, freq, px, px, EPS_MIXED, jobs=jobs, **kw)
+    torch.cuda.synchronize(dev)
+    t_build = time.perf_counter() - t0
+    st = torch.cuda.Stream(dev)
+    models = [torch.zeros((j["npix_x"], j["npix_y"]), device=dev) for j in jobs]
+    for m in models:
+        m[m.shape[0] // 2, m.shape[1] // 2] = 1.0
+    dirty = [torch.empty((j["npix_x"], j["npix_y"]), device=dev) for j in jobs]
+    pred = torch.empty_like(vis)
+    n = 3
+    with torch.cuda.stream(st):
+        for _ in range(3):
+            plan.ms2dirty(vis, dirty)
+            plan.dirty2ms(models, pred)
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record(st)
+        for _ in range(n):
+            plan.ms2dirty(vis, dirty)
+        e[1].record(st)
+        for _ in range(n):
+            plan.dirty2ms(models, pred)
+        e[2].record(st)
+        st.synchronize()
+    tg, td = e[0].elapsed_time(e[1]) / n, e[1].elapsed_time(e[2]) / n
+    W = plan.stats(0)["supp"]
+    plan.close()
+    del dirty, pred, models
+    # plain FP64 form, job by job
+    vis64 = vis.to(torch.complex128)
+    del vis
+    tu = torch.as_tensor(uvw, device=dev)
+    tf = torch.as_tensor(freq, device=dev)
+    sub = jobs[:16]
+    t64 = 0.0
+    for rep in range(2):   # the first pass creates the FFT plans of each facet size
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for j in sub:
+            c0, c1 = j["chan_begin"], j["chan_end"]
+            ctx.ms2dirty(tu, tf[c0:c1], vis64[:, c0:c1].contiguous(), j["npix_x"], j["npix_y"],
+                         px, px, EPS_FP64, precision="fp64", center_x=j["center_x"],
+                         center_y=j["center_y"], dirty_dtype=np.float64, **kw)
+        torch.cuda.synchronize(dev)
+        t64 = (time.perf_counter() - t0) / len(sub) * len(jobs) * 1e3
+    del vis64
+    return {"workload": "config 4: 96 antennas within 10 km, 360 x 10 s, 64 channels 120-180 MHz; "
+                        "16 Voronoi facets (512^2..2048^2, phase centre at the box centre) x 8 "
+                        "output channels = 128 jobs",
+            "rows": nrows, "job_visibilities": jv, "plan_build_s": t_build, "W": W,
+            "mixed_ms2dirty_ms": tg, "mixed_dirty2ms_ms": td,
+            "mixed_ms2dirty_mvis_s": jv / tg / 1e3, "mixed_dirty2ms_mvis_s": jv / td / 1e3,
+            "fp64_per_job_ms2dirty_ms": t64, "fp64_per_job_ms2dirty_mvis_s": jv / t64 / 1e3,
+            "mixed_batched_over_fp64_per_job": t64 / tg,
+            "fp64_timing": "16 of 128 jobs timed (warm FFT plans), scaled to 128"}
 
 
 def dft_pixels(uvw, freq, vis, nx, ny, px, py, pix, torch, dev):
@@ -441,6 +519,15 @@ def run_ours(args, world, rank, local, pg):
     h2d = 2 * h_uvw.numel() * 8 + h_vis.numel() * 8 + h_model.numel() * 4 + 2 * nchan * 8
     d2h = h_dirty.numel() * 4 + h_out.numel() * 8
 
+    # ---- config 4: batched facets x output channels through one plan
+    batched = None
+    if not args.no_batch:
+        try:
+            batched = run_batched(dev, torch, ctx, args)
+        except Exception as e:  # reported, not fatal
+            batched = {"error": str(e)}
+        torch.cuda.empty_cache()
+
     # ---- roofline of the pipeline (algorithmic bytes, the reference's grid)
     B = (algorithmic_bytes(nvis, nrows, nx, nx, DUCC_GRID["mixed"], 8, 8) * 2)
     achieved = B / (ms_per_step / 1e3) / 1e9
@@ -497,6 +584,7 @@ def run_ours(args, world, rank, local, pg):
                          "peak_source": peak_src,
                          "bytes_per_step": B},
             "cpu_baseline": cpu,
+            "batched_facets": batched,
             "clocks": clocks,
             "gpu_launches": launches,
         }
