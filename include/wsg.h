@@ -264,6 +264,44 @@ int wsg_plan_get_stats(const wsg_plan *p, size_t job, wsg_stats *out);
 /* Waits for the work enqueued on the context's stream. */
 int wsg_ctx_synchronize(wsg_ctx *ctx);
 
+/* --------------------------------------- streaming into a resident grid */
+
+/* Streaming gridding of data larger than one call -- WSClean's chunked
+ * AddInversionData / PredictVisibilities loop (wgridder/wgriddingmsgridder.cpp:80-193)
+ * -- with the w-stack of the whole observation resident on the GPU: the grid
+ * is planned once from the declared data extent, every chunk of rows is
+ * copied in (pinned double buffers on a copy stream, so the next chunk's
+ * transfer overlaps this chunk's sort and spread) and spread into the same
+ * grid, and the FFTs, w-screens and correction run once, in
+ * wsg_stream_finish.  Prediction runs the transpose: the model image is
+ * transformed once (wsg_stream_predict_begin) and each chunk is interpolated.
+ * Extension of the reference interface, which re-plans and re-transforms per
+ * chunk.
+ *
+ * a: pixel sizes, image size, epsilon, flags, sigma range, centre,
+ * precision, vis_type, dirty_type, wgt_type, freq/nchan (the channels of
+ * every chunk); nrows, uvw, wgt, mask are ignored.  wmin, wmax: |w| range
+ * and umax, vmax: max |u|, |v| in wavelengths over all chunks (a chunk
+ * outside is rejected); nvis: expected number of visibilities (kernel
+ * choice only). */
+typedef struct wsg_stream wsg_stream;
+int wsg_stream_create(wsg_ctx *ctx, const wsg_args *a, double wmin, double wmax, double umax,
+                      double vmax, size_t nvis, wsg_stream **out);
+int wsg_stream_destroy(wsg_stream *s);
+/* Adds nrows rows (uvw nrows x 3, vis nrows x nchan, wgt/mask or NULL). */
+int wsg_stream_add(wsg_stream *s, size_t nrows, const double *uvw, const void *vis,
+                   const void *wgt, const uint8_t *mask);
+/* Transforms the accumulated grid into dirty (or adds it when accumulate);
+ * the stream is then empty again. */
+int wsg_stream_finish(wsg_stream *s, void *dirty, int accumulate);
+/* Loads a model image for prediction. */
+int wsg_stream_predict_begin(wsg_stream *s, const void *dirty);
+/* Predicts nrows rows into vis (nrows x nchan of vis_type). */
+int wsg_stream_predict(wsg_stream *s, size_t nrows, const double *uvw, void *vis,
+                       const void *wgt, const uint8_t *mask);
+/* Grid choice of the stream (timings are zero). */
+int wsg_stream_get_stats(const wsg_stream *s, wsg_stats *out);
+
 #ifdef __cplusplus
 }
 #endif

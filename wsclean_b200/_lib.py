@@ -30,6 +30,8 @@ EXPORTED = [
     "wsg_plan_grid", "wsg_ms2dirty_noalloc",
     "wsg_plan_create", "wsg_plan_destroy", "wsg_plan_ms2dirty", "wsg_plan_dirty2ms",
     "wsg_plan_get_stats", "wsg_ctx_synchronize",
+    "wsg_stream_create", "wsg_stream_destroy", "wsg_stream_add", "wsg_stream_finish",
+    "wsg_stream_predict_begin", "wsg_stream_predict", "wsg_stream_get_stats",
 ]
 
 c_size_t, c_double, c_int, c_void_p = ctypes.c_size_t, ctypes.c_double, ctypes.c_int, ctypes.c_void_p
@@ -143,6 +145,14 @@ def lib():
         L.wsg_plan_dirty2ms.argtypes = [vp, P(vp), vp]
         L.wsg_plan_get_stats.argtypes = [vp, c_size_t, P(WsgStats)]
         L.wsg_ctx_synchronize.argtypes = [vp]
+        L.wsg_stream_create.argtypes = [vp, P(WsgArgs), c_double, c_double, c_double, c_double,
+                                        c_size_t, P(vp)]
+        L.wsg_stream_destroy.argtypes = [vp]
+        L.wsg_stream_add.argtypes = [vp, c_size_t, vp, vp, vp, vp]
+        L.wsg_stream_finish.argtypes = [vp, vp, c_int]
+        L.wsg_stream_predict_begin.argtypes = [vp, vp]
+        L.wsg_stream_predict.argtypes = [vp, c_size_t, vp, vp, vp, vp]
+        L.wsg_stream_get_stats.argtypes = [vp, P(WsgStats)]
         L.wsg_last_error.restype = ctypes.c_char_p
         L.wsg_abi_version.restype = c_int
         for name in EXPORTED:

@@ -20,6 +20,10 @@ struct wsg_plan {
   std::unique_ptr<wsg::Plan> impl;
   wsg_ctx *ctx = nullptr;
 };
+struct wsg_stream {
+  std::unique_ptr<wsg::StreamGridder> impl;
+  wsg_ctx *ctx = nullptr;
+};
 struct wsg_gridder {
   wsg::Gridder impl;
   wsg_ctx view;
@@ -300,6 +304,68 @@ int wsg_ctx_synchronize(wsg_ctx *ctx) {
   return guarded([&] {
     wsg::require(ctx != nullptr, "ctx is NULL");
     ctx->ctx->synchronize();
+  });
+}
+
+int wsg_stream_create(wsg_ctx *ctx, const wsg_args *a, double wmin, double wmax, double umax,
+                      double vmax, size_t nvis, wsg_stream **out) {
+  return guarded([&] {
+    wsg::require(ctx != nullptr && a != nullptr && out != nullptr, "ctx, args and out are required");
+    auto *h = new wsg_stream;
+    try {
+      h->impl.reset(new wsg::StreamGridder(*ctx->ctx, *a, wmin, wmax, umax, vmax, nvis));
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    h->ctx = ctx;
+    ++ctx->plans;
+    *out = h;
+  });
+}
+
+int wsg_stream_destroy(wsg_stream *s) {
+  return guarded([&] {
+    if (!s) return;
+    if (s->ctx) --s->ctx->plans;
+    delete s;
+  });
+}
+
+int wsg_stream_add(wsg_stream *s, size_t nrows, const double *uvw, const void *vis,
+                   const void *wgt, const uint8_t *mask) {
+  return guarded([&] {
+    wsg::require(s != nullptr, "stream is NULL");
+    s->impl->add(nrows, uvw, vis, wgt, mask);
+  });
+}
+
+int wsg_stream_finish(wsg_stream *s, void *dirty, int accumulate) {
+  return guarded([&] {
+    wsg::require(s != nullptr, "stream is NULL");
+    s->impl->finish(dirty, accumulate);
+  });
+}
+
+int wsg_stream_predict_begin(wsg_stream *s, const void *dirty) {
+  return guarded([&] {
+    wsg::require(s != nullptr, "stream is NULL");
+    s->impl->predict_begin(dirty);
+  });
+}
+
+int wsg_stream_predict(wsg_stream *s, size_t nrows, const double *uvw, void *vis,
+                       const void *wgt, const uint8_t *mask) {
+  return guarded([&] {
+    wsg::require(s != nullptr, "stream is NULL");
+    s->impl->predict(nrows, uvw, vis, wgt, mask);
+  });
+}
+
+int wsg_stream_get_stats(const wsg_stream *s, wsg_stats *out) {
+  return guarded([&] {
+    wsg::require(s != nullptr && out != nullptr, "stream and out are required");
+    s->impl->stats(*out);
   });
 }
 

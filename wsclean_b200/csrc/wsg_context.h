@@ -34,6 +34,7 @@ struct Layout {
 };
 
 class Plan;
+class StreamGridder;
 
 // Device pointers of one call's inputs.
 struct Staged {
@@ -82,6 +83,7 @@ class Context {
 
  private:
   friend class Plan;
+  friend class StreamGridder;
   std::vector<DevBuf *> all_buffers();
   template <typename R>
   bool prepare(const wsg_args &a, const Staged &s, bool gridding, void *vis_out_dev, GridPlan &gp);
@@ -168,6 +170,60 @@ class Plan {
   std::vector<Graph> graphs_;
   std::vector<std::pair<int, std::vector<const void *>>> eager_seen_;
   bool use_graphs_ = true;
+};
+
+// Host buffer in page-locked memory (grow-only).
+struct PinnedBuf {
+  void *p = nullptr;
+  size_t n = 0;
+  void *ensure(size_t bytes);
+  void release();
+};
+
+// Streaming into a resident grid (see wsg_stream_create).
+class StreamGridder {
+ public:
+  StreamGridder(Context &cx, const wsg_args &a, double wmin, double wmax, double umax,
+                double vmax, size_t nvis);
+  ~StreamGridder();
+  StreamGridder(const StreamGridder &) = delete;
+  StreamGridder &operator=(const StreamGridder &) = delete;
+  void add(size_t nrows, const double *uvw, const void *vis, const void *wgt, const uint8_t *mask);
+  void finish(void *dirty, int accumulate);
+  void predict_begin(const void *dirty);
+  void predict(size_t nrows, const double *uvw, void *vis, const void *wgt, const uint8_t *mask);
+  void stats(wsg_stats &out) const;
+
+ private:
+  struct Slot {
+    DevBuf uvw, vis, wgt, mask;
+    PinnedBuf h_uvw, h_vis, h_wgt, h_mask;
+    cudaEvent_t copied = nullptr, done = nullptr;
+  };
+  template <typename R>
+  void add_t(const Staged &s, size_t nrows);
+  template <typename R>
+  void finish_t(void *dirty, int accumulate);
+  template <typename R>
+  void predict_begin_t(const double *img);
+  template <typename R>
+  void predict_t(const Staged &s, size_t nrows, void *vis_dev);
+  Staged stage(Slot &sl, size_t nrows, const double *uvw, const void *vis, const void *wgt,
+               const uint8_t *mask);
+  size_t plane_batch() const;
+
+  Context &cx_;
+  wsg_args a_;
+  std::vector<double> freq_;  // the channels, copied at creation
+  GridPlan gp_;
+  bool dbl_ = false;
+  int mode_ = 0;  // 0 idle, 1 gridding, 2 predicting
+  DevBuf band_, H_, img_, cf_, tw_, fftwork_, vout_;
+  ChebCorr cc_;
+  cufftHandle fft_ = 0;
+  cudaStream_t copy_ = nullptr;
+  Slot slots_[2];
+  size_t k_ = 0;
 };
 
 // Allocation-free mixed-precision ms2dirty (scratch in a static device array).

@@ -127,6 +127,9 @@ struct GridPlan {
   // batch plans: every job uses the kernel (W, sigma) of the first one
   int force_W = 0;
   double force_sigma = 0;
+  // streams: the grid was planned from a declared data extent; chunks are
+  // checked against it instead of re-planning
+  bool fixed = false;
 };
 
 // Parameter choice (the analogue of ducc0 Params::getNuNv, wgridder.h:1503-1576,

@@ -448,3 +448,125 @@ class Plan:
         s = L.WsgStats()
         L.check(L.lib().wsg_plan_get_stats(self._h, int(job), ctypes.byref(s)))
         return s.as_dict()
+
+
+def data_extent(uvw, freq):
+    """(wmin, wmax, umax, vmax) in wavelengths over all rows and channels:
+    the extent a Stream is planned for."""
+    uvw = np.asarray(uvw, dtype=np.float64)
+    f = np.asarray(freq, dtype=np.float64) / 299792458.0
+    au = np.abs(uvw)
+    return (float(au[:, 2].min() * f.min()), float(au[:, 2].max() * f.max()),
+            float(au[:, 0].max() * f.max()), float(au[:, 1].max() * f.max()))
+
+
+class Stream:
+    """Streaming gridding into a resident grid (``wsg_stream_create``): the
+    grid is planned once for the declared extent (see ``data_extent``), each
+    ``add`` sorts and spreads one chunk of rows while the next chunk's copy
+    is in flight, and ``finish`` transforms once.  ``predict_begin`` /
+    ``predict`` run the transpose.  Chunks may be numpy arrays, page-locked
+    torch CPU tensors or CUDA tensors."""
+
+    def __init__(self, freq, npix_x, npix_y, pixsize_x, pixsize_y, epsilon, extent, nvis=0,
+                 do_wgridding=True, negate_v=False, divide_by_n=True, sigma_min=1.1,
+                 sigma_max=2.6, center_x=0.0, center_y=0.0, precision="mixed",
+                 vis_dtype=np.complex64, dirty_dtype=None, wgt_dtype=np.float32, context=None,
+                 device=-1):
+        self.ctx = context if context is not None else Context(device)
+        self._own_ctx = context is None
+        self.nchan = int(np.shape(freq)[0])
+        self.npix = (int(npix_x), int(npix_y))
+        self.vis_dtype = np.dtype(vis_dtype)
+        self.wgt_dtype = np.dtype(wgt_dtype)
+        pr = _precision(precision)
+        self.dirty_dtype = np.dtype(dirty_dtype) if dirty_dtype is not None else (
+            np.dtype(np.float64) if pr == L.WSG_PREC_FP64 else np.dtype(np.float32))
+        keep = []
+        dummy = np.zeros((1, 3))
+        a = self.ctx._args(dummy, freq, 1, self.nchan, None, None, npix_x, npix_y, pixsize_x,
+                           pixsize_y, epsilon, do_wgridding, negate_v, divide_by_n, sigma_min,
+                           sigma_max, center_x, center_y, precision, _NP_C[self.vis_dtype],
+                           _NP_F[self.dirty_dtype], keep)
+        a.wgt_type = _NP_F[self.wgt_dtype]
+        wmin, wmax, umax, vmax = extent
+        h = ctypes.c_void_p()
+        L.check(L.lib().wsg_stream_create(self.ctx._h, ctypes.byref(a), float(wmin), float(wmax),
+                                          float(umax), float(vmax), int(nvis), ctypes.byref(h)))
+        self._h = h
+        self._inflight = []
+
+    def close(self):
+        if getattr(self, "_h", None):
+            L.lib().wsg_stream_destroy(self._h)
+            self._h = None
+        if getattr(self, "_own_ctx", False) and self.ctx is not None:
+            self.ctx.close()
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _hold(self, objs):
+        # inputs of the last two chunks may still be copied from
+        self._inflight = (self._inflight + [objs])[-2:]
+
+    def add(self, uvw, vis, wgt=None, mask=None):
+        u, up, _, _ = _prep(uvw, np.float64)
+        v, vp, _, _ = _prep(vis, self.vis_dtype)
+        w, wp, _, _ = _prep(wgt, self.wgt_dtype)
+        m, mp, _, _ = _prep(mask, np.uint8)
+        nrows = int(u.shape[0])
+        if tuple(v.shape) != (nrows, self.nchan):
+            raise ValueError("vis must be nrows x nchan")
+        self.ctx._bind_stream(u, v, w, m)
+        L.check(L.lib().wsg_stream_add(self._h, nrows, up, vp, wp, mp))
+        self._hold((u, v, w, m))
+
+    def finish(self, dirty=None, accumulate=False):
+        if dirty is None:
+            dirty = np.zeros(self.npix, dtype=self.dirty_dtype)
+        d, dp, ddt, _ = _prep(dirty)
+        if ddt != self.dirty_dtype or (d is not dirty and not _is_torch(dirty)):
+            raise ValueError("dirty must be a contiguous array of the stream's dirty dtype")
+        self.ctx._bind_stream(d)
+        L.check(L.lib().wsg_stream_finish(self._h, dp, int(bool(accumulate))))
+        self._inflight = []
+        return d
+
+    def predict_begin(self, dirty):
+        d, dp, _, _ = _prep(dirty, self.dirty_dtype)
+        self.ctx._bind_stream(d)
+        L.check(L.lib().wsg_stream_predict_begin(self._h, dp))
+        self._model = d
+
+    def predict(self, uvw, vis=None, wgt=None, mask=None):
+        u, up, _, ucuda = _prep(uvw, np.float64)
+        nrows = int(u.shape[0])
+        if vis is None:
+            if ucuda:
+                tdt = torch.complex128 if self.vis_dtype == np.complex128 else torch.complex64
+                vis = torch.zeros((nrows, self.nchan), dtype=tdt, device=u.device)
+            else:
+                vis = np.zeros((nrows, self.nchan), dtype=self.vis_dtype)
+        v, vp, _, _ = _prep(vis, self.vis_dtype)
+        w, wp, _, _ = _prep(wgt, self.wgt_dtype)
+        m, mp, _, _ = _prep(mask, np.uint8)
+        self.ctx._bind_stream(u, v, w, m)
+        L.check(L.lib().wsg_stream_predict(self._h, nrows, up, vp, wp, mp))
+        self._hold((u, w, m))
+        return v
+
+    def stats(self):
+        s = L.WsgStats()
+        L.check(L.lib().wsg_stream_get_stats(self._h, ctypes.byref(s)))
+        return s.as_dict()
