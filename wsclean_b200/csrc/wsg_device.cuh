@@ -527,7 +527,7 @@ __device__ __forceinline__ double take_zero(double *p) {
 constexpr int kMaxOrig = 64;
 
 template <typename R, int W, int PPL, int NWARP>
-__global__ void __launch_bounds__(NWARP * 32)
+__global__ void __launch_bounds__(NWARP * 32, sizeof(R) == 4 ? 3 : 1)
 k_spread(GridArgs a, DevGeom g, DevKernel<R> kc) {
   using Rec = typename RecOf<R>::type;
   using C = typename Cplx<R>::type;
@@ -570,7 +570,7 @@ k_spread(GridArgs a, DevGeom g, DevKernel<R> kc) {
     __syncthreads();
     const int ch = sh_chunk;
     if (ch >= *a.nchunks) break;
-    const JobGeom jb = sh_job;
+    const JobGeom &jb = sh_job;  // read from shared memory where used
     const int s0 = a.chunk_start[ch];
     const int s1 = (ch + 1 < *a.nchunks) ? a.chunk_start[ch + 1] : a.nvis;
     const Rec r0 = recs[s0];
@@ -740,7 +740,7 @@ __device__ __forceinline__ void store_vis(void *out, int dbl, int accumulate, ui
 // (conjugation, conjugate shift phasor and weight); otherwise partial sums
 // go to a per-record accumulator finalised by k_finalize.
 template <typename R, int W, int PPL, int NWARP>
-__global__ void __launch_bounds__(NWARP * 32)
+__global__ void __launch_bounds__(NWARP * 32, sizeof(R) == 4 ? 3 : 1)
 k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
   using Rec = typename RecOf<R>::type;
   using C = typename Cplx<R>::type;
@@ -785,7 +785,7 @@ k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
     __syncthreads();
     const int ch = sh_chunk;
     if (ch >= *a.nchunks) break;
-    const JobGeom jb = sh_job;
+    const JobGeom &jb = sh_job;  // read from shared memory where used
     const int s0 = a.chunk_start[ch];
     const int s1 = (ch + 1 < *a.nchunks) ? a.chunk_start[ch + 1] : a.nvis;
     const Rec r0 = recs[s0];
