@@ -302,6 +302,37 @@ int wsg_stream_predict(wsg_stream *s, size_t nrows, const double *uvw, void *vis
 /* Grid choice of the stream (timings are zero). */
 int wsg_stream_get_stats(const wsg_stream *s, wsg_stats *out);
 
+/* -------------------------------------------------- imaging weights */
+
+/* WSClean's ImageWeights (structures/imageweights.h:30-100,
+ * structures/imageweights.cpp:36-143) on the GPU: visibility weights are
+ * summed on a width x height/2 grid over the v >= 0 half plane
+ * (x = floor(u W psx + W/2), y = floor(v H psy), u, v in wavelengths with
+ * lambda = c / f), finished into natural, uniform or Briggs weights, and
+ * looked up per visibility -- the imaging weight that
+ * MSGridderBase::readAndWeightVisibilities multiplies into each visibility
+ * weight (gridding/msgridderbase.cpp:583-590,642-659). */
+enum { WSG_WEIGHT_NATURAL = 0, WSG_WEIGHT_UNIFORM = 1, WSG_WEIGHT_BRIGGS = 2 };
+typedef struct wsg_weights wsg_weights;
+/* width, height, pixel scales: of the image; super_weight divides the grid
+ * size (rounded, made even); weights_as_taper: grid 1 for every nonzero
+ * weight. */
+int wsg_weights_create(wsg_ctx *ctx, int mode, double briggs_robust, size_t width, size_t height,
+                       double pixel_scale_x, double pixel_scale_y, int weights_as_taper,
+                       double super_weight, wsg_weights **out);
+int wsg_weights_destroy(wsg_weights *w);
+/* Adds nrows x nchan x npol visibility weights (NULL: all ones). */
+int wsg_weights_grid(wsg_weights *w, size_t nrows, size_t nchan, size_t npol, const double *uvw,
+                     const double *freq, const float *weights);
+/* FinishGridding (imageweights.cpp:113-143). */
+int wsg_weights_finish(wsg_weights *w);
+/* out[k] = in[k] (1 if in is NULL) x imaging weight of the visibility's cell. */
+int wsg_weights_apply(wsg_weights *w, size_t nrows, size_t nchan, size_t npol, const double *uvw,
+                      const double *freq, const float *in, float *out);
+/* The grid (width x height/2 doubles, index x + y*width; NULL to skip), its
+ * size and the sum of gridded weights. */
+int wsg_weights_get(wsg_weights *w, double *grid, size_t *width, size_t *height, double *total);
+
 #ifdef __cplusplus
 }
 #endif

@@ -84,3 +84,21 @@ def test_reference_report_parses():
                             prec=g["prec"], nthreads=1, return_report=True)
     r = O.parse_report(rep)
     assert r and r[0]["nu"] >= nx and r[0]["supp"] >= 4
+
+
+def test_imageweights_restatement_matches_briggs_helper():
+    """The oracle's ImageWeights and the synthetic-data Briggs helper are two
+    restatements of imageweights.cpp:113-143; they must agree."""
+    from oracle.imageweights import ImageWeights
+    from wsclean_b200 import synth
+    c = synth.config3(scale=0.02)
+    uvw, freq, nx, px = c["uvw"], c["freq"], c["npix_x"], c["pixsize"]
+    rng = np.random.default_rng(1)
+    noise = rng.uniform(0.5, 2.0, (len(uvw), len(freq)))
+    ref = ImageWeights(ImageWeights.BRIGGS, 0.0, nx, nx, px, px)
+    ref.grid_weights(uvw, freq, noise.astype(np.float32))
+    ref.finish()
+    iw = ref.apply(uvw, freq)[..., 0]
+    helper = synth.briggs_weights(uvw, freq, nx, nx, px, px, robust=0.0,
+                                  noise_weights=noise.astype(np.float32))
+    np.testing.assert_allclose(iw, helper, rtol=1e-6)

@@ -16,6 +16,7 @@ WSG_OK, WSG_ERR_INVALID, WSG_ERR_CUDA, WSG_ERR_NOMEM, WSG_ERR_CUFFT, WSG_ERR_STA
 WSG_ERR_INTERNAL = 7
 WSG_PREC_MIXED, WSG_PREC_FP64 = 0, 1
 WSG_C64, WSG_C128 = 0, 1
+WSG_WEIGHT_NATURAL, WSG_WEIGHT_UNIFORM, WSG_WEIGHT_BRIGGS = 0, 1, 2
 WSG_F32, WSG_F64 = 0, 1
 
 # Every symbol include/wsg.h declares (checked by the CPU test suite).
@@ -32,6 +33,8 @@ EXPORTED = [
     "wsg_plan_get_stats", "wsg_ctx_synchronize",
     "wsg_stream_create", "wsg_stream_destroy", "wsg_stream_add", "wsg_stream_finish",
     "wsg_stream_predict_begin", "wsg_stream_predict", "wsg_stream_get_stats",
+    "wsg_weights_create", "wsg_weights_destroy", "wsg_weights_grid", "wsg_weights_finish",
+    "wsg_weights_apply", "wsg_weights_get",
 ]
 
 c_size_t, c_double, c_int, c_void_p = ctypes.c_size_t, ctypes.c_double, ctypes.c_int, ctypes.c_void_p
@@ -153,6 +156,13 @@ def lib():
         L.wsg_stream_predict_begin.argtypes = [vp, vp]
         L.wsg_stream_predict.argtypes = [vp, c_size_t, vp, vp, vp, vp]
         L.wsg_stream_get_stats.argtypes = [vp, P(WsgStats)]
+        L.wsg_weights_create.argtypes = [vp, c_int, c_double, c_size_t, c_size_t, c_double,
+                                         c_double, c_int, c_double, P(vp)]
+        L.wsg_weights_destroy.argtypes = [vp]
+        L.wsg_weights_grid.argtypes = [vp, c_size_t, c_size_t, c_size_t, vp, vp, vp]
+        L.wsg_weights_finish.argtypes = [vp]
+        L.wsg_weights_apply.argtypes = [vp, c_size_t, c_size_t, c_size_t, vp, vp, vp, vp]
+        L.wsg_weights_get.argtypes = [vp, vp, P(c_size_t), P(c_size_t), P(c_double)]
         L.wsg_last_error.restype = ctypes.c_char_p
         L.wsg_abi_version.restype = c_int
         for name in EXPORTED:

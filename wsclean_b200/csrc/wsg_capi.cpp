@@ -20,6 +20,10 @@ struct wsg_plan {
   std::unique_ptr<wsg::Plan> impl;
   wsg_ctx *ctx = nullptr;
 };
+struct wsg_weights {
+  std::unique_ptr<wsg::ImageWeightsGpu> impl;
+  wsg_ctx *ctx = nullptr;
+};
 struct wsg_stream {
   std::unique_ptr<wsg::StreamGridder> impl;
   wsg_ctx *ctx = nullptr;
@@ -366,6 +370,64 @@ int wsg_stream_get_stats(const wsg_stream *s, wsg_stats *out) {
   return guarded([&] {
     wsg::require(s != nullptr && out != nullptr, "stream and out are required");
     s->impl->stats(*out);
+  });
+}
+
+int wsg_weights_create(wsg_ctx *ctx, int mode, double briggs_robust, size_t width, size_t height,
+                       double pixel_scale_x, double pixel_scale_y, int weights_as_taper,
+                       double super_weight, wsg_weights **out) {
+  return guarded([&] {
+    wsg::require(ctx != nullptr && out != nullptr, "ctx and out are required");
+    auto *h = new wsg_weights;
+    try {
+      h->impl.reset(new wsg::ImageWeightsGpu(*ctx->ctx, mode, briggs_robust, width, height,
+                                             pixel_scale_x, pixel_scale_y, weights_as_taper != 0,
+                                             super_weight));
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    h->ctx = ctx;
+    ++ctx->plans;
+    *out = h;
+  });
+}
+
+int wsg_weights_destroy(wsg_weights *w) {
+  return guarded([&] {
+    if (!w) return;
+    if (w->ctx) --w->ctx->plans;
+    delete w;
+  });
+}
+
+int wsg_weights_grid(wsg_weights *w, size_t nrows, size_t nchan, size_t npol, const double *uvw,
+                     const double *freq, const float *weights) {
+  return guarded([&] {
+    wsg::require(w != nullptr, "weights handle is NULL");
+    w->impl->grid(nrows, nchan, npol, uvw, freq, weights);
+  });
+}
+
+int wsg_weights_finish(wsg_weights *w) {
+  return guarded([&] {
+    wsg::require(w != nullptr, "weights handle is NULL");
+    w->impl->finish();
+  });
+}
+
+int wsg_weights_apply(wsg_weights *w, size_t nrows, size_t nchan, size_t npol, const double *uvw,
+                      const double *freq, const float *in, float *out) {
+  return guarded([&] {
+    wsg::require(w != nullptr, "weights handle is NULL");
+    w->impl->apply(nrows, nchan, npol, uvw, freq, in, out);
+  });
+}
+
+int wsg_weights_get(wsg_weights *w, double *grid, size_t *width, size_t *height, double *total) {
+  return guarded([&] {
+    wsg::require(w != nullptr, "weights handle is NULL");
+    w->impl->get(grid, width, height, total);
   });
 }
 

@@ -226,6 +226,30 @@ class StreamGridder {
   size_t k_ = 0;
 };
 
+// ImageWeights on the device (see wsg_weights_create).
+class ImageWeightsGpu {
+ public:
+  ImageWeightsGpu(Context &cx, int mode, double robust, size_t width, size_t height, double psx,
+                  double psy, bool as_taper, double super_weight);
+  ~ImageWeightsGpu();
+  void grid(size_t nrows, size_t nchan, size_t npol, const double *uvw, const double *freq,
+            const float *w);
+  void finish();
+  void apply(size_t nrows, size_t nchan, size_t npol, const double *uvw, const double *freq,
+             const float *in, float *out);
+  void get(double *grid, size_t *width, size_t *height, double *total);
+
+ private:
+  const double *lambdas(size_t nchan, const double *freq);
+  Context &cx_;
+  int mode_;
+  double robust_;
+  size_t W_, H_;
+  double psx_, psy_;
+  bool as_taper_, finished_ = false;
+  DevBuf grid_, sums_, lambda_, in_, out_;
+};
+
 // Allocation-free mixed-precision ms2dirty (scratch in a static device array).
 void ms2dirty_noalloc(const wsg_args &a, const void *vis, void *dirty, cudaStream_t stream);
 

@@ -1413,6 +1413,99 @@ k_row_fft(void *data, long long rows, const void *twv, int sign) {
     if (rv) d[row * M + t + TPF * r] = bufall[grp * BL + fpad(t + TPF * r)];
 }
 
+// ------------------------------------------------------- image weights
+//
+// WSClean's ImageWeights (structures/imageweights.h:36-100,
+// structures/imageweights.cpp:78-143) on the device: a width x height/2 grid
+// of summed visibility weights over the v >= 0 half plane, finished into
+// natural, uniform or Briggs imaging weights, then looked up per visibility.
+// (u, v) are in wavelengths, u / lambda with lambda = c / f per channel.
+
+struct WeightGrid {
+  int W, H;        // grid is W x H/2
+  double psx, psy; // pixel scales (radians)
+};
+
+__device__ __forceinline__ bool weight_cell(const WeightGrid &g, double u, double v, int &x,
+                                            int &y) {
+  if (v < 0.0) {
+    u = -u;
+    v = -v;
+  }
+  x = int(floor(u * double(g.W) * g.psx + double(g.W / 2)));
+  y = int(floor(v * double(g.H) * g.psy));
+  return x >= 0 && x < g.W && y < g.H / 2;
+}
+
+__global__ void k_weights_grid(size_t nrows, int nchan, int npol, const double *__restrict__ uvw,
+                               const double *__restrict__ lambda, const float *__restrict__ wgt,
+                               int as_taper, WeightGrid g, double *__restrict__ grid,
+                               double *__restrict__ total) {
+  double sum = 0.0;
+  for (size_t r = blockIdx.x * size_t(blockDim.x) + threadIdx.x; r < nrows;
+       r += size_t(gridDim.x) * blockDim.x) {
+    for (int c = 0; c < nchan; ++c) {
+      const double u = uvw[3 * r] / lambda[c], v = uvw[3 * r + 1] / lambda[c];
+      int x, y;
+      const bool in = weight_cell(g, u, v, x, y);
+      for (int p = 0; p < npol; ++p) {
+        float w = wgt ? wgt[(r * nchan + c) * npol + p] : 1.0f;
+        if (as_taper && w != 0.0f) w = 1.0f;
+        if (in) {
+          atomicAdd(&grid[size_t(x) + size_t(y) * g.W], double(w));
+          sum += double(w);
+        }
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+  if ((threadIdx.x & 31) == 0 && sum != 0.0) atomicAdd(total, sum);
+}
+
+__global__ void k_weights_sumsq(size_t n, const double *__restrict__ grid, double *__restrict__ out) {
+  double s = 0.0;
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n;
+       i += size_t(gridDim.x) * blockDim.x)
+    s += grid[i] * grid[i];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0 && s != 0.0) atomicAdd(out, s);
+}
+
+// mode 0 natural, 1 uniform, 2 Briggs (s2 = (5 * 10^-robust)^2 / (sum W^2 / sum W))
+__global__ void k_weights_finish(size_t n, double *__restrict__ grid, int mode,
+                                 const double *__restrict__ sums, double num_sq) {
+  const double s2 = mode == 2 ? num_sq / (sums[1] / sums[0]) : 0.0;
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n;
+       i += size_t(gridDim.x) * blockDim.x) {
+    const double v = grid[i];
+    if (mode == 2)
+      grid[i] = 1.0 / (1.0 + v * s2);
+    else if (mode == 1)
+      grid[i] = v != 0.0 ? 1.0 / v : 0.0;
+    else
+      grid[i] = v != 0.0 ? 1.0 : v;
+  }
+}
+
+// out = in * imaging weight of the visibility's cell (0 outside the grid)
+__global__ void k_weights_apply(size_t nrows, int nchan, int npol, const double *__restrict__ uvw,
+                                const double *__restrict__ lambda, WeightGrid g,
+                                const double *__restrict__ grid, const float *__restrict__ in,
+                                float *__restrict__ out) {
+  for (size_t r = blockIdx.x * size_t(blockDim.x) + threadIdx.x; r < nrows;
+       r += size_t(gridDim.x) * blockDim.x) {
+    for (int c = 0; c < nchan; ++c) {
+      const double u = uvw[3 * r] / lambda[c], v = uvw[3 * r + 1] / lambda[c];
+      int x, y;
+      const double iw = weight_cell(g, u, v, x, y) ? grid[size_t(x) + size_t(y) * g.W] : 0.0;
+      for (int p = 0; p < npol; ++p) {
+        const size_t k = (r * nchan + c) * npol + p;
+        out[k] = float(double(in ? in[k] : 1.0f) * iw);
+      }
+    }
+  }
+}
+
 // ------------------------------------------------------------- screens
 
 struct ScreenArgs {

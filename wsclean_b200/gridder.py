@@ -570,3 +570,78 @@ class Stream:
         s = L.WsgStats()
         L.check(L.lib().wsg_stream_get_stats(self._h, ctypes.byref(s)))
         return s.as_dict()
+
+
+class ImageWeights:
+    """WSClean's ImageWeights on the GPU (``wsg_weights_*``): ``grid`` the
+    visibility weights of any number of chunks, ``finish`` into natural,
+    uniform or Briggs weights, ``apply`` to get each visibility's weight
+    times its imaging weight (what MSGridderBase multiplies into the data)."""
+
+    NATURAL, UNIFORM, BRIGGS = L.WSG_WEIGHT_NATURAL, L.WSG_WEIGHT_UNIFORM, L.WSG_WEIGHT_BRIGGS
+
+    def __init__(self, mode, robust, width, height, pixel_scale_x, pixel_scale_y,
+                 weights_as_taper=False, super_weight=1.0, context=None, device=-1):
+        if isinstance(mode, str):
+            mode = {"natural": self.NATURAL, "uniform": self.UNIFORM, "briggs": self.BRIGGS}[mode]
+        self.ctx = context if context is not None else Context(device)
+        self._own_ctx = context is None
+        h = ctypes.c_void_p()
+        L.check(L.lib().wsg_weights_create(self.ctx._h, int(mode), float(robust), int(width),
+                                           int(height), float(pixel_scale_x),
+                                           float(pixel_scale_y), int(bool(weights_as_taper)),
+                                           float(super_weight), ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            L.lib().wsg_weights_destroy(self._h)
+            self._h = None
+        if getattr(self, "_own_ctx", False) and self.ctx is not None:
+            self.ctx.close()
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def grid(self, uvw, freq, weights=None, npol=1):
+        u, up, _, _ = _prep(uvw, np.float64)
+        f, fp, _, _ = _prep(freq, np.float64)
+        w, wp, _, _ = _prep(weights, np.float32)
+        self.ctx._bind_stream(u, w)
+        L.check(L.lib().wsg_weights_grid(self._h, int(u.shape[0]), int(f.shape[0]), int(npol),
+                                         up, fp, wp))
+
+    def finish(self):
+        L.check(L.lib().wsg_weights_finish(self._h))
+
+    def apply(self, uvw, freq, weights=None, npol=1, out=None):
+        u, up, _, ucuda = _prep(uvw, np.float64)
+        f, fp, _, _ = _prep(freq, np.float64)
+        w, wp, _, _ = _prep(weights, np.float32)
+        shape = (int(u.shape[0]), int(f.shape[0])) + ((int(npol),) if npol > 1 else ())
+        if out is None:
+            out = (torch.zeros(shape, dtype=torch.float32, device=u.device) if ucuda
+                   else np.zeros(shape, dtype=np.float32))
+        o, op, _, _ = _prep(out, np.float32)
+        self.ctx._bind_stream(u, w, o)
+        L.check(L.lib().wsg_weights_apply(self._h, shape[0], shape[1], int(npol), up, fp, wp, op))
+        return o
+
+    def grid_array(self):
+        """(grid as a (height/2, width) array indexed [y, x], total weight)."""
+        wd, ht, tot = ctypes.c_size_t(), ctypes.c_size_t(), ctypes.c_double()
+        L.check(L.lib().wsg_weights_get(self._h, None, ctypes.byref(wd), ctypes.byref(ht),
+                                        ctypes.byref(tot)))
+        g = np.zeros((ht.value // 2, wd.value))
+        L.check(L.lib().wsg_weights_get(self._h, g.ctypes.data, None, None, None))
+        return g, tot.value
