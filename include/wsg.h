@@ -207,6 +207,16 @@ int wsg_get_stats(const wsg_ctx *ctx, wsg_stats *out);
  * kernel_err, wmin, wmax, dw, nshift and precision. */
 int wsg_plan_grid(const wsg_args *a, size_t nvis, double wmin, double wmax, double umax,
                   double vmax, wsg_stats *out);
+/* Autotuner: times ms2dirty + dirty2ms on these arguments and data for the
+ * `candidates` cheapest kernel choices (support W, oversampling sigma, hence
+ * grid size and w-plane count) of the cost model and the bin tile sizes,
+ * and keeps the fastest for later calls on any context of this process with
+ * the same image size, precision, epsilon, w-gridding flag and number of
+ * visibilities within a factor of two.  best: the chosen grid (ms_total =
+ * its time per pair in ms).  Accuracy is unaffected: every candidate meets
+ * epsilon.  Extension of the reference interface. */
+int wsg_autotune(wsg_ctx *ctx, const wsg_args *a, const void *vis, int candidates,
+                 wsg_stats *best);
 /* Message of the last failed call on this thread ("" if none). */
 const char *wsg_last_error(void);
 int wsg_abi_version(void);

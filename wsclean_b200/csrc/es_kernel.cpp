@@ -13,6 +13,9 @@
 #include <algorithm>
 #include <cmath>
 #include <limits>
+#include <tuple>
+#include <utility>
+#include <vector>
 
 #include "wsg_internal.h"
 
@@ -389,6 +392,7 @@ void choose_grid(GridPlan &g, double sigma_min, double sigma_max, int tile, bool
     }
   }
   require(bnu > 0, "no grid size satisfies the pruned-FFT layout (image or band too large)");
+  g.cost = best;
   g.kernel = bestk;
   g.nu = bnu;
   g.nv = bnv;
@@ -434,6 +438,27 @@ void choose_grid(GridPlan &g, double sigma_min, double sigma_max, int tile, bool
   int tbits = ceil_log2(uint64_t(tile));
   g.lbits = std::min(tbits, (30 - bin_bits) / 2);
   g.key_bits = bin_bits + 2 * g.lbits;
+}
+
+std::vector<std::pair<int, double>> rank_kernels(const GridPlan &g, double sigma_min,
+                                                 double sigma_max, int tile, size_t n) {
+  std::vector<std::tuple<double, int, double>> all;
+  for (const auto &k : available_kernels(g.eps, g.do_w ? 3 : 2, g.fp32, sigma_min, sigma_max)) {
+    GridPlan t = g;
+    t.force_W = k.W;
+    t.force_sigma = k.sigma;
+    try {
+      choose_grid(t, sigma_min, sigma_max, tile);
+    } catch (const std::exception &) {
+      continue;
+    }
+    all.emplace_back(t.cost, k.W, k.sigma);
+  }
+  std::sort(all.begin(), all.end());
+  std::vector<std::pair<int, double>> out;
+  for (size_t i = 0; i < all.size() && out.size() < n; ++i)
+    out.emplace_back(std::get<1>(all[i]), std::get<2>(all[i]));
+  return out;
 }
 
 size_t plan_bytes(const GridPlan &g, size_t planes, bool gridding) {

@@ -431,4 +431,12 @@ int wsg_weights_get(wsg_weights *w, double *grid, size_t *width, size_t *height,
   });
 }
 
+int wsg_autotune(wsg_ctx *ctx, const wsg_args *a, const void *vis, int candidates,
+                 wsg_stats *best) {
+  return guarded([&] {
+    wsg::require(ctx != nullptr && a != nullptr && best != nullptr, "ctx, args and best are required");
+    ctx->ctx->autotune(*a, vis, candidates, *best);
+  });
+}
+
 }  // extern "C"

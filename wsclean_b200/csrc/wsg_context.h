@@ -36,6 +36,16 @@ struct Layout {
 class Plan;
 class StreamGridder;
 
+// A timed kernel / tile choice of the autotuner.
+struct TuneChoice {
+  int W = 0;
+  double sigma = 0;
+  int tile = 0;
+  double ms = 0;
+};
+bool tuned_choice(const wsg_args &a, size_t nvis, TuneChoice &out);
+void store_tuned(const wsg_args &a, size_t nvis, const TuneChoice &c);
+
 // Device pointers of one call's inputs.
 struct Staged {
   const double *uvw = nullptr;
@@ -56,6 +66,11 @@ class Context {
   void dirty2ms(const wsg_args &a, const void *dirty, void *vis);
   void release_buffers();
   void synchronize();
+  // Times the pair (ms2dirty + dirty2ms) on these data for the `candidates`
+  // cheapest kernels of the cost model and the tile sizes, and keeps the
+  // fastest for later calls of the same image size, precision, accuracy and
+  // visibility count (within a factor of two).
+  void autotune(const wsg_args &a, const void *vis, int candidates, wsg_stats &best);
   size_t device_bytes();
   void validate(const wsg_args &a);
 
@@ -98,6 +113,10 @@ class Context {
   void mark(const char *what);
   void print_marks(const char *title);
   std::vector<std::pair<const char *, std::chrono::steady_clock::time_point>> marks;
+
+  // autotuner: a forced (W, sigma, tile) while candidates are timed
+  int tune_W = 0, tune_tile = 0;
+  double tune_sigma = 0;
 
   cudaEvent_t ev[8];
   std::map<std::tuple<int, int, int, int, int, int, int>, cufftHandle> fft_plans;

@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace wsg {
@@ -130,6 +131,8 @@ struct GridPlan {
   // streams: the grid was planned from a declared data extent; chunks are
   // checked against it instead of re-planning
   bool fixed = false;
+  // modelled time of the chosen grid (seconds)
+  double cost = 0;
 };
 
 // Parameter choice (the analogue of ducc0 Params::getNuNv, wgridder.h:1503-1576,
@@ -138,6 +141,11 @@ struct GridPlan {
 // pow2_v: restrict nv to a power of two (for the FFT along v by the
 // library's own shared-memory kernel instead of cuFFT).
 void choose_grid(GridPlan &g, double sigma_min, double sigma_max, int tile, bool pow2_v = false);
+
+// The n cheapest kernels (W, sigma) for these inputs by the cost model of
+// choose_grid, cheapest first (the autotuner times them).
+std::vector<std::pair<int, double>> rank_kernels(const GridPlan &g, double sigma_min,
+                                                 double sigma_max, int tile, size_t n);
 
 // Nominal device bytes for one pass with `planes` planes resident.
 size_t plan_bytes(const GridPlan &g, size_t planes, bool gridding);

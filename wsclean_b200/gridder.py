@@ -161,6 +161,30 @@ class Context:
         L.check(L.lib().wsg_ms2dirty(self._h, ctypes.byref(a), vp, dp, int(bool(accumulate))))
         return d
 
+    def autotune(self, uvw, freq, vis, npix_x, npix_y, pixsize_x, pixsize_y, epsilon,
+                 candidates=4, do_wgridding=True, wgt=None, mask=None, negate_v=False,
+                 divide_by_n=True, sigma_min=1.1, sigma_max=2.6, center_x=0.0, center_y=0.0,
+                 precision="mixed", dirty_dtype=None):
+        """Times the pair on these data for the `candidates` cheapest kernel
+        choices and tile sizes and keeps the fastest for later calls with the
+        same image size, precision and epsilon (``wsg_autotune``).  Returns the
+        chosen grid's stats (ms_total = ms per pair)."""
+        keep = []
+        v, vp, vdt, _ = _prep(vis)
+        if vdt not in _NP_C:
+            v, vp, vdt, _ = _prep(vis, np.complex64)
+        keep.append(v)
+        nrows, nchan = v.shape
+        ddt = np.dtype(dirty_dtype) if dirty_dtype is not None else (
+            np.dtype(np.float64) if _precision(precision) == L.WSG_PREC_FP64 else np.dtype(np.float32))
+        a = self._args(uvw, freq, nrows, nchan, wgt, mask, npix_x, npix_y, pixsize_x, pixsize_y,
+                       epsilon, do_wgridding, negate_v, divide_by_n, sigma_min, sigma_max,
+                       center_x, center_y, precision, _NP_C[vdt], _NP_F[ddt], keep)
+        self._bind_stream(v, *keep)
+        s = L.WsgStats()
+        L.check(L.lib().wsg_autotune(self._h, ctypes.byref(a), vp, int(candidates), ctypes.byref(s)))
+        return s.as_dict()
+
     def dirty2ms(self, uvw, freq, dirty, pixsize_x, pixsize_y, epsilon, do_wgridding=True,
                  wgt=None, mask=None, negate_v=False, divide_by_n=True, sigma_min=1.1,
                  sigma_max=2.6, center_x=0.0, center_y=0.0, precision="mixed",
