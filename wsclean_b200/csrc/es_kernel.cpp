@@ -296,6 +296,20 @@ void set_band(GridPlan &g) {
 // nu = K * 2^m with 2^m >= 2L+1, so that the occupied u band fits one pruned
 // FFT of length 2^m (or K = 1, 2^m = nu when the band covers the grid);
 // the smallest such nu >= n0.
+// Shared memory of one spread / interpolation CTA: the W-plane tile of
+// (T + W - 1)^2 cells (odd row stride, plane stride 8 mod 32, real and
+// imaginary parts) and 8 warps' record staging (the layout of the device
+// kernels, GridKernels::smem_bytes).
+size_t tile_smem_bytes(int T, int W, bool fp32) {
+  const size_t rs = fp32 ? 4 : 8;
+  const size_t S = size_t(T + W - 1), RS = S | 1;
+  size_t PS = S * RS;
+  PS += ((8 - (PS % 32)) + 32) % 32;
+  const size_t kst = fp32 ? ((3 * size_t(W) + 3) & ~size_t(3)) : ((3 * size_t(W) + 1) & ~size_t(1));
+  const size_t stage = rs * (32 * kst + 64) + 128;
+  return ((rs * 2 * size_t(W) * PS + 15) & ~size_t(15)) + 8 * stage;
+}
+
 bool pick_nu(double n0, double umax_px, int W, bool fp32, size_t &nu, int &logM, int &K) {
   const int mmax = fp32 ? 13 : 12;
   size_t best = ~size_t(0);
@@ -426,8 +440,10 @@ void choose_grid(GridPlan &g, double sigma_min, double sigma_max, int tile, bool
   double target = g.fp32 ? std::max(0.02 * g.kernel.err, 2e-8) : 0.02 * g.kernel.err;
   g.poly = fit_poly_kernel(g.kernel, target);
 
-  // a tile row plus halo (T + W - 1 cells) is staged by one warp's lanes
+  // a tile row plus halo (T + W - 1 cells) is staged by one warp's lanes,
+  // and the tile plus the warps' staging areas must fit in shared memory
   tile = std::max(1, std::min(tile, 33 - W));
+  while (tile > 1 && tile_smem_bytes(tile, W, g.fp32) > kMaxSmemPerBlock) --tile;
   g.T = tile;
   g.ntu = int((g.nu + 1) / tile) + 1;
   g.ntv = int((g.nv + 1) / tile) + 1;

@@ -324,7 +324,10 @@ struct GridKernels {
     const size_t stage = sizeof(R) * (32 * kst + 64) + 128;  // WarpStage<R, W>::bytes
     size_t tile = ((sizeof(R) * 2 * size_t(W) * tl.PS) + 15) & ~size_t(15);
     (void)spread;
-    return tile + size_t(NWARP) * stage;
+    const size_t b = tile + size_t(NWARP) * stage;
+    require(b == tile_smem_bytes(tl.S - W + 1, W, sizeof(R) == 4) && b <= kMaxSmemPerBlock,
+            "internal: spread tile exceeds shared memory");
+    return b;
   }
   // warps that share one record (more than one when a lane's share of the
   // W x W (plane, u-row) pairs would exceed PPL)
@@ -2276,7 +2279,11 @@ void Context::autotune(const wsg_args &a, const void *vis, int candidates, wsg_s
         double ms;
         try {
           ms = time_pair();
-        } catch (const OutOfMemory &) {
+        } catch (const std::exception &e) {  // a candidate that cannot run is skipped
+          cudaGetLastError();
+          if (verbosity > 0)
+            std::printf("autotune: W=%d sigma=%.3f tile=%d skipped: %s\n", c.first, c.second, T,
+                        e.what());
           continue;
         }
         if (verbosity > 0)

@@ -147,6 +147,10 @@ void choose_grid(GridPlan &g, double sigma_min, double sigma_max, int tile, bool
 std::vector<std::pair<int, double>> rank_kernels(const GridPlan &g, double sigma_min,
                                                  double sigma_max, int tile, size_t n);
 
+// Shared memory of a spread / interpolation CTA for tile T and support W.
+constexpr size_t kMaxSmemPerBlock = 227 * 1024;
+size_t tile_smem_bytes(int T, int W, bool fp32);
+
 // Nominal device bytes for one pass with `planes` planes resident.
 size_t plan_bytes(const GridPlan &g, size_t planes, bool gridding);
 
