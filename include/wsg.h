@@ -73,6 +73,17 @@ int wsg_ctx_destroy(wsg_ctx *ctx);
 int wsg_ctx_set_stream(wsg_ctx *ctx, void *stream);
 /* Releases the cached device buffers and cuFFT plans (they regrow on demand). */
 int wsg_ctx_release_buffers(wsg_ctx *ctx);
+/* Pipelined mode for wsg_ms2dirty / wsg_dirty2ms (0: off, the default).
+ * Every call stages its inputs through one of two buffer slots on a copy
+ * stream and writes host outputs back on a third stream, so consecutive
+ * calls overlap their transfers with each other's kernels; with async != 0
+ * the calls return once their work is enqueued (after the short planning
+ * read-back of the visibility scan), outputs are valid after
+ * wsg_ctx_synchronize, which also reports errors detected on the device,
+ * and host outputs should be page-locked for the copies to overlap.  Not
+ * for a gridder's context (wsg_gridder_ctx).  Extension of the reference
+ * interface, whose calls are synchronous. */
+int wsg_ctx_set_async(wsg_ctx *ctx, int async);
 
 /* ------------------------------------------------------- raw operators */
 

@@ -34,7 +34,7 @@ EXPORTED = [
     "wsg_stream_create", "wsg_stream_destroy", "wsg_stream_add", "wsg_stream_finish",
     "wsg_stream_predict_begin", "wsg_stream_predict", "wsg_stream_get_stats",
     "wsg_weights_create", "wsg_weights_destroy", "wsg_weights_grid", "wsg_weights_finish",
-    "wsg_weights_apply", "wsg_weights_get", "wsg_autotune",
+    "wsg_weights_apply", "wsg_weights_get", "wsg_autotune", "wsg_ctx_set_async",
 ]
 
 c_size_t, c_double, c_int, c_void_p = ctypes.c_size_t, ctypes.c_double, ctypes.c_int, ctypes.c_void_p
@@ -164,6 +164,7 @@ def lib():
         L.wsg_weights_apply.argtypes = [vp, c_size_t, c_size_t, c_size_t, vp, vp, vp, vp]
         L.wsg_weights_get.argtypes = [vp, vp, P(c_size_t), P(c_size_t), P(c_double)]
         L.wsg_autotune.argtypes = [vp, P(WsgArgs), vp, c_int, P(WsgStats)]
+        L.wsg_ctx_set_async.argtypes = [vp, c_int]
         L.wsg_last_error.restype = ctypes.c_char_p
         L.wsg_abi_version.restype = c_int
         for name in EXPORTED:

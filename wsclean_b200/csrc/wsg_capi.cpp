@@ -117,6 +117,15 @@ int wsg_ctx_set_stream(wsg_ctx *ctx, void *stream) {
   });
 }
 
+int wsg_ctx_set_async(wsg_ctx *ctx, int async) {
+  return guarded([&] {
+    wsg::require(ctx != nullptr, "ctx is NULL");
+    wsg::require(ctx->own != nullptr, "a gridder's context stays synchronous");
+    if (!async && ctx->ctx->async_mode) ctx->ctx->synchronize();
+    ctx->ctx->async_mode = async != 0;
+  });
+}
+
 int wsg_ctx_release_buffers(wsg_ctx *ctx) {
   return guarded([&] {
     wsg::require(ctx != nullptr, "ctx is NULL");

@@ -126,6 +126,10 @@ Context::Context(int dev) {
   stream = own_stream;
   CK(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
   for (auto &e : ev) CK(cudaEventCreate(&e));
+  CK(cudaStreamCreateWithFlags(&cpy, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&d2h, cudaStreamNonBlocking));
+  for (cudaEvent_t *e : {&ev_start, &ev_in, &ev_done, &ev_scan, &slots[0].free_ev, &slots[1].free_ev})
+    CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
   std::memset(&stats, 0, sizeof(stats));
   verbosity = env_int("WSG_VERBOSITY", 0);
 }
@@ -152,6 +156,15 @@ Context::~Context() {
   for (auto &kv : fft_plans) cufftDestroy(kv.second);
   for (auto *b : all_buffers()) b->release();
   for (auto &e : ev) cudaEventDestroy(e);
+  for (cudaStream_t st : {cpy, d2h})
+    if (st) {
+      cudaStreamSynchronize(st);
+      cudaStreamDestroy(st);
+    }
+  for (cudaEvent_t e : {ev_start, ev_in, ev_done, ev_scan, slots[0].free_ev, slots[1].free_ev})
+    if (e) cudaEventDestroy(e);
+  for (auto &sl : slots)
+    for (DevBuf *b : {&sl.uvw, &sl.vis, &sl.wgt, &sl.mask, &sl.out, &sl.fovc}) b->release();
   if (own_stream) cudaStreamDestroy(own_stream);
 }
 
@@ -164,11 +177,20 @@ std::vector<DevBuf *> Context::all_buffers() {
 void Context::synchronize() {
   CK(cudaSetDevice(device));
   CK(cudaStreamSynchronize(stream));
+  CK(cudaStreamSynchronize(d2h));
+  if (err_pending) {
+    err_pending = false;
+    check_device_error(reinterpret_cast<const int *>(reinterpret_cast<char *>(b_small.p) + 3072));
+  }
 }
 
 void Context::release_buffers() {
   CK(cudaSetDevice(device));
   CK(cudaStreamSynchronize(stream));
+  CK(cudaStreamSynchronize(d2h));
+  CK(cudaStreamSynchronize(cpy));
+  for (auto &sl : slots)
+    for (DevBuf *b : {&sl.uvw, &sl.vis, &sl.wgt, &sl.mask, &sl.out, &sl.fovc}) b->release();
   for (auto &kv : fft_plans) cufftDestroy(kv.second);
   fft_plans.clear();
   for (auto *b : all_buffers()) b->release();
@@ -215,11 +237,11 @@ void Context::fft_exec(cufftHandle h, void *in, void *out, int dir, bool dbl) {
 
 // Returns a device pointer holding `bytes` of p: p itself if it is device
 // memory, else a copy in buf (asynchronous on the context stream).
-const void *Context::stage_in(const void *p, size_t bytes, DevBuf &buf) {
+const void *Context::stage_in(const void *p, size_t bytes, DevBuf &buf, cudaStream_t st) {
   if (!p) return nullptr;
   if (is_device_pointer(p)) return p;
   void *d = buf.ensure(bytes);
-  CK(cudaMemcpyAsync(d, p, bytes, cudaMemcpyHostToDevice, stream));
+  CK(cudaMemcpyAsync(d, p, bytes, cudaMemcpyHostToDevice, st ? st : stream));
   return d;
 }
 
@@ -456,10 +478,10 @@ namespace {
 
 template <typename TW, typename TV>
 void launch_scan(Context &cx, const wsg_args &a, const Staged &s, bool gridding, TV *vis_out,
-                 ScanOut *d_out) {
+                 ScanOut *d_out, cudaStream_t st) {
   int nb = launch_blocks(a.nrows, 256);
   nb = std::min(nb, cx.num_sms * 8);
-  k_scan<TV, TW><<<nb, 256, 0, cx.stream>>>(
+  k_scan<TV, TW><<<nb, 256, 0, st>>>(
       a.nrows, int(a.nchan), s.uvw, s.fovc, reinterpret_cast<const TV *>(s.vis),
       reinterpret_cast<const TW *>(s.wgt), s.mask, gridding ? 1 : 0, a.negate_v ? -1.0 : 1.0,
       d_out, vis_out);
@@ -538,8 +560,13 @@ bool Context::prepare(const wsg_args &a, const Staged &s, bool gridding, void *v
     if (i > 0) require(freq[i] >= freq[i - 1], "channel frequencies must be sorted in ascending order");
     fovc[i] = freq[i] / kSpeedOfLight;
   }
-  double *d_fovc = reinterpret_cast<double *>(b_fovc.ensure(a.nchan * sizeof(double)));
-  CK(cudaMemcpyAsync(d_fovc, fovc.data(), a.nchan * sizeof(double), cudaMemcpyHostToDevice, stream));
+  // the scan runs on scan_st when the raw operators staged every input it
+  // reads on the copy stream: its read-back then waits for this call's
+  // copies only, not for earlier calls' kernels on the main stream
+  cudaStream_t sst = scan_st ? scan_st : stream;
+  DevBuf &fbuf = fovc_buf ? *fovc_buf : b_fovc;
+  double *d_fovc = reinterpret_cast<double *>(fbuf.ensure(a.nchan * sizeof(double)));
+  CK(cudaMemcpyAsync(d_fovc, fovc.data(), a.nchan * sizeof(double), cudaMemcpyHostToDevice, sst));
   Staged st = s;
   st.fovc = d_fovc;
 
@@ -547,16 +574,22 @@ bool Context::prepare(const wsg_args &a, const Staged &s, bool gridding, void *v
   ScanOut h0{};
   h0.wmin_bits = 0x7ff0000000000000ull;
   ScanOut *d_scan = reinterpret_cast<ScanOut *>(b_small.ensure(4096));
-  CK(cudaMemcpyAsync(d_scan, &h0, sizeof(h0), cudaMemcpyHostToDevice, stream));
+  CK(cudaMemcpyAsync(d_scan, &h0, sizeof(h0), cudaMemcpyHostToDevice, sst));
+  // (off the main stream the caller zeroes the whole output itself)
+  void *zero_out = scan_st ? nullptr : vis_out_dev;
   with_types(a, [&](auto *tw, auto *tv) {
     using TW = std::remove_pointer_t<decltype(tw)>;
     using TV = std::remove_pointer_t<decltype(tv)>;
-    launch_scan<TW, TV>(*this, a, st, gridding, reinterpret_cast<TV *>(vis_out_dev), d_scan);
+    launch_scan<TW, TV>(*this, a, st, gridding, reinterpret_cast<TV *>(zero_out), d_scan, sst);
   });
   ScanOut hs;
-  CK(cudaMemcpyAsync(&hs, d_scan, sizeof(hs), cudaMemcpyDeviceToHost, stream));
+  CK(cudaMemcpyAsync(&hs, d_scan, sizeof(hs), cudaMemcpyDeviceToHost, sst));
   mark("scan-submit");
-  CK(cudaStreamSynchronize(stream));
+  CK(cudaStreamSynchronize(sst));
+  if (sst != stream) {  // keys and records read the uploaded f/c
+    CK(cudaEventRecord(ev_scan, sst));
+    CK(cudaStreamWaitEvent(stream, ev_scan, 0));
+  }
   mark("scan-sync");
   gp.nvis = hs.nvis;
   if (gp.nvis == 0) return false;
@@ -707,7 +740,8 @@ ChebCorr Context::upload_corrections(const GridPlan &g) {
   for (size_t i = 0; i <= g.nx / 2; ++i) cf[i] = cc(double(i) / g.nu);
   for (size_t i = 0; i <= g.ny / 2; ++i) cf[g.nx / 2 + 1 + i] = cc(double(i) / g.nv);
   double *d = reinterpret_cast<double *>(b_cf.ensure(cf.size() * sizeof(double)));
-  CK(cudaMemcpy(d, cf.data(), cf.size() * sizeof(double), cudaMemcpyHostToDevice));
+  // stream-ordered: kernels of earlier (pipelined) calls may still read b_cf
+  CK(cudaMemcpyAsync(d, cf.data(), cf.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
   cheb_err = cc.max_rel_err;
   corr_key = key;
   corr_cc = cc;
@@ -762,11 +796,12 @@ const void *Context::upload_twiddles(const GridPlan &g, bool dbl) {
   if (!(tw_valid && key == tw_key)) {
     const std::vector<double> h = col_twiddle_table(M, g.nu, size_t(g.K));
     void *d = b_tw.ensure(h.size() / 2 * cs);
+    // stream-ordered (pageable sources are staged before the call returns)
     if (dbl) {
-      CK(cudaMemcpy(d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+      CK(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
     } else {
       std::vector<float> hf(h.begin(), h.end());
-      CK(cudaMemcpy(d, hf.data(), hf.size() * sizeof(float), cudaMemcpyHostToDevice));
+      CK(cudaMemcpyAsync(d, hf.data(), hf.size() * sizeof(float), cudaMemcpyHostToDevice, stream));
     }
     tw_key = key;
     tw_valid = true;
@@ -840,7 +875,7 @@ void Context::grid_core(const wsg_args &a, const Staged &s, double *img, bool ac
   int *counter = reinterpret_cast<int *>(reinterpret_cast<char *>(b_small.p) + 2048);
   int *d_nch = reinterpret_cast<int *>(reinterpret_cast<char *>(b_small.p) + 1024);
   int *d_err = reinterpret_cast<int *>(reinterpret_cast<char *>(b_small.p) + 3072);
-  CK(cudaMemsetAsync(d_err, 0, sizeof(int), stream));
+  if (!err_pending) CK(cudaMemsetAsync(d_err, 0, sizeof(int), stream));  // sticky while pipelined
   GridArgs ga{};
   ga.err = d_err;
   ga.rec = b_rec.p;
@@ -880,18 +915,24 @@ void Context::grid_core(const wsg_args &a, const Staged &s, double *img, bool ac
     cuda_check(cudaGetLastError(), "k_screen_add launch");
   g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     CK(cudaEventRecord(ev[5], stream));
-    CK(cudaEventSynchronize(ev[5]));
-    float t;
-    CK(cudaEventElapsedTime(&t, ev[2], ev[3]));
-    t_grid += t;
-    CK(cudaEventElapsedTime(&t, ev[3], ev[4]));
-    t_fft += t;
-    CK(cudaEventElapsedTime(&t, ev[4], ev[5]));
-    t_screen += t;
+    float t = 0;
+    if (!async_mode) CK(cudaEventSynchronize(ev[5]));
+    if (!async_mode) {
+      CK(cudaEventElapsedTime(&t, ev[2], ev[3]));
+      t_grid += t;
+      CK(cudaEventElapsedTime(&t, ev[3], ev[4]));
+      t_fft += t;
+      CK(cudaEventElapsedTime(&t, ev[4], ev[5]));
+      t_screen += t;
+    }
   }
-  check_device_error(d_err);
-  float t_prep;
-  CK(cudaEventElapsedTime(&t_prep, ev[0], ev[1]));
+  float t_prep = 0;
+  if (async_mode) {
+    err_pending = true;
+  } else {
+    check_device_error(d_err);
+    CK(cudaEventElapsedTime(&t_prep, ev[0], ev[1]));
+  }
   record_stats(gp, true, P);
   stats.ms_prep = t_prep;
   stats.ms_grid = t_grid;
@@ -942,7 +983,7 @@ void Context::degrid_core(const wsg_args &a, const Staged &s, const double *img,
   int *counter = reinterpret_cast<int *>(reinterpret_cast<char *>(b_small.p) + 2048);
   int *d_nch = reinterpret_cast<int *>(reinterpret_cast<char *>(b_small.p) + 1024);
   int *d_err = reinterpret_cast<int *>(reinterpret_cast<char *>(b_small.p) + 3072);
-  CK(cudaMemsetAsync(d_err, 0, sizeof(int), stream));
+  if (!err_pending) CK(cudaMemsetAsync(d_err, 0, sizeof(int), stream));  // sticky while pipelined
   GridArgs ga{};
   ga.err = d_err;
   ga.rec = b_rec.p;
@@ -991,14 +1032,16 @@ void Context::degrid_core(const wsg_args &a, const Staged &s, const double *img,
     ga.last_pass = pb0 + npl >= gp.nplanes;
     GridKernels<R>::dispatch(gp.kernel.W, false, num_sms, smem, stream, ga, g, kc);
     CK(cudaEventRecord(ev[5], stream));
-    CK(cudaEventSynchronize(ev[5]));
-    float t;
-    CK(cudaEventElapsedTime(&t, ev[2], ev[3]));
-    t_screen += t;
-    CK(cudaEventElapsedTime(&t, ev[3], ev[4]));
-    t_fft += t;
-    CK(cudaEventElapsedTime(&t, ev[4], ev[5]));
-    t_grid += t;
+    float t = 0;
+    if (!async_mode) CK(cudaEventSynchronize(ev[5]));
+    if (!async_mode) {
+      CK(cudaEventElapsedTime(&t, ev[2], ev[3]));
+      t_screen += t;
+      CK(cudaEventElapsedTime(&t, ev[3], ev[4]));
+      t_fft += t;
+      CK(cudaEventElapsedTime(&t, ev[4], ev[5]));
+      t_grid += t;
+    }
   }
   if (need_acc) {
     k_finalize<R><<<launch_blocks(gp.nvis, 256), 256, 0, stream>>>(int(gp.nvis), b_rec.p, ga.acc,
@@ -1006,9 +1049,13 @@ void Context::degrid_core(const wsg_args &a, const Staged &s, const double *img,
     cuda_check(cudaGetLastError(), "k_finalize launch");
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
   }
-  check_device_error(d_err);
-  float t_prep;
-  CK(cudaEventElapsedTime(&t_prep, ev[0], ev[1]));
+  float t_prep = 0;
+  if (async_mode) {
+    err_pending = true;
+  } else {
+    check_device_error(d_err);
+    CK(cudaEventElapsedTime(&t_prep, ev[0], ev[1]));
+  }
   record_stats(gp, false, P);
   stats.ms_prep = t_prep;
   stats.ms_grid = t_grid;
@@ -1063,23 +1110,67 @@ void Context::print_report(const GridPlan &g, bool gridding, size_t P) {
 
 // ------------------------------------------------------- public drivers
 
+// While alive, prepare() scans on the copy stream with the slot's f/c
+// buffer -- when every input the scan reads was copied into the slot.
+struct ScanPlacement {
+  Context &cx;
+  ScanPlacement(Context &c, Context::Slot &sl, bool staged) : cx(c) {
+    if (staged) {
+      cx.scan_st = cx.cpy;
+      cx.fovc_buf = &sl.fovc;
+    }
+  }
+  ~ScanPlacement() {
+    cx.scan_st = nullptr;
+    cx.fovc_buf = nullptr;
+  }
+};
+
+// Ends a raw operator call: the slot is free once the main stream (and the
+// device-to-host copy, when there is one) is done; synchronous mode waits.
+void Context::finish_call(const wsg_args &a, Slot &sl, cudaStream_t last) {
+  CK(cudaEventRecord(sl.free_ev, last));
+  stats.kernel_launches = g_kernel_launches.load();
+  stats.nrows = a.nrows;
+  stats.nchan = a.nchan;
+  if (async_mode) return;
+  CK(cudaEventRecord(ev[6], last));
+  CK(cudaStreamSynchronize(stream));
+  CK(cudaStreamSynchronize(d2h));
+  float t;
+  CK(cudaEventElapsedTime(&t, ev[0], ev[6]));
+  stats.ms_total = t;
+}
+
 void Context::ms2dirty(const wsg_args &a, const void *vis, void *dirty, int accumulate) {
   validate(a);
   require(vis && dirty, "vis and dirty are required");
   CK(cudaSetDevice(device));
   const size_t nvis = a.nrows * a.nchan;
   const size_t vbytes = nvis * (a.vis_type == WSG_C128 ? 16 : 8);
-  Staged s;
-  s.uvw = reinterpret_cast<const double *>(stage_in(a.uvw, a.nrows * 3 * sizeof(double), b_uvw));
-  s.vis = stage_in(vis, vbytes, b_vis);
-  s.wgt = stage_in(a.wgt, nvis * (a.wgt_type == WSG_F64 ? 8 : 4), b_wgt);
-  s.mask = reinterpret_cast<const uint8_t *>(stage_in(a.mask, nvis, b_mask));
   const size_t npix = a.npix_x * a.npix_y;
   const size_t dsz = a.dirty_type == WSG_F64 ? 8 : 4;
-  double *img = reinterpret_cast<double *>(b_img.ensure(npix * sizeof(double)));
   const bool ddev = is_device_pointer(dirty);
+  // host inputs are copied into this call's slot on the copy stream, which
+  // runs ahead of the main stream (device inputs are used in place, in the
+  // order of the main stream); the slot is reused once its previous call
+  // has finished with it
+  Slot &sl = slots[slot_k++ & 1];
+  CK(cudaEventSynchronize(sl.free_ev));
+  Staged s;
+  s.uvw = reinterpret_cast<const double *>(stage_in(a.uvw, a.nrows * 3 * sizeof(double), sl.uvw, cpy));
+  s.vis = stage_in(vis, vbytes, sl.vis, cpy);
+  s.wgt = stage_in(a.wgt, nvis * (a.wgt_type == WSG_F64 ? 8 : 4), sl.wgt, cpy);
+  s.mask = reinterpret_cast<const uint8_t *>(stage_in(a.mask, nvis, sl.mask, cpy));
+  const void *din = (accumulate && !ddev) ? stage_in(dirty, npix * dsz, sl.out, cpy) : dirty;
+  CK(cudaEventRecord(ev_in, cpy));
+  CK(cudaStreamWaitEvent(stream, ev_in, 0));
+  // (stage_in returns device inputs unchanged: a new pointer means copied)
+  ScanPlacement place(*this, sl, s.uvw != a.uvw && s.vis != vis &&
+                                     (a.wgt == nullptr || s.wgt != a.wgt) &&
+                                     (a.mask == nullptr || s.mask != a.mask));
+  double *img = reinterpret_cast<double *>(b_img.ensure(npix * sizeof(double)));
   if (accumulate) {
-    const void *din = ddev ? dirty : stage_in(dirty, npix * dsz, b_out);
     int nb = launch_blocks(npix, 256);
     if (a.dirty_type == WSG_F64)
       k_load_image<double><<<nb, 256, 0, stream>>>(npix, (const double *)din, img, 0);
@@ -1093,7 +1184,7 @@ void Context::ms2dirty(const wsg_args &a, const void *vis, void *dirty, int accu
   else
     grid_core<float>(a, s, img, accumulate != 0);
   // convert/copy out
-  void *dout = ddev ? dirty : b_out.ensure(npix * dsz);
+  void *dout = ddev ? dirty : sl.out.ensure(npix * dsz);
   int nb = launch_blocks(npix, 256);
   if (a.dirty_type == WSG_F64)
     k_store_image<double><<<nb, 256, 0, stream>>>(npix, img, (double *)dout);
@@ -1101,15 +1192,14 @@ void Context::ms2dirty(const wsg_args &a, const void *vis, void *dirty, int accu
     k_store_image<float><<<nb, 256, 0, stream>>>(npix, img, (float *)dout);
   cuda_check(cudaGetLastError(), "k_store_image launch");
   g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
-  if (!ddev) CK(cudaMemcpyAsync(dirty, dout, npix * dsz, cudaMemcpyDeviceToHost, stream));
-  CK(cudaEventRecord(ev[6], stream));
-  CK(cudaStreamSynchronize(stream));
-  float t;
-  CK(cudaEventElapsedTime(&t, ev[0], ev[6]));
-  stats.ms_total = t;
-  stats.kernel_launches = g_kernel_launches.load();
-  stats.nrows = a.nrows;
-  stats.nchan = a.nchan;
+  cudaStream_t last = stream;
+  if (!ddev) {
+    CK(cudaEventRecord(ev_done, stream));
+    CK(cudaStreamWaitEvent(d2h, ev_done, 0));
+    CK(cudaMemcpyAsync(dirty, dout, npix * dsz, cudaMemcpyDeviceToHost, d2h));
+    last = d2h;
+  }
+  finish_call(a, sl, last);
 }
 
 void Context::dirty2ms(const wsg_args &a, const void *dirty, void *vis) {
@@ -1118,13 +1208,19 @@ void Context::dirty2ms(const wsg_args &a, const void *dirty, void *vis) {
   CK(cudaSetDevice(device));
   const size_t nvis = a.nrows * a.nchan;
   const size_t vbytes = nvis * (a.vis_type == WSG_C128 ? 16 : 8);
-  Staged s;
-  s.uvw = reinterpret_cast<const double *>(stage_in(a.uvw, a.nrows * 3 * sizeof(double), b_uvw));
-  s.wgt = stage_in(a.wgt, nvis * (a.wgt_type == WSG_F64 ? 8 : 4), b_wgt);
-  s.mask = reinterpret_cast<const uint8_t *>(stage_in(a.mask, nvis, b_mask));
   const size_t npix = a.npix_x * a.npix_y;
   const size_t dsz = a.dirty_type == WSG_F64 ? 8 : 4;
-  const void *din = stage_in(dirty, npix * dsz, b_out);
+  Slot &sl = slots[slot_k++ & 1];
+  CK(cudaEventSynchronize(sl.free_ev));
+  Staged s;
+  s.uvw = reinterpret_cast<const double *>(stage_in(a.uvw, a.nrows * 3 * sizeof(double), sl.uvw, cpy));
+  s.wgt = stage_in(a.wgt, nvis * (a.wgt_type == WSG_F64 ? 8 : 4), sl.wgt, cpy);
+  s.mask = reinterpret_cast<const uint8_t *>(stage_in(a.mask, nvis, sl.mask, cpy));
+  const void *din = stage_in(dirty, npix * dsz, sl.out, cpy);
+  CK(cudaEventRecord(ev_in, cpy));
+  CK(cudaStreamWaitEvent(stream, ev_in, 0));
+  ScanPlacement place(*this, sl, s.uvw != a.uvw && (a.wgt == nullptr || s.wgt != a.wgt) &&
+                                     (a.mask == nullptr || s.mask != a.mask));
   double *img = reinterpret_cast<double *>(b_img.ensure(npix * sizeof(double)));
   int nb = launch_blocks(npix, 256);
   if (a.dirty_type == WSG_F64)
@@ -1133,7 +1229,23 @@ void Context::dirty2ms(const wsg_args &a, const void *dirty, void *vis) {
     k_load_image<float><<<nb, 256, 0, stream>>>(npix, (const float *)din, img, 0);
   cuda_check(cudaGetLastError(), "k_load_image launch");
   g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
-  degrid_from_image(a, s, img, vis, vbytes);
+  const bool vdev = is_device_pointer(vis);
+  void *vout = vdev ? vis : sl.vis.ensure(vbytes);
+  // inactive visibilities are zeroed; with no active ones at all the whole
+  // output is zero
+  CK(cudaMemsetAsync(vout, 0, vbytes, stream));
+  if (a.precision == WSG_PREC_FP64)
+    degrid_core<double>(a, s, img, vout);
+  else
+    degrid_core<float>(a, s, img, vout);
+  cudaStream_t last = stream;
+  if (!vdev) {
+    CK(cudaEventRecord(ev_done, stream));
+    CK(cudaStreamWaitEvent(d2h, ev_done, 0));
+    CK(cudaMemcpyAsync(vis, vout, vbytes, cudaMemcpyDeviceToHost, d2h));
+    last = d2h;
+  }
+  finish_call(a, sl, last);
 }
 
 void Context::degrid_from_image(const wsg_args &a, const Staged &s, const double *img, void *vis,
@@ -1339,6 +1451,8 @@ void Plan::build(const std::vector<wsg_job> &js) {
     nchunks_ += nch_j;
     // corrections and twiddles of this grid
     pj.cc = cx_.upload_corrections(gp);
+    cx_.upload_twiddles(gp, sizeof(R) == 8);
+    CK(cudaStreamSynchronize(st));  // the uploads are stream-ordered
     const size_t ncf = gp.nx / 2 + 1 + gp.ny / 2 + 1;
     pj.cf_off = cf_host.size();
     cf_host.resize(cf_host.size() + ncf);
@@ -1346,7 +1460,6 @@ void Plan::build(const std::vector<wsg_job> &js) {
                   cudaMemcpyDeviceToHost));
     const size_t M = size_t(1) << gp.logM;
     const size_t ntw = (M + size_t(gp.K) * (M / 16) + 32 * size_t(gp.K)) * cs;
-    cx_.upload_twiddles(gp, sizeof(R) == 8);
     pj.tw_off = tw_host.size();
     tw_host.resize(align256(tw_host.size() + ntw));
     CK(cudaMemcpy(tw_host.data() + pj.tw_off, cx_.b_tw.p, ntw, cudaMemcpyDeviceToHost));
@@ -1733,12 +1846,13 @@ StreamGridder::StreamGridder(Context &cx, const wsg_args &a, double wmin, double
   band_.ensure(g.band_rows * g.nplanes * g.nv * cs);
   img_.ensure(g.nx * g.ny * sizeof(double));
   cc_ = cx_.upload_corrections(g);
+  cx_.upload_twiddles(g, dbl_);
+  CK(cudaStreamSynchronize(cx_.stream));  // the uploads are stream-ordered
   const size_t ncf = g.nx / 2 + 1 + g.ny / 2 + 1;
   cf_.ensure(ncf * sizeof(double));
   CK(cudaMemcpy(cf_.p, cx_.b_cf.p, ncf * sizeof(double), cudaMemcpyDeviceToDevice));
   const size_t M = size_t(1) << g.logM;
   const size_t ntw = (M + size_t(g.K) * (M / 16) + 32 * size_t(g.K)) * cs;
-  cx_.upload_twiddles(g, dbl_);
   tw_.ensure(ntw);
   CK(cudaMemcpy(tw_.p, cx_.b_tw.p, ntw, cudaMemcpyDeviceToDevice));
   CF(cufftCreate(&fft_));

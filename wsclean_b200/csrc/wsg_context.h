@@ -74,13 +74,33 @@ class Context {
   size_t device_bytes();
   void validate(const wsg_args &a);
 
-  const void *stage_in(const void *p, size_t bytes, DevBuf &buf);
+  const void *stage_in(const void *p, size_t bytes, DevBuf &buf, cudaStream_t st = nullptr);
   template <typename R>
   void grid_core(const wsg_args &a, const Staged &s, double *img, bool accumulate);
   template <typename R>
   void degrid_core(const wsg_args &a, const Staged &s, const double *img, void *vis_out);
   void degrid_from_image(const wsg_args &a, const Staged &s, const double *img, void *vis,
                          size_t vbytes);
+
+  // Pipelined raw operators (wsg_ctx_set_async): wsg_ms2dirty / wsg_dirty2ms
+  // stage their inputs through two slots on a copy stream and write host
+  // outputs back on a third stream, so that consecutive calls overlap their
+  // transfers with each other's kernels; in asynchronous mode they return
+  // without waiting (wsg_ctx_synchronize waits and reports deferred errors).
+  struct Slot {
+    DevBuf uvw, vis, wgt, mask, out, fovc;
+    cudaEvent_t free_ev = nullptr;  // the slot's last use has finished
+  };
+  bool async_mode = false;
+  Slot slots[2];
+  size_t slot_k = 0;
+  cudaStream_t cpy = nullptr, d2h = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_in = nullptr, ev_done = nullptr, ev_scan = nullptr;
+  // where prepare() scans (nullptr: the main stream) and puts f/c
+  cudaStream_t scan_st = nullptr;
+  DevBuf *fovc_buf = nullptr;
+  bool err_pending = false;  // a device-side consistency check not yet read
+  void finish_call(const wsg_args &a, Slot &sl, cudaStream_t last);
 
   int device = 0;
   cudaStream_t stream = nullptr, own_stream = nullptr;

@@ -86,6 +86,21 @@ class Context:
     def release_buffers(self):
         L.check(L.lib().wsg_ctx_release_buffers(self._h))
 
+    def set_async(self, flag=True):
+        """Pipelined mode (``wsg_ctx_set_async``): ms2dirty / dirty2ms return
+        once enqueued and overlap their transfers with each other's kernels;
+        results are valid after ``synchronize()``.  Host inputs and outputs
+        must stay alive (and should be page-locked) until then."""
+        L.check(L.lib().wsg_ctx_set_async(self._h, int(bool(flag))))
+        self._async = bool(flag)
+        if not flag:
+            self._pending = []
+
+    def synchronize(self):
+        """Waits for the context's work; raises errors detected on the device."""
+        L.check(L.lib().wsg_ctx_synchronize(self._h))
+        self._pending = []
+
     def _bind_stream(self, *tensors):
         """Run the call on torch's current stream of the tensors' device when
         any operand is a CUDA tensor, so that it is ordered after the torch
@@ -159,6 +174,8 @@ class Context:
                        center_x, center_y, precision, _NP_C[vdt], _NP_F[ddt], keep)
         self._bind_stream(v, d, *keep)
         L.check(L.lib().wsg_ms2dirty(self._h, ctypes.byref(a), vp, dp, int(bool(accumulate))))
+        if getattr(self, "_async", False):
+            self._pending = (getattr(self, "_pending", []) + [(keep, d)])[-4:]
         return d
 
     def autotune(self, uvw, freq, vis, npix_x, npix_y, pixsize_x, pixsize_y, epsilon,
@@ -209,6 +226,8 @@ class Context:
                        center_x, center_y, precision, _NP_C[vdt], _NP_F[ddt], keep)
         self._bind_stream(d, v, *keep)
         L.check(L.lib().wsg_dirty2ms(self._h, ctypes.byref(a), dp, vp))
+        if getattr(self, "_async", False):
+            self._pending = (getattr(self, "_pending", []) + [(keep, v)])[-4:]
         return v
 
 
