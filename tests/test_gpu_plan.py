@@ -207,3 +207,31 @@ def test_plan_rejects_host_memory_and_bad_jobs():
     with pytest.raises(L.InvalidArgument):
         G.Plan(uvw, freq, px, px, 1e-5, jobs=[dict(npix_x=64, npix_y=64, chan_begin=4,
                                                    chan_end=9)], **KW)
+
+
+def test_plan_jobs_without_data():
+    """A job whose channels are all flagged images to zero and predicts
+    nothing; the shared kernel then comes from the largest job with data."""
+    from wsclean_b200 import gridder as G
+    rng, uvw, freq, vis, px = problem(7)
+    mask = np.ones(vis.shape, np.uint8)
+    mask[:, 3:] = 0   # channels 3..5 flagged
+    jobs = [dict(npix_x=128, npix_y=128, chan_begin=3, chan_end=6),   # largest, no data
+            dict(npix_x=64, npix_y=64, chan_begin=0, chan_end=3)]
+    with G.Plan(uvw, freq, px, px, 1e-5, jobs=jobs, mask=mask, dirty_dtype=np.float64,
+                **KW) as plan:
+        imgs = plan.ms2dirty(torch.as_tensor(vis.astype(np.complex64), device=DEV))
+        torch.cuda.synchronize()
+        assert float(imgs[0].abs().max()) == 0.0
+        ref = O.dft_ms2dirty(uvw, freq[:3], vis[:, :3], 64, 64, px, px, negate_v=True,
+                             divide_by_n=False)
+        assert O.rel_rms(imgs[1].cpu().numpy(), ref) < 1e-5
+        assert plan.stats(0)["nvis"] == 0
+        models = [torch.ones((128, 128), dtype=torch.float64, device=DEV),
+                  torch.zeros((64, 64), dtype=torch.float64, device=DEV)]
+        models[1][10, 20] = 1.0
+        v = plan.dirty2ms(models).cpu().numpy()
+        assert np.all(v[:, 3:] == 0)
+        want = O.dft_dirty2ms(uvw, freq[:3], models[1].cpu().numpy(), px, px, negate_v=True,
+                              divide_by_n=False)
+        assert O.rel_rms(v[:, :3], want) < 1e-5

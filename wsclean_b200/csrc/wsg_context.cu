@@ -1348,7 +1348,7 @@ void Plan::build(const std::vector<wsg_job> &js) {
   else
     std::memcpy(freq.data(), a_.freq, nchan * sizeof(double));
 
-  // the shared kernel: the one chosen for the largest job
+  // the shared kernel: the one chosen for the largest job with active data
   size_t big = 0;
   for (size_t j = 1; j < js.size(); ++j)
     if (js[j].npix_x * js[j].npix_y > js[big].npix_x * js[big].npix_y) big = j;
@@ -1414,8 +1414,7 @@ void Plan::build(const std::vector<wsg_job> &js) {
     gp.force_W = forceW;
     gp.force_sigma = forceS;
     const bool any = cx_.prepare<R>(aj, sj, false, nullptr, gp);
-    if (oi == 0) {
-      require(any, "the largest job has no active visibilities");
+    if (forceW == 0 && any) {  // the largest job with active visibilities
       forceW = gp.kernel.W;
       forceS = gp.kernel.sigma;
       DevKernel<R> kc = make_kernel<R>(gp.poly);
