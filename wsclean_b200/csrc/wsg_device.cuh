@@ -91,6 +91,30 @@ __device__ __forceinline__ double2 cexp_turns(double t) {
   return make_double2(c, s);
 }
 
+// Complex sum and difference: one packed two-lane instruction each in FP32
+// (fadd / fma .f32x2), two scalar ones in FP64.
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) {
+  return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a);
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) {
+  return make_double2(a.x + b.x, a.y + b.y);
+}
+__device__ __forceinline__ double2 csub(double2 a, double2 b) {
+  return make_double2(a.x - b.x, a.y - b.y);
+}
+
+// a * s + acc for a complex a and a real s: one packed two-lane FMA in FP32
+// (Blackwell's fma.rn.f32x2), two scalar FMAs in FP64.
+__device__ __forceinline__ float2 cfma_real(float2 a, float s, float2 acc) {
+  return __ffma2_rn(a, make_float2(s, s), acc);
+}
+__device__ __forceinline__ double2 cfma_real(double2 a, double s, double2 acc) {
+  acc.x = fma(a.x, s, acc.x);
+  acc.y = fma(a.y, s, acc.y);
+  return acc;
+}
+
 // FP64 coordinates of one visibility: (u, v', w) already scaled by f/c.
 struct VisPix {
   int iu0, iv0, iw;
@@ -585,11 +609,13 @@ k_spread(GridArgs a, DevGeom g, DevKernel<R> kc) {
 #pragma unroll
       for (int k = 0; k < PPL; ++k)
         ok[k] = (pp[k] < W) && (mp + pp[k] >= jb.pb0) && (mp + pp[k] < jb.pb1);
-      R accr[PPL][W], acci[PPL][W];
+      // (re, im) accumulators; in FP32 updated with Blackwell's packed
+      // two-lane FMA (one instruction per complex cell)
+      C acc[PPL][W];
 #pragma unroll
       for (int k = 0; k < PPL; ++k)
 #pragma unroll
-        for (int c = 0; c < W; ++c) accr[k][c] = acci[k][c] = R(0);
+        for (int c = 0; c < W; ++c) acc[k][c].x = acc[k][c].y = R(0);
       uint32_t cur = 0xffffffffu;
       int bb0 = 1 << 30, bb1 = -1, bb2 = 1 << 30, bb3 = -1;
       auto commit = [&]() {
@@ -601,9 +627,9 @@ k_spread(GridArgs a, DevGeom g, DevKernel<R> kc) {
           const int base = pp[k] * tl.PS + (lu + cu[k]) * tl.RS + lv;
 #pragma unroll
           for (int c = 0; c < W; ++c) {
-            atomicAdd(&tre[base + c], accr[k][c]);
-            atomicAdd(&tim[base + c], acci[k][c]);
-            accr[k][c] = acci[k][c] = R(0);
+            atomicAdd(&tre[base + c], acc[k][c].x);
+            atomicAdd(&tim[base + c], acc[k][c].y);
+            acc[k][c].x = acc[k][c].y = R(0);
           }
         }
       };
@@ -631,12 +657,11 @@ k_spread(GridArgs a, DevGeom g, DevKernel<R> kc) {
 #pragma unroll
           for (int k = 0; k < PPL; ++k) {
             const R f = kb[2 * W + (ok[k] ? pp[k] : 0)] * kb[ok[k] ? cu[k] : 0];
-            const R ar = vr * f, ai = vi * f;
+            C a;
+            a.x = vr * f;
+            a.y = vi * f;
 #pragma unroll
-            for (int c = 0; c < W; ++c) {
-              accr[k][c] = fma(ar, kvv[c], accr[k][c]);
-              acci[k][c] = fma(ai, kvv[c], acci[k][c]);
-            }
+            for (int c = 0; c < W; ++c) acc[k][c] = cfma_real(a, kvv[c], acc[k][c]);
           }
         }
         __syncwarp();
@@ -867,7 +892,7 @@ k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
     if (slice < NSL) {
       const int n = s1 - s0;
       const int j0 = s0 + (n * slice) / NSL, j1 = s0 + (n * (slice + 1)) / NSL;
-      R cr[PPL][W], ci[PPL][W];
+      C cl[PPL][W];  // the lane's cells (re, im) at the current origin
       uint32_t cur = 0xffffffffu;
       int bb0 = 0, bb1 = 0, bb2 = 0, bb3 = 0;
       for (int b0 = j0; b0 < j1; b0 += 32) {
@@ -886,8 +911,8 @@ k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
               const int base = (ok[k] ? pp[k] * tl.PS + (lu + cu[k]) * tl.RS : 0) + lv;
 #pragma unroll
               for (int c = 0; c < W; ++c) {
-                cr[k][c] = ok[k] ? tre[base + c] : R(0);
-                ci[k][c] = ok[k] ? tim[base + c] : R(0);
+                cl[k][c].x = ok[k] ? tre[base + c] : R(0);
+                cl[k][c].y = ok[k] ? tim[base + c] : R(0);
               }
             }
           }
@@ -895,21 +920,19 @@ k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
           R kvv[W];
 #pragma unroll
           for (int c = 0; c < W; ++c) kvv[c] = kb[W + c];
-          R sr = R(0), si = R(0);
+          C sacc;
+          sacc.x = sacc.y = R(0);
 #pragma unroll
           for (int k = 0; k < PPL; ++k) {
-            R tr = R(0), ti = R(0);
+            C t;
+            t.x = t.y = R(0);
 #pragma unroll
-            for (int c = 0; c < W; ++c) {
-              tr = fma(cr[k][c], kvv[c], tr);
-              ti = fma(ci[k][c], kvv[c], ti);
-            }
+            for (int c = 0; c < W; ++c) t = cfma_real(cl[k][c], kvv[c], t);
             const R f = ok[k] ? kb[2 * W + pp[k]] * kb[cu[k]] : R(0);
-            sr = fma(tr, f, sr);
-            si = fma(ti, f, si);
+            sacc = cfma_real(t, f, sacc);
           }
-          sr = warp_sum(sr);
-          si = warp_sum(si);
+          R sr = warp_sum(sacc.x);
+          R si = warp_sum(sacc.y);
           if (lane == 0) {
             const int s = b0 + jj;
             if (direct) {
@@ -1016,10 +1039,8 @@ __device__ __forceinline__ void dft_reg(C *v, int sign) {
         b = cmul(b, w);
       }
       const int d = (j / NS) * 2 * NS + k;
-      y[d].x = a.x + b.x;
-      y[d].y = a.y + b.y;
-      y[d + NS].x = a.x - b.x;
-      y[d + NS].y = a.y - b.y;
+      y[d] = cadd(a, b);
+      y[d + NS] = csub(a, b);
     }
 #pragma unroll
     for (int j = 0; j < N; ++j) v[j] = y[j];
