@@ -74,7 +74,7 @@ int wsg_ctx_set_stream(wsg_ctx *ctx, void *stream);
 /* Releases the cached device buffers and cuFFT plans (they regrow on demand). */
 int wsg_ctx_release_buffers(wsg_ctx *ctx);
 /* Pipelined mode for wsg_ms2dirty / wsg_dirty2ms (0: off, the default).
- * Every call stages its inputs through one of two buffer slots on a copy
+ * Every call stages its inputs through one of three buffer slots on a copy
  * stream and writes host outputs back on a third stream, so consecutive
  * calls overlap their transfers with each other's kernels; with async != 0
  * the calls return once their work is enqueued (after the short planning

@@ -128,8 +128,9 @@ Context::Context(int dev) {
   for (auto &e : ev) CK(cudaEventCreate(&e));
   CK(cudaStreamCreateWithFlags(&cpy, cudaStreamNonBlocking));
   CK(cudaStreamCreateWithFlags(&d2h, cudaStreamNonBlocking));
-  for (cudaEvent_t *e : {&ev_start, &ev_in, &ev_done, &ev_scan, &slots[0].free_ev, &slots[1].free_ev})
+  for (cudaEvent_t *e : {&ev_start, &ev_in, &ev_done, &ev_scan})
     CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+  for (auto &sl : slots) CK(cudaEventCreateWithFlags(&sl.free_ev, cudaEventDisableTiming));
   std::memset(&stats, 0, sizeof(stats));
   verbosity = env_int("WSG_VERBOSITY", 0);
 }
@@ -161,8 +162,10 @@ Context::~Context() {
       cudaStreamSynchronize(st);
       cudaStreamDestroy(st);
     }
-  for (cudaEvent_t e : {ev_start, ev_in, ev_done, ev_scan, slots[0].free_ev, slots[1].free_ev})
+  for (cudaEvent_t e : {ev_start, ev_in, ev_done, ev_scan})
     if (e) cudaEventDestroy(e);
+  for (auto &sl : slots)
+    if (sl.free_ev) cudaEventDestroy(sl.free_ev);
   for (auto &sl : slots)
     for (DevBuf *b : {&sl.uvw, &sl.vis, &sl.wgt, &sl.mask, &sl.out, &sl.fovc}) b->release();
   if (own_stream) cudaStreamDestroy(own_stream);
@@ -1155,7 +1158,7 @@ void Context::ms2dirty(const wsg_args &a, const void *vis, void *dirty, int accu
   // runs ahead of the main stream (device inputs are used in place, in the
   // order of the main stream); the slot is reused once its previous call
   // has finished with it
-  Slot &sl = slots[slot_k++ & 1];
+  Slot &sl = slots[slot_k++ % kSlots];
   CK(cudaEventSynchronize(sl.free_ev));
   Staged s;
   s.uvw = reinterpret_cast<const double *>(stage_in(a.uvw, a.nrows * 3 * sizeof(double), sl.uvw, cpy));
@@ -1210,7 +1213,7 @@ void Context::dirty2ms(const wsg_args &a, const void *dirty, void *vis) {
   const size_t vbytes = nvis * (a.vis_type == WSG_C128 ? 16 : 8);
   const size_t npix = a.npix_x * a.npix_y;
   const size_t dsz = a.dirty_type == WSG_F64 ? 8 : 4;
-  Slot &sl = slots[slot_k++ & 1];
+  Slot &sl = slots[slot_k++ % kSlots];
   CK(cudaEventSynchronize(sl.free_ev));
   Staged s;
   s.uvw = reinterpret_cast<const double *>(stage_in(a.uvw, a.nrows * 3 * sizeof(double), sl.uvw, cpy));

@@ -83,7 +83,7 @@ class Context {
                          size_t vbytes);
 
   // Pipelined raw operators (wsg_ctx_set_async): wsg_ms2dirty / wsg_dirty2ms
-  // stage their inputs through two slots on a copy stream and write host
+  // stage their inputs through three slots on a copy stream and write host
   // outputs back on a third stream, so that consecutive calls overlap their
   // transfers with each other's kernels; in asynchronous mode they return
   // without waiting (wsg_ctx_synchronize waits and reports deferred errors).
@@ -92,7 +92,8 @@ class Context {
     cudaEvent_t free_ev = nullptr;  // the slot's last use has finished
   };
   bool async_mode = false;
-  Slot slots[2];
+  static constexpr int kSlots = 3;
+  Slot slots[kSlots];
   size_t slot_k = 0;
   cudaStream_t cpy = nullptr, d2h = nullptr;
   cudaEvent_t ev_start = nullptr, ev_in = nullptr, ev_done = nullptr, ev_scan = nullptr;
