@@ -235,3 +235,22 @@ def test_plan_jobs_without_data():
         want = O.dft_dirty2ms(uvw, freq[:3], models[1].cpu().numpy(), px, px, negate_v=True,
                               divide_by_n=False)
         assert O.rel_rms(v[:, :3], want) < 1e-5
+
+
+def test_context_outlives_its_plans():
+    """The C ABI refuses to destroy a context that still has plans."""
+    import ctypes
+    from wsclean_b200 import gridder as G
+    from wsclean_b200 import _lib as L
+    rng, uvw, freq, vis, px = problem(8)
+    ctx = G.Context(0)
+    plan = G.Plan(uvw, freq, px, px, 1e-5, 64, 64, context=ctx, **KW)
+    assert L.lib().wsg_ctx_destroy(ctx._h) == L.WSG_ERR_STATE
+    plan.close()
+    assert L.lib().wsg_ctx_destroy(ctx._h) == L.WSG_OK
+    ctx._h = None
+    # a gridder's context cannot be switched to pipelined mode
+    g = G.WGriddingGridder(64, 64, 64, 64, px, px, 0.0, 0.0)
+    view = L.lib().wsg_gridder_ctx(g._h)
+    assert L.lib().wsg_ctx_set_async(ctypes.c_void_p(view), 1) == L.WSG_ERR_INVALID
+    g.close()

@@ -309,6 +309,17 @@ TileLayout make_layout(int T, int W) {
   return tl;
 }
 
+// Before the transposed u transform fills the band grid: it writes every
+// band row of the ny image columns (v indices [nv - ny/2, nv) and
+// [0, ny/2)), so only the nv - ny columns between them need clearing.
+void clear_outside_columns(void *band, size_t rows, size_t nv, size_t ny, size_t cs,
+                           cudaStream_t st) {
+  if (nv <= ny) return;
+  cuda_check(cudaMemset2DAsync(static_cast<char *>(band) + (ny / 2) * cs, nv * cs, 0,
+                               (nv - ny) * cs, rows, st),
+             "cudaMemset2DAsync");
+}
+
 int launch_blocks(size_t n, int threads) {
   size_t b = (n + threads - 1) / threads;
   return int(std::min<size_t>(std::max<size_t>(b, 1), 65535 * 8));
@@ -1020,7 +1031,7 @@ void Context::degrid_core(const wsg_args &a, const Staged &s, const double *img,
     CK(cudaEventRecord(ev[3], stream));
     // pruned transform along u (transposed): image rows -> band rows of the
     // image columns; the other columns of the band grid stay zero
-    CK(cudaMemsetAsync(band, 0, gp.band_rows * P * nv * cs, stream));
+    clear_outside_columns(band, gp.band_rows * P, nv, gp.ny, cs, stream);
     ColKernels<R>::run(gp.logM, false, ca, int(npl), stream);
     // transform along v
     {
@@ -1621,7 +1632,7 @@ void Plan::enqueue_degrid(const void *const *dirty, void *vis) {
     k_screen_put<R><<<sg, 256, 0, st>>>(sa, img, H_.p);
     cuda_check(cudaGetLastError(), "k_screen_put launch");
     char *band = static_cast<char *>(band_.p) + pj.band_off;
-    CK(cudaMemsetAsync(band, 0, pj.band_bytes, st));
+    clear_outside_columns(band, gp.band_rows * gp.nplanes, gp.nv, gp.ny, cs, st);
     ColArgs ca = make_col(gp, gp.nplanes, static_cast<char *>(tw_.p) + pj.tw_off, band, H_.p);
     ColKernels<R>::run(gp.logM, false, ca, int(gp.nplanes), st);
     CF(cufftSetStream(pj.fft, st));
