@@ -1239,6 +1239,24 @@ __device__ __forceinline__ C col_twist(const ColArgs &a, const C *twB, const C *
   return cmul(__ldg(&twQ[(k2 * 16 + q) * 2 + neg]), base);
 }
 
+// Copies N table entries to shared memory with all of a thread's loads in
+// flight together (a strided copy loop would wait for each load in turn).
+template <typename C, int N, int THREADS>
+__device__ __forceinline__ void fill_table(C *dst, const C *src) {
+  constexpr int NF = (N + THREADS - 1) / THREADS;
+  C tmp[NF];
+#pragma unroll
+  for (int n = 0; n < NF; ++n) {
+    const int i = threadIdx.x + n * THREADS;
+    if (i < N) tmp[n] = __ldg(&src[i]);
+  }
+#pragma unroll
+  for (int n = 0; n < NF; ++n) {
+    const int i = threadIdx.x + n * THREADS;
+    if (i < N) dst[i] = tmp[n];
+  }
+}
+
 // Shared memory of a column CTA: two padded buffers per column, then the
 // M stage twiddles.
 template <typename R, int M>
@@ -1269,7 +1287,7 @@ k_ucol_bwd(ColArgs a) {
   const C *twB = reinterpret_cast<const C *>(a.twB);
   const C *twQ = reinterpret_cast<const C *>(a.twQ);
   C *H = reinterpret_cast<C *>(a.H);
-  for (int i = threadIdx.x; i < M; i += blockDim.x) tws[i] = reinterpret_cast<const C *>(a.twM)[i];
+  fill_table<C, M, ColCfg<R, M>::THREADS>(tws, reinterpret_cast<const C *>(a.twM));
   // coalesced load (slot-major, adjacent image columns innermost) into the
   // A buffers, all sixteen loads of a thread in flight together
   constexpr int ITEMS = NB * M / ColCfg<R, M>::THREADS;  // 16
@@ -1349,7 +1367,7 @@ k_ucol_fwd(ColArgs a) {
   const C *twB = reinterpret_cast<const C *>(a.twB);
   const C *twQ = reinterpret_cast<const C *>(a.twQ);
   const C *rowp = reinterpret_cast<const C *>(a.H) + (size_t(lp) * a.ny + (jv ? j : 0)) * a.nx;
-  for (int i = threadIdx.x; i < M; i += blockDim.x) tws[i] = reinterpret_cast<const C *>(a.twM)[i];
+  fill_table<C, M, ColCfg<R, M>::THREADS>(tws, reinterpret_cast<const C *>(a.twM));
   const int half_nu = a.nu / 2, half_nx = a.nx / 2;
   C acc[16];
 #pragma unroll
@@ -1598,12 +1616,20 @@ __global__ void __launch_bounds__(256) k_screen_add(ScreenArgs s, const void *Hv
         const double w0 = s.wmin + s.pb0 * s.dw;
         double2 sc = cexp_turns(-w0 * q);
         const double2 st = cexp_turns(-s.dw * q);
-        for (int p = 0; p < s.npl; ++p) {
-          const C h = hp[p * pstride];
-          acc += double(h.x) * sc.x - double(h.y) * sc.y;
-          const double nr = sc.x * st.x - sc.y * st.y;
-          sc.y = sc.x * st.y + sc.y * st.x;
-          sc.x = nr;
+        for (int p0 = 0; p0 < s.npl; p0 += 8) {
+          C hb[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u)
+            if (p0 + u < s.npl) hb[u] = hp[(p0 + u) * pstride];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            if (p0 + u < s.npl) {
+              acc += double(hb[u].x) * sc.x - double(hb[u].y) * sc.y;
+              const double nr = sc.x * st.x - sc.y * st.y;
+              sc.y = sc.x * st.y + sc.y * st.x;
+              sc.x = nr;
+            }
+          }
         }
       } else {
         for (int p = 0; p < s.npl; ++p) acc += double(hp[p * pstride].x);
