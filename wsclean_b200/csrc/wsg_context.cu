@@ -827,24 +827,25 @@ const void *Context::upload_twiddles(const GridPlan &g, bool dbl) {
 // in what is free (plus what this context already holds).  cudaMemGetInfo is
 // a slow driver query (milliseconds, and tens of them when other processes
 // query the GPU), so a repeated plan whose buffers are still held reuses the
-// previous answer.
+// previous answer -- kept per direction, for alternating ms2dirty / dirty2ms.
 size_t Context::choose_planes(const GridPlan &g, bool gridding) {
   const size_t per = plan_bytes(g, 1, gridding);
   const size_t held = b_band.n + b_H.n;
   const auto key = std::make_tuple(per, g.nplanes, int(gridding));
-  if (planes_valid && key == planes_key && held >= planes_last * per) return planes_last;
-  size_t total = 0, freeb = 0;
-  CK(cudaMemGetInfo(&freeb, &total));
-  double budget = 0.55 * double(total);
-  size_t avail = size_t(std::min<double>(budget, double(freeb + held) - 2e9));
-  size_t P = std::max<size_t>(1, std::min<size_t>(g.nplanes, per ? avail / per : g.nplanes));
-  int lim = env_int("WSG_MAX_PLANES", 0);
+  PlanesMemo &pm = planes_memo[gridding ? 1 : 0];
+  if (!(pm.valid && key == pm.key && held >= pm.P * per)) {
+    size_t total = 0, freeb = 0;
+    CK(cudaMemGetInfo(&freeb, &total));
+    double budget = 0.55 * double(total);
+    size_t avail = size_t(std::min<double>(budget, double(freeb + held) - 2e9));
+    pm.P = std::max<size_t>(1, std::min<size_t>(g.nplanes, per ? avail / per : g.nplanes));
+    pm.key = key;
+    pm.valid = true;
+  }
+  size_t P = pm.P;
+  const int lim = env_int("WSG_MAX_PLANES", 0);  // a test and debugging limit
   if (lim > 0) P = std::min<size_t>(P, size_t(lim));
-  P = std::min(P, g.nplanes);
-  planes_key = key;
-  planes_last = P;
-  planes_valid = true;
-  return P;
+  return std::min(P, g.nplanes);
 }
 
 template <typename R>

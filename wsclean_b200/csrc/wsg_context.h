@@ -145,9 +145,12 @@ class Context {
   std::tuple<size_t, size_t, int> tw_key;
   bool tw_valid = false;
   // last plane-batch choice (choose_planes)
-  std::tuple<size_t, size_t, int> planes_key;
-  size_t planes_last = 0;
-  bool planes_valid = false;
+  struct PlanesMemo {
+    std::tuple<size_t, size_t, int> key;
+    size_t P = 0;
+    bool valid = false;
+  };
+  PlanesMemo planes_memo[2];  // degridding, gridding
   // correction-table cache
   std::tuple<int, double, double, size_t, size_t, size_t, size_t, double> corr_key;
   ChebCorr corr_cc;
