@@ -5,6 +5,7 @@
 #include <cufft.h>
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -638,7 +639,22 @@ bool Context::prepare(const wsg_args &a, const Staged &s, bool gridding, void *v
         tile = tc.tile;
       }
     }
-    choose_grid(gp, a.sigma_min, a.sigma_max, tile);
+    // the same data statistics and arguments give the same plan: repeated
+    // calls reuse the previous one of their direction
+    const std::array<double, 22> key{
+        double(gp.nx), double(gp.ny), gp.px, gp.py, gp.eps, double(gp.do_w), double(gp.fp32),
+        double(gp.negate_v), double(gp.divide_by_n), gp.lshift, gp.mshift, double(gp.nvis),
+        gp.wmin_d, gp.wmax_d, gp.umax, gp.vmax, double(gp.force_W), gp.force_sigma,
+        a.sigma_min, a.sigma_max, double(tile), double(gp.gridding)};
+    GridMemo &gm = grid_memo[gridding ? 1 : 0];
+    if (gm.valid && gm.key == key) {
+      gp = gm.plan;
+    } else {
+      choose_grid(gp, a.sigma_min, a.sigma_max, tile);
+      gm.key = key;
+      gm.plan = gp;
+      gm.valid = true;
+    }
   }
   DevGeom g = make_geom(gp);
   mark("choose_grid");

@@ -5,6 +5,7 @@
 #include <cufft.h>
 
 #include <chrono>
+#include <array>
 #include <map>
 #include <utility>
 #include <tuple>
@@ -151,6 +152,13 @@ class Context {
     bool valid = false;
   };
   PlanesMemo planes_memo[2];  // degridding, gridding
+  // last grid plan per direction, keyed by the arguments and data statistics
+  struct GridMemo {
+    std::array<double, 22> key{};
+    GridPlan plan;
+    bool valid = false;
+  };
+  GridMemo grid_memo[2];
   // correction-table cache
   std::tuple<int, double, double, size_t, size_t, size_t, size_t, double> corr_key;
   ChebCorr corr_cc;
