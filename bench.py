@@ -74,29 +74,48 @@ def parse_args():
 
 def launch_summary(path, steps):
     """Per-kernel totals of the last `steps` steps (two gridder calls each,
-    each starting with k_scan) of an ncu --csv launch list."""
+    each starting with k_scan) of an ncu --csv launch list: launches, device
+    time and share, and -- when the list holds dram__bytes_read/write.sum --
+    the DRAM bytes read and written, with the total per step."""
     import collections
     import csv
     rows = list(csv.reader(open(path)))
     hi = next(i for i, r in enumerate(rows) if "Kernel Name" in r)
     h = rows[hi]
-    ki, vi, ui = h.index("Kernel Name"), h.index("Metric Value"), h.index("Metric Unit")
-    scale = {"nsecond": 1e-6, "usecond": 1e-3, "msecond": 1.0, "second": 1e3}
-    launches = [(r[ki], float(r[vi].replace(",", "")) * scale.get(r[ui], 1e-6))
-                for r in rows[hi + 1:] if len(r) > vi and r[vi]]
+    ii, ki = h.index("ID"), h.index("Kernel Name")
+    mi, vi, ui = h.index("Metric Name"), h.index("Metric Value"), h.index("Metric Unit")
+    scale = {"nsecond": 1e-6, "ns": 1e-6, "usecond": 1e-3, "us": 1e-3, "msecond": 1.0, "ms": 1.0,
+             "second": 1e3, "s": 1e3,
+             "byte": 1.0, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9, "Tbyte": 1e12}
+    launches = collections.OrderedDict()  # launch id -> (kernel, {metric: value})
+    for r in rows[hi + 1:]:
+        if len(r) <= vi or not r[vi]:
+            continue
+        ent = launches.setdefault(r[ii], (r[ki], {}))
+        ent[1][r[mi]] = float(r[vi].replace(",", "")) * scale.get(r[ui], 1.0)
+    launches = list(launches.values())
     starts = [i for i, (k, _) in enumerate(launches) if "k_scan" in k]
     seg = launches[starts[-2 * steps]:] if len(starts) >= 2 * steps else launches
     tot = collections.OrderedDict()
-    for k, ms in seg:
+    for k, m in seg:
         name = k.split("(")[0].replace("void ", "")
-        c = tot.setdefault(name, [0, 0.0])
+        c = tot.setdefault(name, [0, 0.0, 0.0, 0.0])
         c[0] += 1
-        c[1] += ms
-    T = sum(v for _, v in tot.values())
-    print(f"{'kernel':72s} {'launches':>8s} {'ms':>8s} {'share':>6s}")
-    for k, (n, ms) in sorted(tot.items(), key=lambda x: -x[1][1]):
-        print(f"{k[:72]:72s} {n:8d} {ms:8.3f} {100 * ms / T:5.1f}%")
-    print(f"total {T:.3f} ms over {sum(n for n, _ in tot.values())} launches in {steps} step(s)")
+        c[1] += m.get("gpu__time_duration.sum", 0.0)
+        c[2] += m.get("dram__bytes_read.sum", 0.0)
+        c[3] += m.get("dram__bytes_write.sum", 0.0)
+    T = sum(v[1] for v in tot.values()) or 1.0
+    dram = any(v[2] or v[3] for v in tot.values())
+    print(f"{'kernel':72s} {'launches':>8s} {'ms':>8s} {'share':>6s}"
+          + (f" {'read GB':>8s} {'write GB':>8s}" if dram else ""))
+    for k, (n, ms, rd, wr) in sorted(tot.items(), key=lambda x: -x[1][1]):
+        print(f"{k[:72]:72s} {n:8d} {ms:8.3f} {100 * ms / T:5.1f}%"
+              + (f" {rd / 1e9:8.3f} {wr / 1e9:8.3f}" if dram else ""))
+    print(f"total {T:.3f} ms over {sum(v[0] for v in tot.values())} launches in {steps} step(s)")
+    if dram:
+        b = sum(v[2] + v[3] for v in tot.values())
+        print(f"total DRAM {b / 1e9:.3f} GB")
+        print(f"traffic_bytes_per_step: {int(b / steps)}")
 
 
 def profiled_traffic():
@@ -225,14 +244,14 @@ def run_reference(args, world, rank):
         O.ref_dirty2ms(uvw, freq, model, px, px, EPS_MIXED, **kw)
         return time.perf_counter() - t0
 
-    for _ in range(min(args.warmup, 1)):
+    for _ in range(args.warmup):
         step()
     ts = [step() for _ in range(args.steps)]
     tot = sum(ts)
     value = nvis * len(ts) / tot / 1e6
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": len(ts), "warmup": min(args.warmup, 1), "ms_per_step": 1e3 * tot / len(ts),
+        "steps": len(ts), "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(ts),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded Earth-rotation observation, 200 point sources)",
         "config": {"workload": "config-2 adjoint pair: 8.1M vis, 4096^2 @ 5\", eps 1e-5",
