@@ -394,13 +394,15 @@ def run_ours(args, world, rank, local, pg):
                      dirty=torch.zeros((nx, nx), dtype=torch.float64, device=dev),
                      out=torch.zeros((nrows, nchan), dtype=torch.complex128, device=dev)),
     }
+    # the plain FP64 form at the mixed form's accuracy (same buffers)
+    forms["fp64_eps_mixed"] = dict(forms["fp64"], eps=EPS_MIXED, prec="fp64")
     stream = torch.cuda.current_stream(dev)
 
     def call_pair(form, f):
-        ctx.ms2dirty(d_uvw, d_freq, f["vis"], nx, nx, px, px, f["eps"], precision=form,
+        ctx.ms2dirty(d_uvw, d_freq, f["vis"], nx, nx, px, px, f["eps"], precision=f.get("prec", form),
                      dirty=f["dirty"], **kw)
         st1 = ctx.stats()
-        ctx.dirty2ms(d_uvw, d_freq, f["model"], px, px, f["eps"], precision=form, vis=f["out"], **kw)
+        ctx.dirty2ms(d_uvw, d_freq, f["model"], px, px, f["eps"], precision=f.get("prec", form), vis=f["out"], **kw)
         st2 = ctx.stats()
         return st1, st2
 
@@ -429,11 +431,11 @@ def run_ours(args, world, rank, local, pg):
             # returning, so events on the current stream bracket each call
             ev[0].record(stream)
             st1 = None
-            ctx.ms2dirty(d_uvw, d_freq, f["vis"], nx, nx, px, px, f["eps"], precision=form,
+            ctx.ms2dirty(d_uvw, d_freq, f["vis"], nx, nx, px, px, f["eps"], precision=f.get("prec", form),
                          dirty=f["dirty"], **kw)
             ev[1].record(stream)
             st1 = ctx.stats()
-            ctx.dirty2ms(d_uvw, d_freq, f["model"], px, px, f["eps"], precision=form,
+            ctx.dirty2ms(d_uvw, d_freq, f["model"], px, px, f["eps"], precision=f.get("prec", form),
                          vis=f["out"], **kw)
             ev[2].record(stream)
             st2 = ctx.stats()
@@ -485,6 +487,12 @@ def run_ours(args, world, rank, local, pg):
                 "dirty2ms_mvis_s": world * nvis * k64 / (t64_dm / 1e3) / 1e6,
                 "ms_per_step": (t64_ms + t64_dm) / k64,
                 "grid": {"nu": s64["nu"], "nplanes": s64["nplanes"], "W": s64["supp"]}}
+        # the same FP64 form at the mixed form's accuracy (epsilon 1e-5)
+        t5_ms, t5_dm, _, _, s5, _, _ = timed("fp64_eps_mixed", k64, 1)
+        fp64["at_eps_mixed"] = {
+            "eps": EPS_MIXED, "value": world * nvis * k64 / ((t5_ms + t5_dm) / 1e3) / 1e6,
+            "ms_per_step": (t5_ms + t5_dm) / k64,
+            "grid": {"nu": s5["nu"], "nplanes": s5["nplanes"], "W": s5["supp"]}}
 
     # ---- accuracy (outside the timed region): FP64 direct sums
     rng = np.random.default_rng(99)
@@ -508,9 +516,9 @@ def run_ours(args, world, rank, local, pg):
         x = torch.randn((nx, nx), generator=g, dtype=torch.float64).to(dev)
         y = (torch.randn((nrows, nchan), generator=g, dtype=torch.float64)
              + 1j * torch.randn((nrows, nchan), generator=g, dtype=torch.float64)).to(dev)
-        Ax = ctx.dirty2ms(d_uvw, d_freq, x, px, px, f["eps"], precision=form,
+        Ax = ctx.dirty2ms(d_uvw, d_freq, x, px, px, f["eps"], precision=f.get("prec", form),
                           vis_dtype=np.complex128, **kw)
-        Aty = ctx.ms2dirty(d_uvw, d_freq, y, nx, nx, px, px, f["eps"], precision=form,
+        Aty = ctx.ms2dirty(d_uvw, d_freq, y, nx, nx, px, px, f["eps"], precision=f.get("prec", form),
                            dirty_dtype=np.float64, **kw)
         a = torch.vdot(y.ravel(), Ax.ravel()).real.item()
         b = torch.vdot(Aty.ravel().to(torch.complex128), x.ravel().to(torch.complex128)).real.item()
@@ -612,6 +620,7 @@ def run_ours(args, world, rank, local, pg):
             "dirty2ms_mvis_s": world * nvis * args.steps / (t_dm / 1e3) / 1e6,
             "fp64": fp64,
             "mixed_over_fp64": (value / fp64["value"]) if fp64 else None,
+            "mixed_over_fp64_same_eps": (value / fp64["at_eps_mixed"]["value"]) if fp64 else None,
             "accuracy": acc,
             "phases_ms": phases,
             "step_ms": step_ms,

@@ -626,7 +626,7 @@ bool Context::prepare(const wsg_args &a, const Staged &s, bool gridding, void *v
     gp.wmax_d = bits2d(hs.wmax_bits);
     gp.umax = bits2d(hs.umax_bits);
     gp.vmax = bits2d(hs.vmax_bits);
-    int tile = env_int("WSG_TILE", sizeof(R) == 4 ? 16 : 8);
+    int tile = env_int("WSG_TILE", 16);
     if (tune_W) {  // a candidate being timed by the autotuner
       gp.force_W = tune_W;
       gp.force_sigma = tune_sigma;
@@ -1364,7 +1364,7 @@ void Plan::build(const std::vector<wsg_job> &js) {
   const size_t cs = 2 * sizeof(R);
   const size_t nchan = a_.nchan, nrows = a_.nrows;
   cudaStream_t st = cx_.stream;
-  const int tile = env_int("WSG_TILE", sizeof(R) == 4 ? 16 : 8);
+  const int tile = env_int("WSG_TILE", 16);
 
   // coordinates on the device (kept only while building)
   Staged s;
@@ -1870,7 +1870,7 @@ StreamGridder::StreamGridder(Context &cx, const wsg_args &a, double wmin, double
   g.wmax_d = wmax;
   g.umax = umax;
   g.vmax = vmax;
-  choose_grid(g, a.sigma_min, a.sigma_max, env_int("WSG_TILE", dbl_ ? 8 : 16));
+  choose_grid(g, a.sigma_min, a.sigma_max, env_int("WSG_TILE", 16));
   g.fixed = true;
   const size_t cs = dbl_ ? 16 : 8;
   band_.ensure(g.band_rows * g.nplanes * g.nv * cs);
@@ -2396,9 +2396,9 @@ void Context::autotune(const wsg_args &a, const void *vis, int candidates, wsg_s
     gp.umax = um * fm;
     gp.vmax = vm * fm;
   }
-  const int tile0 = env_int("WSG_TILE", gp.fp32 ? 16 : 8);
+  const int tile0 = env_int("WSG_TILE", 16);
   auto cands = rank_kernels(gp, a.sigma_min, a.sigma_max, tile0, size_t(candidates));
-  std::vector<int> tiles = gp.fp32 ? std::vector<int>{8, 12, 16} : std::vector<int>{8};
+  std::vector<int> tiles{8, 12, 16};
   TuneChoice win;
   win.ms = 1e300;
   auto time_pair = [&]() {
