@@ -80,6 +80,12 @@ static int env_int(const char *name, int dflt) {
   return (s && *s) ? std::atoi(s) : dflt;
 }
 
+// Bin tile edge asked of the planner (which shrinks it until the W-plane
+// tile fits shared memory): measured on the 8.1M-visibility 4096^2 pair,
+// 20 is the fastest in mixed precision (3 -> 2 CTAs per SM, but half the
+// tile flushes of 16) and 24 in FP64; WSG_TILE overrides it.
+static int default_tile(bool fp32) { return env_int("WSG_TILE", fp32 ? 20 : 24); }
+
 // ------------------------------------------------------------ autotuner
 //
 // Process-wide table of timed choices: (image size, precision, accuracy,
@@ -626,7 +632,7 @@ bool Context::prepare(const wsg_args &a, const Staged &s, bool gridding, void *v
     gp.wmax_d = bits2d(hs.wmax_bits);
     gp.umax = bits2d(hs.umax_bits);
     gp.vmax = bits2d(hs.vmax_bits);
-    int tile = env_int("WSG_TILE", 16);
+    int tile = default_tile(sizeof(R) == 4);
     if (tune_W) {  // a candidate being timed by the autotuner
       gp.force_W = tune_W;
       gp.force_sigma = tune_sigma;
@@ -1364,7 +1370,7 @@ void Plan::build(const std::vector<wsg_job> &js) {
   const size_t cs = 2 * sizeof(R);
   const size_t nchan = a_.nchan, nrows = a_.nrows;
   cudaStream_t st = cx_.stream;
-  const int tile = env_int("WSG_TILE", 16);
+  const int tile = default_tile(sizeof(R) == 4);
 
   // coordinates on the device (kept only while building)
   Staged s;
@@ -1870,7 +1876,7 @@ StreamGridder::StreamGridder(Context &cx, const wsg_args &a, double wmin, double
   g.wmax_d = wmax;
   g.umax = umax;
   g.vmax = vmax;
-  choose_grid(g, a.sigma_min, a.sigma_max, env_int("WSG_TILE", 16));
+  choose_grid(g, a.sigma_min, a.sigma_max, default_tile(!dbl_));
   g.fixed = true;
   const size_t cs = dbl_ ? 16 : 8;
   band_.ensure(g.band_rows * g.nplanes * g.nv * cs);
@@ -2396,9 +2402,9 @@ void Context::autotune(const wsg_args &a, const void *vis, int candidates, wsg_s
     gp.umax = um * fm;
     gp.vmax = vm * fm;
   }
-  const int tile0 = env_int("WSG_TILE", 16);
+  const int tile0 = default_tile(gp.fp32);
   auto cands = rank_kernels(gp, a.sigma_min, a.sigma_max, tile0, size_t(candidates));
-  std::vector<int> tiles{8, 12, 16};
+  std::vector<int> tiles{12, 16, 20, 24};
   TuneChoice win;
   win.ms = 1e300;
   auto time_pair = [&]() {

@@ -108,7 +108,7 @@ class Context {
   cudaStream_t stream = nullptr, own_stream = nullptr;
   int num_sms = 148;
   int verbosity = 0;
-  int chunk_size = 1024;
+  int chunk_size = 2048;  // records per chunk at most (a bin may take several)
   wsg_stats stats;
   double cheb_err = 0;
 

@@ -419,6 +419,31 @@ __device__ __forceinline__ int band_index_j(const JobGeom &j, int u) {
   return -1;
 }
 
+// The job geometry a tile flush or stage needs, copied out of shared memory
+// into registers: inside loops that also store to shared memory the compiler
+// would otherwise reload every field for every cell.
+struct JobRegs {
+  int nu, nv, Lu, rows, P, pb0, pb1;
+  bool full;
+  void *grid;
+  __device__ __forceinline__ explicit JobRegs(const JobGeom &j)
+      : nu(j.nu), nv(j.nv), Lu(j.Lu), rows(j.band_rows), P(j.P), pb0(j.pb0), pb1(j.pb1),
+        full(j.band_full), grid(j.grid) {}
+  // band row of grid row u (wrapped into [0, nu)), or -1 outside the band
+  __device__ __forceinline__ int band_row(int u) const {
+    if (full || u <= Lu) return u;
+    return (u >= nu - Lu) ? u - (nu - rows) : -1;
+  }
+  __device__ __forceinline__ int wrap_u(int u) const {
+    u += (u < 0) ? nu : 0;
+    return u - ((u >= nu) ? nu : 0);
+  }
+  __device__ __forceinline__ int wrap_v(int v) const {
+    v += (v < 0) ? nv : 0;
+    return v - ((v >= nv) ? nv : 0);
+  }
+};
+
 constexpr uint32_t kSkip = 0xfffffffeu;  // record marker: outside its chunk's tile
 
 __device__ __forceinline__ int band_index(const DevGeom &g, int u) {
@@ -682,9 +707,11 @@ k_spread(GridArgs a, DevGeom g, DevKernel<R> kc) {
     const int ucorner = tu * g.T - g.nsafe, vcorner = tv * g.T - g.nsafe;
     const int norig = sh_norig;
     const bool by_list = norig <= kMaxOrig && norig * W * W < nbu * nbv;
-    // one (plane, row) line per warp-iteration, lanes along v (no divisions)
+    // one (plane, row) line per warp-iteration, lanes along v (no divisions);
+    // the line's band row is found once, then each cell only wraps v
     const int nline = by_list ? norig * W * W : W * nbu;
     const int linelen = by_list ? W : nbv;
+    const JobRegs jr(jb);
     for (int line = warp; line < nline; line += NWARP) {
       int p, ia, ib0;
       if (by_list) {
@@ -698,30 +725,28 @@ k_spread(GridArgs a, DevGeom g, DevKernel<R> kc) {
         ia = lu0 + (line - p * nbu);
         ib0 = lv0;
       }
-      for (int c = lane; c < linelen; c += 32) {
-      const int ib = ib0 + c;
-      const int sidx = p * tl.PS + ia * tl.RS + ib;
-      R xr, xi;
-      if (by_list) {
-        xr = take_zero(&tre[sidx]);
-        xi = take_zero(&tim[sidx]);
-      } else {
-        xr = tre[sidx];
-        xi = tim[sidx];
-        tre[sidx] = R(0);
-        tim[sidx] = R(0);
-      }
       const int plane = mp + p;
-      if ((xr != R(0) || xi != R(0)) && plane >= jb.pb0 && plane < jb.pb1) {
-        int u = ucorner + ia;
-        u += (u < 0) ? jb.nu : 0;
-        u -= (u >= jb.nu) ? jb.nu : 0;
-        int v = vcorner + ib;
-        v += (v < 0) ? jb.nv : 0;
-        v -= (v >= jb.nv) ? jb.nv : 0;
-        const int bi = band_index_j(jb, u);
-        if (bi >= 0) {
-          C *dst = reinterpret_cast<C *>(jb.grid) + (size_t(bi) * jb.P + (plane - jb.pb0)) * size_t(jb.nv) + v;
+      const int bi = jr.band_row(jr.wrap_u(ucorner + ia));
+      C *const rowp = (plane >= jr.pb0 && plane < jr.pb1 && bi >= 0)
+                          ? reinterpret_cast<C *>(jr.grid) +
+                                (size_t(bi) * jr.P + (plane - jr.pb0)) * size_t(jr.nv)
+                          : nullptr;
+      R *const lre = tre + p * tl.PS + ia * tl.RS;
+      R *const lim = tim + p * tl.PS + ia * tl.RS;
+      for (int c = lane; c < linelen; c += 32) {
+        const int ib = ib0 + c;
+        R xr, xi;
+        if (by_list) {
+          xr = take_zero(&lre[ib]);
+          xi = take_zero(&lim[ib]);
+        } else {
+          xr = lre[ib];
+          xi = lim[ib];
+          lre[ib] = R(0);
+          lim[ib] = R(0);
+        }
+        if (rowp && (xr != R(0) || xi != R(0))) {
+          C *dst = rowp + jr.wrap_v(vcorner + ib);
           if constexpr (sizeof(R) == 4) {
             atomicAdd(reinterpret_cast<float2 *>(dst), make_float2(xr, xi));
           } else {
@@ -729,7 +754,6 @@ k_spread(GridArgs a, DevGeom g, DevKernel<R> kc) {
             atomicAdd(&dst->y, xi);
           }
         }
-      }
       }
     }
   }
@@ -842,6 +866,7 @@ k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
       // (plane, row) lines over warps, lanes along v, four lines in flight
       const int nline = by_list ? norig * W * W : W * nbu;
       const int linelen = by_list ? W : nbv;
+      const JobRegs jr(jb);
       for (int l0 = warp; l0 < nline; l0 += 4 * NWARP) {
         C val[4];
         int sidx[4];
@@ -866,16 +891,12 @@ k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
             }
             sidx[q] = p * tl.PS + ia * tl.RS + ib;
             const int plane = mp + p;
-            if (plane >= jb.pb0 && plane < jb.pb1) {
-              int u = ucorner + ia;
-              u += (u < 0) ? jb.nu : 0;
-              u -= (u >= jb.nu) ? jb.nu : 0;
-              int v = vcorner + ib;
-              v += (v < 0) ? jb.nv : 0;
-              v -= (v >= jb.nv) ? jb.nv : 0;
-              const int bi = band_index_j(jb, u);
+            if (plane >= jr.pb0 && plane < jr.pb1) {
+              const int bi = jr.band_row(jr.wrap_u(ucorner + ia));
               if (bi >= 0)
-                val[q] = reinterpret_cast<const C *>(jb.grid)[(size_t(bi) * jb.P + (plane - jb.pb0)) * size_t(jb.nv) + v];
+                val[q] = reinterpret_cast<const C *>(jr.grid)[(size_t(bi) * jr.P + (plane - jr.pb0)) *
+                                                                  size_t(jr.nv) +
+                                                              jr.wrap_v(vcorner + ib)];
             }
           }
         }
