@@ -256,15 +256,24 @@ ChebCorr fit_cheb_corr(const KernelTransform &tr, double vmax) {
   return best;
 }
 
-size_t good_size_cufft(size_t n) {
-  if (n <= 2) return 2;
-  size_t best = 2 * n;
-  for (size_t f2 = 1; f2 < best; f2 *= 2)
-    for (size_t f3 = f2; f3 < best; f3 *= 3)
-      for (size_t f5 = f3; f5 < best; f5 *= 5)
-        for (size_t f7 = f5; f7 < best; f7 *= 7)
-          if (f7 >= n) best = std::min(best, f7);
-  return best;
+// Grid height for the v transform (cuFFT): the smallest n' >= n with prime
+// factors 2, 3, 5, 7, unless 2^a or 3 * 2^a is at most 8% longer -- cuFFT
+// transforms those fastest per point on the B200 (6144 takes 7% less time
+// than 6000 = 2^4 * 3 * 5^3 for 2.4% more points).
+size_t good_size_v(size_t n) {
+  n = std::max<size_t>(n, 2);
+  size_t smooth = 2 * n;
+  for (size_t f2 = 1; f2 < smooth; f2 *= 2)
+    for (size_t f3 = f2; f3 < smooth; f3 *= 3)
+      for (size_t f5 = f3; f5 < smooth; f5 *= 5)
+        for (size_t f7 = f5; f7 < smooth; f7 *= 7)
+          if (f7 >= n) smooth = std::min(smooth, f7);
+  size_t p23 = ~size_t(0);
+  for (size_t p = 1; p < 4 * n; p *= 2) {
+    if (p >= n) p23 = std::min(p23, p);
+    if (3 * p >= n) p23 = std::min(p23, 3 * p);
+  }
+  return (double(p23) <= 1.08 * double(smooth)) ? p23 : smooth;
 }
 
 namespace {
@@ -376,7 +385,7 @@ void choose_grid(GridPlan &g, double sigma_min, double sigma_max, int tile, bool
     GridPlan t = g;
     t.kernel = k;
     if (!pick_nu(g.nx * k.sigma, umax_px, k.W, g.fp32, t.nu, t.logM, t.K)) continue;
-    t.nv = 2 * good_size_cufft(size_t(g.ny * k.sigma * 0.5) + 1);
+    t.nv = 2 * good_size_v(size_t(g.ny * k.sigma * 0.5) + 1);
     if (pow2_v) {
       size_t p2 = 256;
       while (p2 < size_t(g.ny * k.sigma) + 2) p2 *= 2;

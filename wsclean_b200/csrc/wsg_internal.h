@@ -88,8 +88,9 @@ struct ChebCorr {
 };
 ChebCorr fit_cheb_corr(const KernelTransform &tr, double vmax);
 
-// Smallest n' >= n whose prime factors are 2,3,5,7 (fast cuFFT sizes).
-size_t good_size_cufft(size_t n);
+// Half grid height for the v transform: the smallest 2,3,5,7-smooth n' >= n,
+// or 2^a / 3 * 2^a when that is at most 8% longer (fastest in cuFFT).
+size_t good_size_v(size_t n);
 
 // Everything one ms2dirty/dirty2ms call needs to know, in FP64.
 struct GridPlan {
