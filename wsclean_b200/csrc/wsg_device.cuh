@@ -921,6 +921,7 @@ k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
         stage_batch<R, W>(recs, b0, nb, lane, tu, tv, mp, g, kc, kv, vv, luvs, a.err, bb0, bb1,
                           bb2, bb3, a.vis_in, a.vis_in_double);
         __syncwarp();
+        R osr = R(0), osi = R(0);  // this lane's record of the batch
         for (int jj = 0; jj < nb; ++jj) {
           const uint32_t luv = luvs[jj];
           if (luv == kSkip) continue;
@@ -952,22 +953,29 @@ k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
             const R f = ok[k] ? kb[2 * W + pp[k]] * kb[cu[k]] : R(0);
             sacc = cfma_real(t, f, sacc);
           }
-          R sr = warp_sum(sacc.x);
-          R si = warp_sum(sacc.y);
-          if (lane == 0) {
-            const int s = b0 + jj;
-            if (direct) {
-              const Rec rr = recs[s];
-              const uint32_t idx = rr.idx & 0x7fffffffu;
-              if (rr.idx & 0x80000000u) si = -si;
-              const double orr = double(rr.vr) * double(sr) - double(rr.vi) * double(si);
-              const double oi = double(rr.vr) * double(si) + double(rr.vi) * double(sr);
-              store_vis(a.vis_out, a.vis_double, a.vis_accumulate, idx, orr, oi);
-            } else {
-              C *accp = reinterpret_cast<C *>(a.acc) + s;
-              atomicAdd(&accp->x, sr);
-              atomicAdd(&accp->y, si);
-            }
+          // every lane gets the sum; lane jj keeps record jj's
+          const R sr = warp_sum(sacc.x);
+          const R si = warp_sum(sacc.y);
+          if (lane == jj) {
+            osr = sr;
+            osi = si;
+          }
+        }
+        // lanes finalise their own records of the batch together (one
+        // coalesced record load, instead of one lane per record in turn)
+        if (lane < nb && luvs[lane] != kSkip) {
+          const int s = b0 + lane;
+          if (direct) {
+            const Rec rr = recs[s];
+            const uint32_t idx = rr.idx & 0x7fffffffu;
+            const R si = (rr.idx & 0x80000000u) ? -osi : osi;
+            const double orr = double(rr.vr) * double(osr) - double(rr.vi) * double(si);
+            const double oi = double(rr.vr) * double(si) + double(rr.vi) * double(osr);
+            store_vis(a.vis_out, a.vis_double, a.vis_accumulate, idx, orr, oi);
+          } else {
+            C *accp = reinterpret_cast<C *>(a.acc) + s;
+            atomicAdd(&accp->x, osr);
+            atomicAdd(&accp->y, osi);
           }
         }
         __syncwarp();
