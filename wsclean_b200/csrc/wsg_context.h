@@ -159,6 +159,9 @@ class Context {
     bool valid = false;
   };
   GridMemo grid_memo[2];
+  // device geometry (DevGeom bytes) of the last planned grid: the next scan
+  // writes sort keys for it, used when the next plan comes out the same
+  std::vector<unsigned char> spec_geom;
   // correction-table cache
   std::tuple<int, double, double, size_t, size_t, size_t, size_t, double> corr_key;
   ChebCorr corr_cc;

@@ -181,11 +181,18 @@ __device__ __forceinline__ T warp_sum(T v) {
 
 // --------------------------------------------------------------- k_scan
 
-template <typename TV, typename TW>
-__global__ void k_scan(size_t nrows, int nchan, const double *__restrict__ uvw,
-                       const double *__restrict__ fovc, const TV *__restrict__ vis,
-                       const TW *__restrict__ wgt, const uint8_t *__restrict__ mask,
-                       int gridding, double vfac, ScanOut *out, TV *__restrict__ vis_out) {
+// Active mask, |w| range, max |u|, |v| and the active count of the
+// visibilities (scanData, wgridder.h:1578-1618); with KEYS, also the sort
+// key of every visibility for the grid geometry g, as k_keys writes it (the
+// caller checks afterwards that the planned geometry is g).
+template <typename TV, typename TW, bool KEYS>
+__device__ __forceinline__ void scan_rows(size_t nrows, int nchan, const double *__restrict__ uvw,
+                                          const double *__restrict__ fovc,
+                                          const TV *__restrict__ vis, const TW *__restrict__ wgt,
+                                          const uint8_t *__restrict__ mask, int gridding,
+                                          double vfac, ScanOut *out, TV *__restrict__ vis_out,
+                                          const DevGeom &g, uint32_t *__restrict__ keys,
+                                          uint32_t *__restrict__ vals) {
   double lwmin = 1e300, lwmax = 0, lumax = 0, lvmax = 0;
   unsigned long long cnt = 0;
   for (size_t r = blockIdx.x * size_t(blockDim.x) + threadIdx.x; r < nrows;
@@ -204,6 +211,7 @@ __global__ void k_scan(size_t nrows, int nchan, const double *__restrict__ uvw,
         act = (!wgt || wgt[k] != 0) && (!mask || mask[k] != 0);
         if (!act && vis_out) vis_out[k] = TV{0, 0};
       }
+      uint32_t key = KEYS ? g.inactive_key : 0u;
       if (act) {
         double f = fovc[c];
         double aw = fabs(w * f);
@@ -212,6 +220,15 @@ __global__ void k_scan(size_t nrows, int nchan, const double *__restrict__ uvw,
         lumax = fmax(lumax, fabs(u * f));
         lvmax = fmax(lvmax, fabs(v * f));
         ++cnt;
+        if constexpr (KEYS) {
+          VisPix p;
+          vis_pixel(g, u * f, v * f, w * f, p);
+          key = bin_key(g, p);
+        }
+      }
+      if constexpr (KEYS) {
+        keys[k] = key;
+        vals[k] = uint32_t(k);
       }
     }
   }
@@ -230,6 +247,29 @@ __global__ void k_scan(size_t nrows, int nchan, const double *__restrict__ uvw,
     atomicMax(&out->vmax_bits, (unsigned long long)__double_as_longlong(lvmax));
     atomicAdd(&out->nvis, cnt);
   }
+}
+
+template <typename TV, typename TW>
+__global__ void k_scan(size_t nrows, int nchan, const double *__restrict__ uvw,
+                       const double *__restrict__ fovc, const TV *__restrict__ vis,
+                       const TW *__restrict__ wgt, const uint8_t *__restrict__ mask,
+                       int gridding, double vfac, ScanOut *out, TV *__restrict__ vis_out) {
+  const DevGeom g{};
+  scan_rows<TV, TW, false>(nrows, nchan, uvw, fovc, vis, wgt, mask, gridding, vfac, out, vis_out,
+                           g, nullptr, nullptr);
+}
+
+// The scan with the keys of an expected geometry: when consecutive calls
+// plan the same grid (the usual case: the same image and data extent), the
+// separate pass of k_keys over uvw and the visibilities is not needed.
+template <typename TV, typename TW>
+__global__ void k_scan_keys(size_t nrows, int nchan, const double *__restrict__ uvw,
+                            const double *__restrict__ fovc, const TV *__restrict__ vis,
+                            const TW *__restrict__ wgt, const uint8_t *__restrict__ mask,
+                            int gridding, double vfac, ScanOut *out, TV *__restrict__ vis_out,
+                            DevGeom g, uint32_t *__restrict__ keys, uint32_t *__restrict__ vals) {
+  scan_rows<TV, TW, true>(nrows, nchan, uvw, fovc, vis, wgt, mask, gridding, vfac, out, vis_out,
+                          g, keys, vals);
 }
 
 // --------------------------------------------------------------- k_keys
