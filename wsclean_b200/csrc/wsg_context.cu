@@ -895,7 +895,8 @@ size_t Context::choose_planes(const GridPlan &g, bool gridding) {
 }
 
 template <typename R>
-void Context::grid_core(const wsg_args &a, const Staged &s, double *img, bool accumulate) {
+bool Context::grid_core(const wsg_args &a, const Staged &s, double *img, bool accumulate,
+                        void *direct_out) {
   const bool dbl = sizeof(R) == 8;
   GridPlan gp;
   gp.nx = a.npix_x;
@@ -913,10 +914,10 @@ void Context::grid_core(const wsg_args &a, const Staged &s, double *img, bool ac
   const size_t npix = a.npix_x * a.npix_y;
 
   CK(cudaEventRecord(ev[0], stream));
-  if (!accumulate) CK(cudaMemsetAsync(img, 0, npix * sizeof(double), stream));
   if (!prepare<R>(a, s, true, nullptr, gp)) {
+    if (!accumulate) CK(cudaMemsetAsync(img, 0, npix * sizeof(double), stream));
     record_stats(gp, true, 0);
-    return;
+    return false;
   }
   CK(cudaEventRecord(ev[1], stream));
   ChebCorr cc = upload_corrections(gp);
@@ -925,6 +926,11 @@ void Context::grid_core(const wsg_args &a, const Staged &s, double *img, bool ac
   mark("corrections");
   const size_t P = choose_planes(gp, true);
   mark("choose_planes");
+  // one pass over all planes and nothing to accumulate: the w-screen sum
+  // goes straight to the caller's image, else through the FP64 accumulator
+  const bool direct = direct_out && !accumulate && P >= gp.nplanes;
+  const int out_mode = direct ? (a.dirty_type == WSG_F64 ? 2 : 1) : 0;
+  if (!accumulate && !direct) CK(cudaMemsetAsync(img, 0, npix * sizeof(double), stream));
   const size_t cs = 2 * sizeof(R);
   const size_t nv = gp.nv;
   char *band = reinterpret_cast<char *>(b_band.ensure(gp.band_rows * P * nv * cs));
@@ -972,7 +978,7 @@ void Context::grid_core(const wsg_args &a, const Staged &s, double *img, bool ac
     sa.pb0 = int(pb0);
     sa.npl = int(npl);
     dim3 sg((gp.nx + 31) / 32, (gp.ny + 31) / 32);
-    k_screen_add<R><<<sg, 256, 0, stream>>>(sa, H, img);
+    k_screen_add<R><<<sg, 256, 0, stream>>>(sa, H, img, direct_out, out_mode);
     cuda_check(cudaGetLastError(), "k_screen_add launch");
   g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     CK(cudaEventRecord(ev[5], stream));
@@ -1002,10 +1008,12 @@ void Context::grid_core(const wsg_args &a, const Staged &s, double *img, bool ac
   mark("passes-done");
   if (verbosity > 0) print_report(gp, true, P);
   print_marks("ms2dirty");
+  return direct;
 }
 
 template <typename R>
-void Context::degrid_core(const wsg_args &a, const Staged &s, const double *img, void *vis_out) {
+void Context::degrid_core(const wsg_args &a, const Staged &s, const double *img, void *vis_out,
+                          const void *direct_in) {
   const bool dbl = sizeof(R) == 8;
   GridPlan gp;
   gp.nx = a.npix_x;
@@ -1072,7 +1080,10 @@ void Context::degrid_core(const wsg_args &a, const Staged &s, const double *img,
     sa.pb0 = int(pb0);
     sa.npl = int(npl);
     dim3 sg((gp.nx + 31) / 32, (gp.ny + 31) / 32);
-    k_screen_put<R><<<sg, 256, 0, stream>>>(sa, img, H);
+    // the caller's image itself (FP32 or FP64) when given, else the FP64 copy
+    const void *src = direct_in ? direct_in : static_cast<const void *>(img);
+    const int src_f32 = (direct_in && a.dirty_type == WSG_F32) ? 1 : 0;
+    k_screen_put<R><<<sg, 256, 0, stream>>>(sa, src, src_f32, H);
     cuda_check(cudaGetLastError(), "k_screen_put launch");
   g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     CK(cudaEventRecord(ev[3], stream));
@@ -1240,19 +1251,19 @@ void Context::ms2dirty(const wsg_args &a, const void *vis, void *dirty, int accu
     cuda_check(cudaGetLastError(), "k_load_image launch");
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
   }
-  if (a.precision == WSG_PREC_FP64)
-    grid_core<double>(a, s, img, accumulate != 0);
-  else
-    grid_core<float>(a, s, img, accumulate != 0);
-  // convert/copy out
   void *dout = ddev ? dirty : sl.out.ensure(npix * dsz);
-  int nb = launch_blocks(npix, 256);
-  if (a.dirty_type == WSG_F64)
-    k_store_image<double><<<nb, 256, 0, stream>>>(npix, img, (double *)dout);
-  else
-    k_store_image<float><<<nb, 256, 0, stream>>>(npix, img, (float *)dout);
-  cuda_check(cudaGetLastError(), "k_store_image launch");
-  g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+  const bool direct = (a.precision == WSG_PREC_FP64)
+                          ? grid_core<double>(a, s, img, accumulate != 0, dout)
+                          : grid_core<float>(a, s, img, accumulate != 0, dout);
+  if (!direct) {  // convert/copy out of the FP64 accumulator
+    int nb = launch_blocks(npix, 256);
+    if (a.dirty_type == WSG_F64)
+      k_store_image<double><<<nb, 256, 0, stream>>>(npix, img, (double *)dout);
+    else
+      k_store_image<float><<<nb, 256, 0, stream>>>(npix, img, (float *)dout);
+    cuda_check(cudaGetLastError(), "k_store_image launch");
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+  }
   cudaStream_t last = stream;
   if (!ddev) {
     CK(cudaEventRecord(ev_done, stream));
@@ -1282,23 +1293,16 @@ void Context::dirty2ms(const wsg_args &a, const void *dirty, void *vis) {
   CK(cudaStreamWaitEvent(stream, ev_in, 0));
   ScanPlacement place(*this, sl, s.uvw != a.uvw && (a.wgt == nullptr || s.wgt != a.wgt) &&
                                      (a.mask == nullptr || s.mask != a.mask));
-  double *img = reinterpret_cast<double *>(b_img.ensure(npix * sizeof(double)));
-  int nb = launch_blocks(npix, 256);
-  if (a.dirty_type == WSG_F64)
-    k_load_image<double><<<nb, 256, 0, stream>>>(npix, (const double *)din, img, 0);
-  else
-    k_load_image<float><<<nb, 256, 0, stream>>>(npix, (const float *)din, img, 0);
-  cuda_check(cudaGetLastError(), "k_load_image launch");
-  g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+  // (the w-screen reads the model image in place: no FP64 copy)
   const bool vdev = is_device_pointer(vis);
   void *vout = vdev ? vis : sl.vis.ensure(vbytes);
   // inactive visibilities are zeroed; with no active ones at all the whole
   // output is zero
   CK(cudaMemsetAsync(vout, 0, vbytes, stream));
   if (a.precision == WSG_PREC_FP64)
-    degrid_core<double>(a, s, img, vout);
+    degrid_core<double>(a, s, nullptr, vout, din);
   else
-    degrid_core<float>(a, s, img, vout);
+    degrid_core<float>(a, s, nullptr, vout, din);
   cudaStream_t last = stream;
   if (!vdev) {
     CK(cudaEventRecord(ev_done, stream));
@@ -1637,7 +1641,7 @@ void Plan::enqueue_grid(const void *vis, void *const *dirty, int accumulate) {
     sa.pb0 = 0;
     sa.npl = int(gp.nplanes);
     dim3 sg((gp.nx + 31) / 32, (gp.ny + 31) / 32);
-    k_screen_add<R><<<sg, 256, 0, st>>>(sa, H_.p, img);
+    k_screen_add<R><<<sg, 256, 0, st>>>(sa, H_.p, img, nullptr, 0);
     cuda_check(cudaGetLastError(), "k_screen_add launch");
     if (a_.dirty_type == WSG_F64)
       k_store_image<double><<<nb, 256, 0, st>>>(npix, img, (double *)dirty[j]);
@@ -1676,7 +1680,7 @@ void Plan::enqueue_degrid(const void *const *dirty, void *vis) {
     sa.pb0 = 0;
     sa.npl = int(gp.nplanes);
     dim3 sg((gp.nx + 31) / 32, (gp.ny + 31) / 32);
-    k_screen_put<R><<<sg, 256, 0, st>>>(sa, img, H_.p);
+    k_screen_put<R><<<sg, 256, 0, st>>>(sa, img, 0, H_.p);
     cuda_check(cudaGetLastError(), "k_screen_put launch");
     char *band = static_cast<char *>(band_.p) + pj.band_off;
     clear_outside_columns(band, gp.band_rows * gp.nplanes, gp.nv, gp.ny, cs, st);
@@ -2080,7 +2084,7 @@ void StreamGridder::finish_t(void *dirty, int accumulate) {
     sa.pb0 = int(p0);
     sa.npl = int(np);
     dim3 sg((g.nx + 31) / 32, (g.ny + 31) / 32);
-    k_screen_add<R><<<sg, 256, 0, st>>>(sa, H_.p, img);
+    k_screen_add<R><<<sg, 256, 0, st>>>(sa, H_.p, img, nullptr, 0);
     cuda_check(cudaGetLastError(), "k_screen_add launch");
   }
   void *dout = ddev ? dirty : cx_.b_out.ensure(npix * dsz);
@@ -2117,7 +2121,7 @@ void StreamGridder::predict_begin_t(const double *img) {
     sa.pb0 = int(p0);
     sa.npl = int(np);
     dim3 sg((g.nx + 31) / 32, (g.ny + 31) / 32);
-    k_screen_put<R><<<sg, 256, 0, st>>>(sa, img, H_.p);
+    k_screen_put<R><<<sg, 256, 0, st>>>(sa, img, 0, H_.p);
     cuda_check(cudaGetLastError(), "k_screen_put launch");
     ColArgs ca = make_col(g, g.nplanes, tw_.p, static_cast<char *>(band_.p) + p0 * g.nv * cs, H_.p);
     ColKernels<R>::run(g.logM, false, ca, int(np), st);
@@ -2598,10 +2602,12 @@ void Gridder::predict_visibilities(size_t nrows, size_t nchan, const double *uvw
 
 template bool Context::prepare<float>(const wsg_args &, const Staged &, bool, void *, GridPlan &);
 template bool Context::prepare<double>(const wsg_args &, const Staged &, bool, void *, GridPlan &);
-template void Context::grid_core<float>(const wsg_args &, const Staged &, double *, bool);
-template void Context::grid_core<double>(const wsg_args &, const Staged &, double *, bool);
-template void Context::degrid_core<float>(const wsg_args &, const Staged &, const double *, void *);
-template void Context::degrid_core<double>(const wsg_args &, const Staged &, const double *, void *);
+template bool Context::grid_core<float>(const wsg_args &, const Staged &, double *, bool, void *);
+template bool Context::grid_core<double>(const wsg_args &, const Staged &, double *, bool, void *);
+template void Context::degrid_core<float>(const wsg_args &, const Staged &, const double *, void *,
+                                          const void *);
+template void Context::degrid_core<double>(const wsg_args &, const Staged &, const double *, void *,
+                                           const void *);
 
 
 // ====================================================================
@@ -2894,7 +2900,7 @@ void ms2dirty_noalloc(const wsg_args &a, const void *vis, void *dirty, cudaStrea
       sa.pb0 = int(pb0);
       sa.npl = int(npl);
       dim3 sg((gp.nx + 31) / 32, (gp.ny + 31) / 32);
-      k_screen_add<float><<<sg, 256, 0, stream>>>(sa, H, img);
+      k_screen_add<float><<<sg, 256, 0, stream>>>(sa, H, img, nullptr, 0);
       cuda_check(cudaGetLastError(), "k_screen_add launch");
       g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     }

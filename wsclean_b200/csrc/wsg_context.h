@@ -77,9 +77,17 @@ class Context {
 
   const void *stage_in(const void *p, size_t bytes, DevBuf &buf, cudaStream_t st = nullptr);
   template <typename R>
-  void grid_core(const wsg_args &a, const Staged &s, double *img, bool accumulate);
+  // Grids into the FP64 accumulator img (+= with accumulate, else =), or --
+  // when direct_out is given, nothing is accumulated and one pass covers all
+  // planes -- writes the image of type a.dirty_type to direct_out and
+  // returns true.
+  bool grid_core(const wsg_args &a, const Staged &s, double *img, bool accumulate,
+                 void *direct_out = nullptr);
   template <typename R>
-  void degrid_core(const wsg_args &a, const Staged &s, const double *img, void *vis_out);
+  // Degrids the FP64 image img, or the caller's image direct_in (of type
+  // a.dirty_type) when given.
+  void degrid_core(const wsg_args &a, const Staged &s, const double *img, void *vis_out,
+                   const void *direct_in = nullptr);
   void degrid_from_image(const wsg_args &a, const Staged &s, const double *img, void *vis,
                          size_t vbytes);
 

@@ -1710,7 +1710,11 @@ __device__ __forceinline__ void pixel_terms(const ScreenArgs &s, int i, int j,
 // ms2dirty: img(i,j) += corr(i,j) * sum_p Re(H[p][j][i] * exp(-2 pi i w_p q)),
 // FP64 phases (recurrence over planes) and FP64 accumulation.
 template <typename R>
-__global__ void __launch_bounds__(256) k_screen_add(ScreenArgs s, const void *Hv, double *img) {
+// out_mode 0: img += the sum (FP64 accumulator); 1 / 2: out = the sum as
+// FP32 / FP64 (the caller's image, when one pass covers all planes and
+// nothing is accumulated)
+__global__ void __launch_bounds__(256) k_screen_add(ScreenArgs s, const void *Hv, double *img,
+                                                    void *out, int out_mode) {
   using C = typename Cplx<R>::type;
   const C *H = reinterpret_cast<const C *>(Hv);
   __shared__ double tile[32][33];
@@ -1756,13 +1760,24 @@ __global__ void __launch_bounds__(256) k_screen_add(ScreenArgs s, const void *Hv
   __syncthreads();
   for (int k = 0; k < 4; ++k) {
     const int ii = i0 + ty + 8 * k, jj = j0 + tx;
-    if (ii < s.nx && jj < s.ny) img[size_t(ii) * s.ny + jj] += tile[tx][ty + 8 * k];
+    if (ii < s.nx && jj < s.ny) {
+      const size_t o = size_t(ii) * s.ny + jj;
+      const double x = tile[tx][ty + 8 * k];
+      if (out_mode == 0)
+        img[o] += x;
+      else if (out_mode == 1)
+        reinterpret_cast<float *>(out)[o] = float(x);
+      else
+        reinterpret_cast<double *>(out)[o] = x;
+    }
   }
 }
 
 // dirty2ms: H[p][j][i] = dirty(i,j) * corr(i,j) * exp(+2 pi i w_p q)
 template <typename R>
-__global__ void __launch_bounds__(256) k_screen_put(ScreenArgs s, const double *img, void *Hv) {
+// in_f32: img points to the caller's FP32 image instead of the FP64 copy
+__global__ void __launch_bounds__(256) k_screen_put(ScreenArgs s, const void *img, int in_f32,
+                                                    void *Hv) {
   using C = typename Cplx<R>::type;
   C *H = reinterpret_cast<C *>(Hv);
   __shared__ double tile[32][33];
@@ -1770,7 +1785,13 @@ __global__ void __launch_bounds__(256) k_screen_put(ScreenArgs s, const double *
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   for (int k = 0; k < 4; ++k) {  // coalesced read along j
     const int ii = i0 + ty + 8 * k, jj = j0 + tx;
-    tile[tx][ty + 8 * k] = (ii < s.nx && jj < s.ny) ? img[size_t(ii) * s.ny + jj] : 0.0;
+    double x = 0.0;
+    if (ii < s.nx && jj < s.ny) {
+      const size_t o = size_t(ii) * s.ny + jj;
+      x = in_f32 ? double(reinterpret_cast<const float *>(img)[o])
+                 : reinterpret_cast<const double *>(img)[o];
+    }
+    tile[tx][ty + 8 * k] = x;
   }
   __syncthreads();
   const int i = i0 + tx;
