@@ -180,7 +180,7 @@ Context::~Context() {
 
 std::vector<DevBuf *> Context::all_buffers() {
   return {&b_uvw, &b_fovc, &b_vis, &b_wgt, &b_mask, &b_keys_a, &b_keys_b, &b_vals_a,
-          &b_vals_b, &b_cub, &b_rec, &b_chunks, &b_small, &b_band, &b_H,
+          &b_vals_b, &b_cub, &b_rec, &b_chunks, &b_small, &b_band, &b_bandf, &b_H,
           &b_img, &b_img2, &b_acc, &b_cf, &b_tw, &b_fftwork, &b_out};
 }
 
@@ -204,6 +204,7 @@ void Context::release_buffers() {
   for (auto &kv : fft_plans) cufftDestroy(kv.second);
   fft_plans.clear();
   for (auto *b : all_buffers()) b->release();
+  band_dirty = BandDirty{};
   corr_valid = false;
   tw_valid = false;
 }
@@ -326,6 +327,15 @@ void clear_outside_columns(void *band, size_t rows, size_t nv, size_t ny, size_t
   cuda_check(cudaMemset2DAsync(static_cast<char *>(band) + (ny / 2) * cs, nv * cs, 0,
                                (nv - ny) * cs, rows, st),
              "cudaMemset2DAsync");
+}
+
+// Half-width in cells of the v columns the spread can write ([0, Lv] and
+// [nv - Lv, nv)): the largest |v| plus half a kernel and a margin, as the u
+// band (set_band); -1 when that covers the whole row.
+long band_v_halfwidth(const GridPlan &g) {
+  const double L = std::ceil(g.vmax * g.py * double(g.nv) + 0.5 * g.kernel.W + 2.0);
+  if (!(L >= 0) || 2.0 * L + 1.0 >= double(g.nv)) return -1;
+  return long(L);
 }
 
 int launch_blocks(size_t n, int threads) {
@@ -874,9 +884,25 @@ const void *Context::upload_twiddles(const GridPlan &g, bool dbl) {
 // a slow driver query (milliseconds, and tens of them when other processes
 // query the GPU), so a repeated plan whose buffers are still held reuses the
 // previous answer -- kept per direction, for alternating ms2dirty / dirty2ms.
+// Zeroes the spread's band grid before a pass: whole when its layout or
+// address changed (or nothing is known), else only the v columns the last
+// spread into it can have written.
+void Context::clear_band(void *band, size_t rows, size_t nv, size_t cs) {
+  const BandDirty d = band_dirty;
+  band_dirty = BandDirty{};  // unknown until the caller records the new spread
+  if (d.p == band && d.rows == rows && d.nv == nv && d.cs == cs && d.Lv >= 0) {
+    const size_t L = size_t(d.Lv);
+    CK(cudaMemset2DAsync(band, nv * cs, 0, (L + 1) * cs, rows, stream));
+    CK(cudaMemset2DAsync(static_cast<char *>(band) + (nv - L) * cs, nv * cs, 0, L * cs, rows,
+                         stream));
+  } else {
+    CK(cudaMemsetAsync(band, 0, rows * nv * cs, stream));
+  }
+}
+
 size_t Context::choose_planes(const GridPlan &g, bool gridding) {
   const size_t per = plan_bytes(g, 1, gridding);
-  const size_t held = b_band.n + b_H.n;
+  const size_t held = b_band.n + b_bandf.n + b_H.n;
   const auto key = std::make_tuple(per, g.nplanes, int(gridding));
   PlanesMemo &pm = planes_memo[gridding ? 1 : 0];
   if (!(pm.valid && key == pm.key && held >= pm.P * per)) {
@@ -933,10 +959,15 @@ bool Context::grid_core(const wsg_args &a, const Staged &s, double *img, bool ac
   if (!accumulate && !direct) CK(cudaMemsetAsync(img, 0, npix * sizeof(double), stream));
   const size_t cs = 2 * sizeof(R);
   const size_t nv = gp.nv;
-  char *band = reinterpret_cast<char *>(b_band.ensure(gp.band_rows * P * nv * cs));
+  // the spread writes `band`; the v transform goes out of place to `bandf`,
+  // so `band` stays zero outside the columns the spread wrote
+  const size_t rowsP = gp.band_rows * P;
+  char *band = reinterpret_cast<char *>(b_band.ensure(rowsP * nv * cs));
+  char *bandf = reinterpret_cast<char *>(b_bandf.ensure(rowsP * nv * cs));
   char *H = reinterpret_cast<char *>(b_H.ensure(P * gp.ny * gp.nx * cs));
   const void *tw = upload_twiddles(gp, dbl);
-  ColArgs ca = make_col(gp, P, tw, band, H);
+  ColArgs ca = make_col(gp, P, tw, bandf, H);
+  const long Lv = band_v_halfwidth(gp);
   const TileLayout tl = make_layout(gp.T, gp.kernel.W);
   const size_t smem = GridKernels<R>::smem_bytes(tl, gp.kernel.W, true);
   int *counter = reinterpret_cast<int *>(reinterpret_cast<char *>(b_small.p) + 2048);
@@ -960,16 +991,17 @@ bool Context::grid_core(const wsg_args &a, const Staged &s, double *img, bool ac
   for (size_t pb0 = 0; pb0 < gp.nplanes; pb0 += P) {
     const size_t npl = std::min(P, gp.nplanes - pb0);
     CK(cudaEventRecord(ev[2], stream));
-    CK(cudaMemsetAsync(band, 0, gp.band_rows * P * nv * cs, stream));
+    clear_band(band, rowsP, nv, cs);
     CK(cudaMemsetAsync(counter, 0, sizeof(int), stream));
     ga.pb0 = int(pb0);
     ga.pb1 = int(pb0 + npl);
     GridKernels<R>::dispatch(gp.kernel.W, true, num_sms, smem, stream, ga, g, kc);
+    band_dirty = BandDirty{band, rowsP, nv, cs, Lv};
     CK(cudaEventRecord(ev[3], stream));
     // transform along v: every (band row, plane) is a contiguous row of nv
     {
-      cufftHandle h = fft_plan(int(nv), 1, int(nv), 1, int(nv), int(gp.band_rows * P), dbl);
-      fft_exec(h, band, band, dir, dbl);
+      cufftHandle h = fft_plan(int(nv), 1, int(nv), 1, int(nv), int(rowsP), dbl);
+      fft_exec(h, band, bandf, dir, dbl);
     }
     // pruned transform along u: band rows of the image columns -> image rows
     ColKernels<R>::run(gp.logM, true, ca, int(npl), stream);
@@ -1043,7 +1075,7 @@ void Context::degrid_core(const wsg_args &a, const Staged &s, const double *img,
   mark("choose_planes");
   const size_t cs = 2 * sizeof(R);
   const size_t nv = gp.nv;
-  char *band = reinterpret_cast<char *>(b_band.ensure(gp.band_rows * P * nv * cs));
+  char *band = reinterpret_cast<char *>(b_bandf.ensure(gp.band_rows * P * nv * cs));
   char *H = reinterpret_cast<char *>(b_H.ensure(P * gp.ny * gp.nx * cs));
   const void *tw = upload_twiddles(gp, dbl);
   ColArgs ca = make_col(gp, P, tw, band, H);

@@ -123,7 +123,16 @@ class Context {
   // buffers
   DevBuf b_uvw, b_fovc, b_vis, b_wgt, b_mask;
   DevBuf b_keys_a, b_keys_b, b_vals_a, b_vals_b, b_cub, b_rec, b_chunks, b_small;
-  DevBuf b_band, b_H;
+  DevBuf b_band, b_bandf, b_H;  // spread grid, v-transformed grid, u-transformed rows
+  // the part of b_band the last spread may have written: columns [0, Lv]
+  // and [nv - Lv, nv) of its rows (Lv < 0: unknown)
+  struct BandDirty {
+    void *p = nullptr;
+    size_t rows = 0, nv = 0, cs = 0;
+    long Lv = -1;
+  };
+  BandDirty band_dirty;
+  void clear_band(void *band, size_t rows, size_t nv, size_t cs);
   DevBuf b_img, b_img2, b_acc, b_cf, b_tw, b_fftwork, b_out;
 
  private:
