@@ -488,8 +488,9 @@ std::vector<std::pair<int, double>> rank_kernels(const GridPlan &g, double sigma
 
 size_t plan_bytes(const GridPlan &g, size_t planes, bool gridding) {
   const size_t cs = g.fp32 ? 8 : 16;
-  // gridding keeps the spread grid and its v transform apart
-  return planes * cs * ((gridding ? 2 : 1) * g.band_rows * g.nv + g.ny * g.nx);
+  // both directions keep the grid and its v transform apart
+  (void)gridding;
+  return planes * cs * (2 * g.band_rows * g.nv + g.ny * g.nx);
 }
 
 }  // namespace wsg

@@ -180,7 +180,7 @@ Context::~Context() {
 
 std::vector<DevBuf *> Context::all_buffers() {
   return {&b_uvw, &b_fovc, &b_vis, &b_wgt, &b_mask, &b_keys_a, &b_keys_b, &b_vals_a,
-          &b_vals_b, &b_cub, &b_rec, &b_chunks, &b_small, &b_band, &b_bandf, &b_H,
+          &b_vals_b, &b_cub, &b_rec, &b_chunks, &b_small, &b_band, &b_bandf, &b_bandd, &b_H,
           &b_img, &b_img2, &b_acc, &b_cf, &b_tw, &b_fftwork, &b_out};
 }
 
@@ -205,6 +205,7 @@ void Context::release_buffers() {
   fft_plans.clear();
   for (auto *b : all_buffers()) b->release();
   band_dirty = BandDirty{};
+  bandd_zero = BandDirty{};
   corr_valid = false;
   tw_valid = false;
 }
@@ -902,7 +903,7 @@ void Context::clear_band(void *band, size_t rows, size_t nv, size_t cs) {
 
 size_t Context::choose_planes(const GridPlan &g, bool gridding) {
   const size_t per = plan_bytes(g, 1, gridding);
-  const size_t held = b_band.n + b_bandf.n + b_H.n;
+  const size_t held = b_band.n + b_bandf.n + b_bandd.n + b_H.n;
   const auto key = std::make_tuple(per, g.nplanes, int(gridding));
   PlanesMemo &pm = planes_memo[gridding ? 1 : 0];
   if (!(pm.valid && key == pm.key && held >= pm.P * per)) {
@@ -1075,10 +1076,15 @@ void Context::degrid_core(const wsg_args &a, const Staged &s, const double *img,
   mark("choose_planes");
   const size_t cs = 2 * sizeof(R);
   const size_t nv = gp.nv;
-  char *band = reinterpret_cast<char *>(b_bandf.ensure(gp.band_rows * P * nv * cs));
+  // the transposed u transform fills the image columns of `bandi`, whose
+  // other columns stay zero from call to call; the v transform goes out of
+  // place to `band`, which the interpolation reads
+  const size_t rowsP = gp.band_rows * P;
+  char *bandi = reinterpret_cast<char *>(b_bandd.ensure(rowsP * nv * cs));
+  char *band = reinterpret_cast<char *>(b_bandf.ensure(rowsP * nv * cs));
   char *H = reinterpret_cast<char *>(b_H.ensure(P * gp.ny * gp.nx * cs));
   const void *tw = upload_twiddles(gp, dbl);
-  ColArgs ca = make_col(gp, P, tw, band, H);
+  ColArgs ca = make_col(gp, P, tw, bandi, H);
   const TileLayout tl = make_layout(gp.T, gp.kernel.W);
   const size_t smem = GridKernels<R>::smem_bytes(tl, gp.kernel.W, false);
   int *counter = reinterpret_cast<int *>(reinterpret_cast<char *>(b_small.p) + 2048);
@@ -1121,12 +1127,18 @@ void Context::degrid_core(const wsg_args &a, const Staged &s, const double *img,
     CK(cudaEventRecord(ev[3], stream));
     // pruned transform along u (transposed): image rows -> band rows of the
     // image columns; the other columns of the band grid stay zero
-    clear_outside_columns(band, gp.band_rows * P, nv, gp.ny, cs, stream);
+    const BandDirty zl{bandi, rowsP, nv, cs, long(gp.ny)};
+    if (!(bandd_zero.p == zl.p && bandd_zero.rows == zl.rows && bandd_zero.nv == zl.nv &&
+          bandd_zero.cs == zl.cs && bandd_zero.Lv == zl.Lv)) {
+      bandd_zero = BandDirty{};
+      clear_outside_columns(bandi, rowsP, nv, gp.ny, cs, stream);
+      bandd_zero = zl;
+    }
     ColKernels<R>::run(gp.logM, false, ca, int(npl), stream);
     // transform along v
     {
-      cufftHandle h = fft_plan(int(nv), 1, int(nv), 1, int(nv), int(gp.band_rows * P), dbl);
-      fft_exec(h, band, band, dir, dbl);
+      cufftHandle h = fft_plan(int(nv), 1, int(nv), 1, int(nv), int(rowsP), dbl);
+      fft_exec(h, bandi, band, dir, dbl);
     }
     CK(cudaEventRecord(ev[4], stream));
     CK(cudaMemsetAsync(counter, 0, sizeof(int), stream));

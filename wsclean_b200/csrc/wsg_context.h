@@ -123,7 +123,8 @@ class Context {
   // buffers
   DevBuf b_uvw, b_fovc, b_vis, b_wgt, b_mask;
   DevBuf b_keys_a, b_keys_b, b_vals_a, b_vals_b, b_cub, b_rec, b_chunks, b_small;
-  DevBuf b_band, b_bandf, b_H;  // spread grid, v-transformed grid, u-transformed rows
+  // spread grid, v-transformed grid, degridding input grid, u-transformed rows
+  DevBuf b_band, b_bandf, b_bandd, b_H;
   // the part of b_band the last spread may have written: columns [0, Lv]
   // and [nv - Lv, nv) of its rows (Lv < 0: unknown)
   struct BandDirty {
@@ -132,6 +133,9 @@ class Context {
     long Lv = -1;
   };
   BandDirty band_dirty;
+  // b_bandd's layout whose columns outside the ny image columns are known to
+  // be zero (Lv holds ny; p == nullptr: unknown)
+  BandDirty bandd_zero;
   void clear_band(void *band, size_t rows, size_t nv, size_t cs);
   DevBuf b_img, b_img2, b_acc, b_cf, b_tw, b_fftwork, b_out;
 
