@@ -386,9 +386,10 @@ struct GridKernels {
   }
   // warps that share one record (more than one when a lane's share of the
   // W x W (plane, u-row) pairs would exceed PPL)
-  static int groups(int W) {
+  static int groups(int W) {  // WarpGroups<W, ppl, NWARP>::NG
     const int ppl = (sizeof(R) == 4 && W * W > 32) ? 2 : 1;
-    return (W * W + 32 * ppl - 1) / (32 * ppl);
+    const int ng = (W * W + 32 * ppl - 1) / (32 * ppl);
+    return ng > NWARP / 2 ? NWARP : ng;
   }
   template <int W>
   static void run(bool spread, dim3 grid, size_t smem, cudaStream_t st, const GridArgs &a,

@@ -524,6 +524,48 @@ __device__ __forceinline__ void eval_const(const DevKernel<R> &k, R x, R *out) {
   }
 }
 
+// The per-record part of staging that is not kernel evaluation: the packed
+// in-tile origin (or kSkip when the record lies outside its chunk's tile),
+// the bounding box of origins, and the visibility to spread (gathered and
+// multiplied by the static factor for plan execution).  Returns false for a
+// skipped record.
+template <typename R, typename Rec>
+__device__ __forceinline__ bool stage_meta(const Rec &rr, int lane, int tu, int tv, int mp,
+                                           const DevGeom &g, R *vv, uint32_t *luv, int *err,
+                                           int &bb0, int &bb1, int &bb2, int &bb3,
+                                           const void *vis_in, int vis_in_double) {
+  const int lu = int(rr.iuv >> 16) - tu * g.T;
+  const int lv = int(rr.iuv & 0xffffu) - tv * g.T;
+  if (lu < 0 || lu >= g.T || lv < 0 || lv >= g.T || int(rr.mp) != mp) {
+    atomicOr(err, 1);
+    luv[lane] = kSkip;
+    return false;
+  }
+  luv[lane] = (uint32_t(lu) << 16) | uint32_t(lv);
+  bb0 = min(bb0, lu); bb1 = max(bb1, lu);
+  bb2 = min(bb2, lv); bb3 = max(bb3, lv);
+  R vr = rr.vr, vi = rr.vi;
+  if (vis_in) {
+    const uint32_t id = rr.idx & 0x7fffffffu;
+    R xr, xi;
+    if (vis_in_double) {
+      const double2 x = reinterpret_cast<const double2 *>(vis_in)[id];
+      xr = R(x.x);
+      xi = R(x.y);
+    } else {
+      const float2 x = reinterpret_cast<const float2 *>(vis_in)[id];
+      xr = R(x.x);
+      xi = R(x.y);
+    }
+    vr = xr * rr.vr + xi * rr.vi;
+    vi = xi * rr.vr - xr * rr.vi;
+    if (rr.idx & 0x80000000u) vi = -vi;
+  }
+  vv[2 * lane] = vr;
+  vv[2 * lane + 1] = vi;
+  return true;
+}
+
 // Stages records [b0, b0+nb) of the warp's slice; returns via luv the packed
 // in-tile origin (or kSkip).  Lanes >= nb do nothing.
 template <typename R, int W, typename Rec>
@@ -535,15 +577,8 @@ __device__ __forceinline__ void stage_batch(const Rec *recs, int b0, int nb, int
   constexpr int KST = KStride<R, W>::value;
   if (lane < nb) {
     const Rec rr = recs[b0 + lane];
-    const int lu = int(rr.iuv >> 16) - tu * g.T;
-    const int lv = int(rr.iuv & 0xffffu) - tv * g.T;
-    if (lu < 0 || lu >= g.T || lv < 0 || lv >= g.T || int(rr.mp) != mp) {
-      atomicOr(err, 1);
-      luv[lane] = kSkip;
-    } else {
-      luv[lane] = (uint32_t(lu) << 16) | uint32_t(lv);
-      bb0 = min(bb0, lu); bb1 = max(bb1, lu);
-      bb2 = min(bb2, lv); bb3 = max(bb3, lv);
+    if (stage_meta<R>(rr, lane, tu, tv, mp, g, vv, luv, err, bb0, bb1, bb2, bb3, vis_in,
+                      vis_in_double)) {
       R vals[W];
       R *row = kv + lane * KST;
       eval_const<W>(kc, rr.xu, vals);
@@ -560,28 +595,60 @@ __device__ __forceinline__ void stage_batch(const Rec *recs, int b0, int nb, int
 #pragma unroll
         for (int i = 0; i < W; ++i) row[2 * W + i] = R(i == 0);
       }
-      R vr = rr.vr, vi = rr.vi;
-      if (vis_in) {
-        const uint32_t id = rr.idx & 0x7fffffffu;
-        R xr, xi;
-        if (vis_in_double) {
-          const double2 x = reinterpret_cast<const double2 *>(vis_in)[id];
-          xr = R(x.x);
-          xi = R(x.y);
-        } else {
-          const float2 x = reinterpret_cast<const float2 *>(vis_in)[id];
-          xr = R(x.x);
-          xi = R(x.y);
-        }
-        vr = xr * rr.vr + xi * rr.vi;
-        vi = xi * rr.vr - xr * rr.vi;
-        if (rr.idx & 0x80000000u) vi = -vi;
-      }
-      vv[2 * lane] = vr;
-      vv[2 * lane + 1] = vi;
     }
   }
 }
+
+// Staging shared by all NW warps of a CTA that works as one slice (large W
+// in FP64): lane l of warp w evaluates kernel values [w Q, (w + 1) Q) of the
+// 3W of record l (Q = ceil(3W / NW)), instead of every warp evaluating all of
+// them; warp 0 also does the rest of the staging.  The caller brackets it
+// with CTA barriers.
+template <typename R, int W, int NW, typename Rec>
+__device__ __forceinline__ void stage_batch_split(const Rec *recs, int b0, int nb, int lane, int w,
+                                                  int tu, int tv, int mp, const DevGeom &g,
+                                                  const DevKernel<R> &kc, R *kv, R *vv,
+                                                  uint32_t *luv, int *err, int &bb0, int &bb1,
+                                                  int &bb2, int &bb3, const void *vis_in,
+                                                  int vis_in_double) {
+  constexpr int KST = KStride<R, W>::value;
+  constexpr int Q = (3 * W + NW - 1) / NW;
+  constexpr int DEG = KDeg<W>::value;
+  if (lane < nb) {
+    const Rec rr = recs[b0 + lane];
+    if (w == 0)
+      stage_meta<R>(rr, lane, tu, tv, mp, g, vv, luv, err, bb0, bb1, bb2, bb3, vis_in,
+                    vis_in_double);
+    R *row = kv + lane * KST;
+#pragma unroll
+    for (int qi = 0; qi < Q; ++qi) {
+      const int v = w * Q + qi;  // the same for every lane of the warp
+      if (v < 3 * W) {
+        const int axis = v / W, piece = v - axis * W;
+        R val;
+        if (axis == 2 && !g.do_w) {
+          val = R(piece == 0);
+        } else {
+          const R x = axis == 0 ? rr.xu : (axis == 1 ? rr.xv : rr.xw);
+          val = kc.c[DEG][piece];
+#pragma unroll
+          for (int j = DEG - 1; j >= 0; --j) val = fma(val, x, kc.c[j][piece]);
+        }
+        row[v] = val;
+      }
+    }
+  }
+}
+
+// Warps sharing one record's footprint: when more than half the warps would,
+// all of them do, as one slice whose warps also share the record staging.
+template <int W, int PPL, int NWARP>
+struct WarpGroups {
+  static constexpr int NG0 = (W * W + 32 * PPL - 1) / (32 * PPL);
+  static constexpr int NG = NG0 > NWARP / 2 ? NWARP : NG0;
+  static constexpr int NSL = NWARP / NG;
+  static constexpr bool SPLIT = (NG == NWARP) && NG > 1;
+};
 
 // Warp sums of G complex values at once (G = 1, 2, 4 or 8), as a
 // reduce-scatter: at each of the first log2(G) butterfly stages a lane keeps
@@ -653,8 +720,9 @@ __global__ void __launch_bounds__(NWARP * 32, sizeof(R) == 4 ? 3 : 1)
 k_spread(GridArgs a, DevGeom g, DevKernel<R> kc) {
   using Rec = typename RecOf<R>::type;
   using C = typename Cplx<R>::type;
-  constexpr int NG = (W * W + 32 * PPL - 1) / (32 * PPL);  // warps per record
-  constexpr int NSL = NWARP / NG;                          // record slices
+  constexpr int NG = WarpGroups<W, PPL, NWARP>::NG;    // warps per record
+  constexpr int NSL = WarpGroups<W, PPL, NWARP>::NSL;  // record slices
+  constexpr bool SPLIT = WarpGroups<W, PPL, NWARP>::SPLIT;
   constexpr int KST = KStride<R, W>::value;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const TileLayout tl = a.tl;
@@ -666,7 +734,10 @@ k_spread(GridArgs a, DevGeom g, DevKernel<R> kc) {
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int grp = warp % NG, slice = warp / NG;
-  unsigned char *wbase = smem_raw + size_t(2 * W * tl.PS) * sizeof(R) + warp * WarpStage<R, W>::bytes;
+  // the warp's own staging area, and the one it reads records from (warp 0's
+  // when the CTA's warps share the staging)
+  unsigned char *wown = smem_raw + size_t(2 * W * tl.PS) * sizeof(R) + warp * WarpStage<R, W>::bytes;
+  unsigned char *wbase = SPLIT ? smem_raw + size_t(2 * W * tl.PS) * sizeof(R) : wown;
   R *kv = reinterpret_cast<R *>(wbase);
   R *vv = kv + 32 * KST;
   uint32_t *luvs = reinterpret_cast<uint32_t *>(vv + 64);
@@ -733,9 +804,17 @@ k_spread(GridArgs a, DevGeom g, DevKernel<R> kc) {
       };
       for (int b0 = j0; b0 < j1; b0 += 32) {
         const int nb = min(32, j1 - b0);
-        stage_batch<R, W>(recs, b0, nb, lane, tu, tv, mp, g, kc, kv, vv, luvs, a.err, bb0, bb1,
-                          bb2, bb3, a.vis_in, a.vis_in_double);
-        __syncwarp();
+        if constexpr (SPLIT) {
+          __syncthreads();  // every warp is done with the previous batch
+          stage_batch_split<R, W, NWARP>(recs, b0, nb, lane, warp, tu, tv, mp, g, kc, kv, vv,
+                                         luvs, a.err, bb0, bb1, bb2, bb3, a.vis_in,
+                                         a.vis_in_double);
+          __syncthreads();
+        } else {
+          stage_batch<R, W>(recs, b0, nb, lane, tu, tv, mp, g, kc, kv, vv, luvs, a.err, bb0, bb1,
+                            bb2, bb3, a.vis_in, a.vis_in_double);
+          __syncwarp();
+        }
         for (int jj = 0; jj < nb; ++jj) {
           const uint32_t luv = luvs[jj];
           if (luv == kSkip) continue;
@@ -868,8 +947,9 @@ __global__ void __launch_bounds__(NWARP * 32, sizeof(R) == 4 ? 3 : 1)
 k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
   using Rec = typename RecOf<R>::type;
   using C = typename Cplx<R>::type;
-  constexpr int NG = (W * W + 32 * PPL - 1) / (32 * PPL);
-  constexpr int NSL = NWARP / NG;
+  constexpr int NG = WarpGroups<W, PPL, NWARP>::NG;
+  constexpr int NSL = WarpGroups<W, PPL, NWARP>::NSL;
+  constexpr bool SPLIT = WarpGroups<W, PPL, NWARP>::SPLIT;
   constexpr int KST = KStride<R, W>::value;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const TileLayout tl = a.tl;
@@ -881,7 +961,10 @@ k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int grp = warp % NG, slice = warp / NG;
-  unsigned char *wbase = smem_raw + size_t(2 * W * tl.PS) * sizeof(R) + warp * WarpStage<R, W>::bytes;
+  // the warp's own staging area, and the one it reads records from (warp 0's
+  // when the CTA's warps share the staging)
+  unsigned char *wown = smem_raw + size_t(2 * W * tl.PS) * sizeof(R) + warp * WarpStage<R, W>::bytes;
+  unsigned char *wbase = SPLIT ? smem_raw + size_t(2 * W * tl.PS) * sizeof(R) : wown;
   R *kv = reinterpret_cast<R *>(wbase);
   R *vv = kv + 32 * KST;
   uint32_t *luvs = reinterpret_cast<uint32_t *>(vv + 64);
@@ -993,14 +1076,22 @@ k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
       int bb0 = 0, bb1 = 0, bb2 = 0, bb3 = 0;
       for (int b0 = j0; b0 < j1; b0 += 32) {
         const int nb = min(32, j1 - b0);
-        stage_batch<R, W>(recs, b0, nb, lane, tu, tv, mp, g, kc, kv, vv, luvs, a.err, bb0, bb1,
-                          bb2, bb3, a.vis_in, a.vis_in_double);
-        __syncwarp();
+        if constexpr (SPLIT) {
+          __syncthreads();  // every warp is done with the previous batch
+          stage_batch_split<R, W, NWARP>(recs, b0, nb, lane, warp, tu, tv, mp, g, kc, kv, vv,
+                                         luvs, a.err, bb0, bb1, bb2, bb3, a.vis_in,
+                                         a.vis_in_double);
+          __syncthreads();
+        } else {
+          stage_batch<R, W>(recs, b0, nb, lane, tu, tv, mp, g, kc, kv, vv, luvs, a.err, bb0, bb1,
+                            bb2, bb3, a.vis_in, a.vis_in_double);
+          __syncwarp();
+        }
         // record sums of the batch, G records at a time (reduce-scatter);
         // the staged visibility slots of the warp are free here and hold them
         constexpr int G = IG;
         constexpr int LG = G == 1 ? 0 : G == 2 ? 1 : G == 4 ? 2 : 3;
-        R *osum = vv;
+        R *osum = reinterpret_cast<R *>(wown) + 32 * KST;
         for (int g0 = 0; g0 < nb; g0 += G) {
           C part[G];
 #pragma unroll
