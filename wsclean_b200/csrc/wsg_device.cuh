@@ -162,15 +162,6 @@ __device__ __forceinline__ uint32_t bin_key(const DevGeom &g, const VisPix &p) {
   return (bin << (2 * g.lbits)) | q;
 }
 
-template <int W, typename R>
-__device__ __forceinline__ void eval_pieces(const DevKernel<R> &k, R x, R *out) {
-#pragma unroll
-  for (int i = 0; i < W; ++i) out[i] = k.c[k.D][i];
-  for (int j = k.D - 1; j >= 0; --j) {
-#pragma unroll
-    for (int i = 0; i < W; ++i) out[i] = fma(out[i], x, k.c[j][i]);
-  }
-}
 
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
@@ -452,12 +443,6 @@ __device__ __forceinline__ JobGeom load_job(const GridArgs &a, const DevGeom &g,
   return j;
 }
 
-__device__ __forceinline__ int band_index_j(const JobGeom &j, int u) {
-  if (j.band_full) return u;
-  if (u <= j.Lu) return u;
-  if (u >= j.nu - j.Lu) return u - (j.nu - j.band_rows);
-  return -1;
-}
 
 // The job geometry a tile flush or stage needs, copied out of shared memory
 // into registers: inside loops that also store to shared memory the compiler
@@ -486,12 +471,6 @@ struct JobRegs {
 
 constexpr uint32_t kSkip = 0xfffffffeu;  // record marker: outside its chunk's tile
 
-__device__ __forceinline__ int band_index(const DevGeom &g, int u) {
-  if (g.band_full) return u;
-  if (u <= g.Lu) return u;
-  if (u >= g.nu - g.Lu) return u - (g.nu - g.band_rows);
-  return -1;
-}
 
 // ------------------------------------------------- per-warp record staging
 //
