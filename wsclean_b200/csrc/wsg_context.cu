@@ -469,6 +469,15 @@ struct GridKernels {
   }
 };
 
+// Whether `extra` bytes of shared memory fit beside a CTA's `base` bytes
+// without lowering the CTAs an SM holds (228 KB a SM, 227 KB a CTA, 1 KB
+// reserved a CTA).
+bool twist_tables_fit(size_t base, size_t extra) {
+  constexpr size_t kSM = 228 * 1024, kCTA = 227 * 1024, kRes = 1024;
+  if (base + extra > kCTA) return false;
+  return kSM / (base + extra + kRes) == kSM / (base + kRes);
+}
+
 // Pruned u-transform kernels, dispatched over log2(M).
 template <typename R>
 struct ColKernels {
@@ -482,8 +491,16 @@ struct ColKernels {
       smem_attr(k_ucol_bwd<R, LOGM>, smem);
       k_ucol_bwd<R, LOGM><<<grid, Cfg::THREADS, smem, st>>>(a);
     } else {
-      smem_attr(k_ucol_fwd<R, LOGM>, smem);
-      k_ucol_fwd<R, LOGM><<<grid, Cfg::THREADS, smem, st>>>(a);
+      // the forward kernel keeps its twist tables in shared memory when they
+      // fit without costing a resident CTA
+      const size_t extra = size_t(a.K) * (M / 16 + 32) * 2 * sizeof(R);
+      if (twist_tables_fit(smem, extra)) {
+        smem_attr(k_ucol_fwd<R, LOGM, true>, smem + extra);
+        k_ucol_fwd<R, LOGM, true><<<grid, Cfg::THREADS, smem + extra, st>>>(a);
+      } else {
+        smem_attr(k_ucol_fwd<R, LOGM, false>, smem);
+        k_ucol_fwd<R, LOGM, false><<<grid, Cfg::THREADS, smem, st>>>(a);
+      }
     }
     cuda_check(cudaGetLastError(), bwd ? "k_ucol_bwd launch" : "k_ucol_fwd launch");
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);

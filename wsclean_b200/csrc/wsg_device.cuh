@@ -1532,8 +1532,10 @@ k_ucol_bwd(ColArgs a) {
 
 // dirty2ms direction, the exact transpose: H image rows -> band rows of the
 // image columns, forward (-) transform along u.  Band entries of other
-// columns are left untouched (zeroed by the caller).
-template <typename R, int LOGM>
+// columns are left untouched (zeroed by the caller).  TWS: the twist tables
+// are copied to shared memory after the stage twiddles (K (M/16 + 32) more
+// entries), where the host finds room for them without losing a resident CTA.
+template <typename R, int LOGM, bool TWS>
 __global__ void __launch_bounds__(ColCfg<R, (1 << LOGM)>::THREADS, ColCfg<R, (1 << LOGM)>::MINB)
 k_ucol_fwd(ColArgs a) {
   using C = typename Cplx<R>::type;
@@ -1551,21 +1553,30 @@ k_ucol_fwd(ColArgs a) {
   C *band = reinterpret_cast<C *>(a.band);
   const C *twB = reinterpret_cast<const C *>(a.twB);
   const C *twQ = reinterpret_cast<const C *>(a.twQ);
+  if constexpr (TWS) {  // ordered before use by the first transform's barriers
+    C *twBs = tws + M, *twQs = twBs + a.K * TPF;
+    for (int i = threadIdx.x; i < a.K * TPF; i += blockDim.x) twBs[i] = twB[i];
+    for (int i = threadIdx.x; i < a.K * 32; i += blockDim.x) twQs[i] = twQ[i];
+    twB = twBs;
+    twQ = twQs;
+  }
   const C *rowp = reinterpret_cast<const C *>(a.H) + (size_t(lp) * a.ny + (jv ? j : 0)) * a.nx;
   fill_table<C, M, ColCfg<R, M>::THREADS>(tws, reinterpret_cast<const C *>(a.twM));
-  const int half_nu = a.nu / 2, half_nx = a.nx / 2;
+  const int half_nx = a.nx / 2;
   C acc[16];
 #pragma unroll
   for (int q = 0; q < 16; ++q) acc[q].x = acc[q].y = R(0);
   for (int k2 = 0; k2 < a.K; ++k2) {
     C v[16];
+    // output row k = K (t + TPF q) + k2 is image row k + nx/2 for q < 8 and
+    // k - nu + nx/2 for q >= 8 (nu = 16 K TPF: the wrap at nu/2 falls at q = 8)
+    const int ib = a.K * t + k2 + half_nx, istep = a.K * TPF;
 #pragma unroll
     for (int q = 0; q < 16; ++q) {
-      const int k = a.K * (t + TPF * q) + k2;
-      const int i = (k < half_nu ? k : k - a.nu) + half_nx;
+      const int i = ib + istep * (q < 8 ? q : q - 16);
       v[q].x = R(0);
       v[q].y = R(0);
-      if (jv && i >= 0 && i < a.nx) v[q] = rowp[i];
+      if (jv && unsigned(i) < unsigned(a.nx)) v[q] = rowp[i];
     }
     C *S = (kFlip && (k2 & 1)) ? B : A;
     C *O = (kFlip && (k2 & 1)) ? A : B;
@@ -1579,10 +1590,17 @@ k_ucol_fwd(ColArgs a) {
         acc[q].y += o[q].y;
       }
     } else {
-      const C base = __ldg(&twB[k2 * TPF + t]);
+      const C base = TWS ? twB[k2 * TPF + t] : __ldg(&twB[k2 * TPF + t]);
 #pragma unroll
       for (int q = 0; q < 16; ++q) {
-        C w = col_twist<C, TPF>(a, twB, twQ, k2, t, q, M, base);
+        C w;
+        if constexpr (TWS) {
+          const int b = t + TPF * q;
+          const int neg = (!a.band_full && b >= M - a.L) ? 1 : 0;
+          w = cmul(twQ[(k2 * 16 + q) * 2 + neg], base);
+        } else {
+          w = col_twist<C, TPF>(a, twB, twQ, k2, t, q, M, base);
+        }
         w.y = -w.y;
         const C val = cmul(o[q], w);
         acc[q].x += val.x;
@@ -1791,27 +1809,39 @@ __global__ void __launch_bounds__(256) k_screen_add(ScreenArgs s, const void *Hv
   const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
   const int i = i0 + tx;
+  // planes loaded together; the first batch is in flight while the pixel's
+  // FP64 terms are computed
+  constexpr int PB = sizeof(R) == 4 ? 16 : 8;
   for (int k = 0; k < 4; ++k) {
     const int j = j0 + ty + 8 * k;
     double val = 0;
     if (i < s.nx && j < s.ny) {
+      const C *hp = H + size_t(j) * s.nx + i;
+      const size_t pstride = size_t(s.ny) * s.nx;
+      C hb[PB];
+#pragma unroll
+      for (int u = 0; u < PB; ++u)
+        if (u < s.npl) hb[u] = hp[u * pstride];
       double corr, q;
       bool inside;
       pixel_terms(s, i, j, corr, q, inside);
-      double acc = 0;
-      const C *hp = H + size_t(j) * s.nx + i;
-      const size_t pstride = size_t(s.ny) * s.nx;
-      if (s.do_w && inside) {
+      const bool screen = s.do_w && inside;
+      double2 sc = make_double2(1.0, 0.0), st = make_double2(1.0, 0.0);
+      if (screen) {
         const double w0 = s.wmin + s.pb0 * s.dw;
-        double2 sc = cexp_turns(-w0 * q);
-        const double2 st = cexp_turns(-s.dw * q);
-        for (int p0 = 0; p0 < s.npl; p0 += 8) {
-          C hb[8];
+        sc = cexp_turns(-w0 * q);
+        st = cexp_turns(-s.dw * q);
+      }
+      double acc = 0;
+      for (int p0 = 0; p0 < s.npl; p0 += PB) {
+        if (p0 > 0) {
 #pragma unroll
-          for (int u = 0; u < 8; ++u)
+          for (int u = 0; u < PB; ++u)
             if (p0 + u < s.npl) hb[u] = hp[(p0 + u) * pstride];
+        }
+        if (screen) {
 #pragma unroll
-          for (int u = 0; u < 8; ++u) {
+          for (int u = 0; u < PB; ++u) {
             if (p0 + u < s.npl) {
               acc += double(hb[u].x) * sc.x - double(hb[u].y) * sc.y;
               const double nr = sc.x * st.x - sc.y * st.y;
@@ -1819,9 +1849,11 @@ __global__ void __launch_bounds__(256) k_screen_add(ScreenArgs s, const void *Hv
               sc.x = nr;
             }
           }
+        } else {
+#pragma unroll
+          for (int u = 0; u < PB; ++u)
+            if (p0 + u < s.npl) acc += double(hb[u].x);
         }
-      } else {
-        for (int p = 0; p < s.npl; ++p) acc += double(hp[p * pstride].x);
       }
       val = acc * corr;
     }
