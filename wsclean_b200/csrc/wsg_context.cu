@@ -133,7 +133,12 @@ Context::Context(int dev) {
   stream = own_stream;
   CK(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
   for (auto &e : ev) CK(cudaEventCreate(&e));
-  CK(cudaStreamCreateWithFlags(&cpy, cudaStreamNonBlocking));
+  // the copy stream also runs a staged call's scan, which the host waits
+  // for before it can plan and return; at the highest priority its blocks
+  // are scheduled ahead of the previous call's kernels on the main stream
+  int prio_lo = 0, prio_hi = 0;
+  CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+  CK(cudaStreamCreateWithPriority(&cpy, cudaStreamNonBlocking, prio_hi));
   CK(cudaStreamCreateWithFlags(&d2h, cudaStreamNonBlocking));
   for (cudaEvent_t *e : {&ev_start, &ev_in, &ev_done, &ev_scan})
     CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
@@ -181,7 +186,14 @@ Context::~Context() {
 std::vector<DevBuf *> Context::all_buffers() {
   return {&b_uvw, &b_fovc, &b_vis, &b_wgt, &b_mask, &b_keys_a, &b_keys_b, &b_vals_a,
           &b_vals_b, &b_cub, &b_rec, &b_chunks, &b_small, &b_band, &b_bandf, &b_bandd, &b_H,
-          &b_img, &b_img2, &b_acc, &b_cf, &b_tw, &b_fftwork, &b_out};
+          &b_img, &b_img2, &b_acc, &b_fftwork, &b_out, &corr_cache[0].buf, &corr_cache[1].buf,
+          &tw_cache[0].buf, &tw_cache[1].buf};
+}
+
+void Context::invalidate_tables() {
+  for (auto &e : corr_cache) e.valid = false;
+  for (auto &e : tw_cache) e.valid = false;
+  cf_cur = nullptr;
 }
 
 void Context::synchronize() {
@@ -206,8 +218,7 @@ void Context::release_buffers() {
   for (auto *b : all_buffers()) b->release();
   band_dirty = BandDirty{};
   bandd_zero = BandDirty{};
-  corr_valid = false;
-  tw_valid = false;
+  invalidate_tables();
 }
 
 size_t Context::device_bytes() {
@@ -806,7 +817,8 @@ ColArgs make_col(const GridPlan &g, size_t P, const void *tw, void *band, void *
 
 // Grid-correction tables for the chosen kernel: 1/Phi as a Chebyshev series
 // in v^2 (evaluated per pixel on the device for the w term) and the 1-D u/v
-// correction arrays; cached per geometry, uploaded to b_cf.
+// correction arrays; cached per geometry (two entries), the chosen entry's
+// device copy left in cf_cur.
 ChebCorr Context::upload_corrections(const GridPlan &g) {
   double vmax = 0.5 * std::max(double(g.nx) / g.nu, double(g.ny) / g.nv) * 1.0000001;
   if (g.do_w) {
@@ -822,19 +834,27 @@ ChebCorr Context::upload_corrections(const GridPlan &g) {
     vmax = std::min(vmax, 1.0);
   }
   auto key = std::make_tuple(g.kernel.W, g.kernel.beta, g.kernel.e0, g.nx, g.ny, g.nu, g.nv, vmax);
-  if (corr_valid && key == corr_key) return corr_cc;
+  for (auto &e : corr_cache)
+    if (e.valid && e.key == key) {
+      e.used = ++cache_tick;
+      cf_cur = reinterpret_cast<const double *>(e.buf.p);
+      return e.cc;
+    }
+  CorrEntry &e = corr_cache[0].used <= corr_cache[1].used ? corr_cache[0] : corr_cache[1];
   KernelTransform tr(g.kernel);
   ChebCorr cc = fit_cheb_corr(tr, vmax);
   std::vector<double> cf(g.nx / 2 + 1 + g.ny / 2 + 1);
   for (size_t i = 0; i <= g.nx / 2; ++i) cf[i] = cc(double(i) / g.nu);
   for (size_t i = 0; i <= g.ny / 2; ++i) cf[g.nx / 2 + 1 + i] = cc(double(i) / g.nv);
-  double *d = reinterpret_cast<double *>(b_cf.ensure(cf.size() * sizeof(double)));
-  // stream-ordered: kernels of earlier (pipelined) calls may still read b_cf
+  double *d = reinterpret_cast<double *>(e.buf.ensure(cf.size() * sizeof(double)));
+  // stream-ordered: kernels of earlier (pipelined) calls may still read it
   CK(cudaMemcpyAsync(d, cf.data(), cf.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
   cheb_err = cc.max_rel_err;
-  corr_key = key;
-  corr_cc = cc;
-  corr_valid = true;
+  e.key = key;
+  e.cc = cc;
+  e.valid = true;
+  e.used = ++cache_tick;
+  cf_cur = d;
   return cc;
 }
 
@@ -882,9 +902,15 @@ const void *Context::upload_twiddles(const GridPlan &g, bool dbl) {
   const size_t M = size_t(1) << g.logM;
   auto key = std::make_tuple(M, g.nu, int(dbl));
   const size_t cs = dbl ? 16 : 8;
-  if (!(tw_valid && key == tw_key)) {
+  for (auto &e : tw_cache)
+    if (e.valid && e.key == key) {
+      e.used = ++cache_tick;
+      return e.buf.p;
+    }
+  TwEntry &e = tw_cache[0].used <= tw_cache[1].used ? tw_cache[0] : tw_cache[1];
+  {
     const std::vector<double> h = col_twiddle_table(M, g.nu, size_t(g.K));
-    void *d = b_tw.ensure(h.size() / 2 * cs);
+    void *d = e.buf.ensure(h.size() / 2 * cs);
     // stream-ordered (pageable sources are staged before the call returns)
     if (dbl) {
       CK(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
@@ -892,10 +918,11 @@ const void *Context::upload_twiddles(const GridPlan &g, bool dbl) {
       std::vector<float> hf(h.begin(), h.end());
       CK(cudaMemcpyAsync(d, hf.data(), hf.size() * sizeof(float), cudaMemcpyHostToDevice, stream));
     }
-    tw_key = key;
-    tw_valid = true;
+    e.key = key;
+    e.valid = true;
+    e.used = ++cache_tick;
   }
-  return b_tw.p;
+  return e.buf.p;
 }
 
 // Planes resident per pass: as many as fit in 55% of the device memory and
@@ -1025,7 +1052,7 @@ bool Context::grid_core(const wsg_args &a, const Staged &s, double *img, bool ac
     // pruned transform along u: band rows of the image columns -> image rows
     ColKernels<R>::run(gp.logM, true, ca, int(npl), stream);
     CK(cudaEventRecord(ev[4], stream));
-    ScreenArgs sa = make_screen(gp, reinterpret_cast<const double *>(b_cf.p), cc, P);
+    ScreenArgs sa = make_screen(gp, cf_cur, cc, P);
     sa.pb0 = int(pb0);
     sa.npl = int(npl);
     dim3 sg((gp.nx + 31) / 32, (gp.ny + 31) / 32);
@@ -1132,7 +1159,7 @@ void Context::degrid_core(const wsg_args &a, const Staged &s, const double *img,
   for (size_t pb0 = 0; pb0 < gp.nplanes; pb0 += P) {
     const size_t npl = std::min(P, gp.nplanes - pb0);
     CK(cudaEventRecord(ev[2], stream));
-    ScreenArgs sa = make_screen(gp, reinterpret_cast<const double *>(b_cf.p), cc, P);
+    ScreenArgs sa = make_screen(gp, cf_cur, cc, P);
     sa.pb0 = int(pb0);
     sa.npl = int(npl);
     dim3 sg((gp.nx + 31) / 32, (gp.ny + 31) / 32);
@@ -1577,18 +1604,18 @@ void Plan::build(const std::vector<wsg_job> &js) {
     nchunks_ += nch_j;
     // corrections and twiddles of this grid
     pj.cc = cx_.upload_corrections(gp);
-    cx_.upload_twiddles(gp, sizeof(R) == 8);
+    const void *twd = cx_.upload_twiddles(gp, sizeof(R) == 8);
     CK(cudaStreamSynchronize(st));  // the uploads are stream-ordered
     const size_t ncf = gp.nx / 2 + 1 + gp.ny / 2 + 1;
     pj.cf_off = cf_host.size();
     cf_host.resize(cf_host.size() + ncf);
-    CK(cudaMemcpy(cf_host.data() + pj.cf_off, cx_.b_cf.p, ncf * sizeof(double),
+    CK(cudaMemcpy(cf_host.data() + pj.cf_off, cx_.cf_cur, ncf * sizeof(double),
                   cudaMemcpyDeviceToHost));
     const size_t M = size_t(1) << gp.logM;
     const size_t ntw = (M + size_t(gp.K) * (M / 16) + 32 * size_t(gp.K)) * cs;
     pj.tw_off = tw_host.size();
     tw_host.resize(align256(tw_host.size() + ntw));
-    CK(cudaMemcpy(tw_host.data() + pj.tw_off, cx_.b_tw.p, ntw, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(tw_host.data() + pj.tw_off, twd, ntw, cudaMemcpyDeviceToHost));
     // the job's band grid with all its planes, and its v-FFT plan
     pj.band_bytes = gp.band_rows * gp.nplanes * gp.nv * cs;
     pj.band_off = band_total_;
@@ -1972,15 +1999,15 @@ StreamGridder::StreamGridder(Context &cx, const wsg_args &a, double wmin, double
   band_.ensure(g.band_rows * g.nplanes * g.nv * cs);
   img_.ensure(g.nx * g.ny * sizeof(double));
   cc_ = cx_.upload_corrections(g);
-  cx_.upload_twiddles(g, dbl_);
+  const void *twd = cx_.upload_twiddles(g, dbl_);
   CK(cudaStreamSynchronize(cx_.stream));  // the uploads are stream-ordered
   const size_t ncf = g.nx / 2 + 1 + g.ny / 2 + 1;
   cf_.ensure(ncf * sizeof(double));
-  CK(cudaMemcpy(cf_.p, cx_.b_cf.p, ncf * sizeof(double), cudaMemcpyDeviceToDevice));
+  CK(cudaMemcpy(cf_.p, cx_.cf_cur, ncf * sizeof(double), cudaMemcpyDeviceToDevice));
   const size_t M = size_t(1) << g.logM;
   const size_t ntw = (M + size_t(g.K) * (M / 16) + 32 * size_t(g.K)) * cs;
   tw_.ensure(ntw);
-  CK(cudaMemcpy(tw_.p, cx_.b_tw.p, ntw, cudaMemcpyDeviceToDevice));
+  CK(cudaMemcpy(tw_.p, twd, ntw, cudaMemcpyDeviceToDevice));
   CF(cufftCreate(&fft_));
   CF(cufftSetAutoAllocation(fft_, 0));
   int n = int(g.nv), inembed = n, onembed = n;

@@ -137,7 +137,7 @@ class Context {
   // be zero (Lv holds ny; p == nullptr: unknown)
   BandDirty bandd_zero;
   void clear_band(void *band, size_t rows, size_t nv, size_t cs);
-  DevBuf b_img, b_img2, b_acc, b_cf, b_tw, b_fftwork, b_out;
+  DevBuf b_img, b_img2, b_acc, b_fftwork, b_out;
 
  private:
   friend class Plan;
@@ -164,8 +164,6 @@ class Context {
   cudaEvent_t ev[8];
   std::map<std::tuple<int, int, int, int, int, int, int>, cufftHandle> fft_plans;
   size_t fft_work_need = 0;
-  std::tuple<size_t, size_t, int> tw_key;
-  bool tw_valid = false;
   // last plane-batch choice (choose_planes)
   struct PlanesMemo {
     std::tuple<size_t, size_t, int> key;
@@ -183,10 +181,29 @@ class Context {
   // device geometry (DevGeom bytes) of the last planned grid: the next scan
   // writes sort keys for it, used when the next plan comes out the same
   std::vector<unsigned char> spec_geom;
-  // correction-table cache
-  std::tuple<int, double, double, size_t, size_t, size_t, size_t, double> corr_key;
-  ChebCorr corr_cc;
-  bool corr_valid = false;
+  // correction and column-twiddle tables, two of each cached on the device
+  // (ms2dirty and dirty2ms plan their grids apart, so alternating calls
+  // would otherwise upload both every call -- from pageable memory, which
+  // holds the host until the main stream has drained); the least recently
+  // used entry is replaced
+  struct CorrEntry {
+    std::tuple<int, double, double, size_t, size_t, size_t, size_t, double> key;
+    ChebCorr cc;
+    DevBuf buf;
+    uint64_t used = 0;
+    bool valid = false;
+  };
+  struct TwEntry {
+    std::tuple<size_t, size_t, int> key;
+    DevBuf buf;
+    uint64_t used = 0;
+    bool valid = false;
+  };
+  CorrEntry corr_cache[2];
+  TwEntry tw_cache[2];
+  uint64_t cache_tick = 0;
+  const double *cf_cur = nullptr;  // the tables the last upload_corrections chose
+  void invalidate_tables();
 };
 
 // One job of a plan (see wsg_plan_create).
