@@ -110,6 +110,10 @@ class Context {
   cudaStream_t scan_st = nullptr;
   DevBuf *fovc_buf = nullptr;
   bool err_pending = false;  // a device-side consistency check not yet read
+  // the scan's statistics come back through mapped pinned memory written by
+  // a kernel: a copy-engine read-back would queue behind the previous call's
+  // device-to-host copy of its output
+  void *h_scan = nullptr, *h_scan_dev = nullptr;  // ScanOut
   void finish_call(const wsg_args &a, Slot &sl, cudaStream_t last);
 
   int device = 0;

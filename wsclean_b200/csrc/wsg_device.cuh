@@ -56,6 +56,14 @@ struct ScanOut {
   unsigned long long nvis;
 };
 
+// Copies the scan's statistics into mapped pinned host memory (one warp).
+__global__ void k_scan_readback(const ScanOut *src, ScanOut *dst_host) {
+  constexpr int N = sizeof(ScanOut) / sizeof(unsigned long long);
+  const auto *s = reinterpret_cast<const unsigned long long *>(src);
+  auto *d = reinterpret_cast<volatile unsigned long long *>(dst_host);
+  if (threadIdx.x < N) d[threadIdx.x] = s[threadIdx.x];
+}
+
 // Visibility record, mixed precision (32 bytes, two 128-bit loads).
 struct __align__(16) RecF {
   float xu, xv, xw;   // local kernel coordinates in (-1, 1]
