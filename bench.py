@@ -79,6 +79,7 @@ def launch_summary(path, steps):
     the DRAM bytes read and written, with the total per step."""
     import collections
     import csv
+    import re
     rows = list(csv.reader(open(path)))
     hi = next(i for i, r in enumerate(rows) if "Kernel Name" in r)
     h = rows[hi]
@@ -94,7 +95,9 @@ def launch_summary(path, steps):
         ent = launches.setdefault(r[ii], (r[ki], {}))
         ent[1][r[mi]] = float(r[vi].replace(",", "")) * scale.get(r[ui], 1.0)
     launches = list(launches.values())
-    starts = [i for i, (k, _) in enumerate(launches) if "k_scan" in k]
+    # each call starts with its visibility scan (k_scan or k_scan_keys; not
+    # the read-back of the scan's statistics)
+    starts = [i for i, (k, _) in enumerate(launches) if re.search(r"\bk_scan(_keys)?[<(]", k)]
     seg = launches[starts[-2 * steps]:] if len(starts) >= 2 * steps else launches
     tot = collections.OrderedDict()
     for k, m in seg:
