@@ -183,6 +183,7 @@ Context::~Context() {
   for (auto &sl : slots)
     for (DevBuf *b : {&sl.uvw, &sl.vis, &sl.wgt, &sl.mask, &sl.out, &sl.fovc}) b->release();
   if (h_scan) cudaFreeHost(h_scan);
+  if (h_small) cudaFreeHost(h_small);
   if (own_stream) cudaStreamDestroy(own_stream);
 }
 
@@ -631,7 +632,18 @@ bool Context::prepare(const wsg_args &a, const Staged &s, bool gridding, void *v
   cudaStream_t sst = scan_st ? scan_st : stream;
   DevBuf &fbuf = fovc_buf ? *fovc_buf : b_fovc;
   double *d_fovc = reinterpret_cast<double *>(fbuf.ensure(a.nchan * sizeof(double)));
-  CK(cudaMemcpyAsync(d_fovc, fovc.data(), a.nchan * sizeof(double), cudaMemcpyHostToDevice, sst));
+  const size_t small_bytes = sizeof(ScanOut) + a.nchan * sizeof(double);
+  if (h_small_cap < small_bytes) {
+    if (h_small) CK(cudaFreeHost(h_small));
+    h_small = nullptr;
+    h_small_cap = 0;
+    CK(cudaHostAlloc(&h_small, small_bytes, cudaHostAllocDefault));
+    h_small_cap = small_bytes;
+  }
+  unsigned char *hsm = reinterpret_cast<unsigned char *>(h_small);
+  std::memcpy(hsm + sizeof(ScanOut), fovc.data(), a.nchan * sizeof(double));
+  CK(cudaMemcpyAsync(d_fovc, hsm + sizeof(ScanOut), a.nchan * sizeof(double),
+                     cudaMemcpyHostToDevice, sst));
   Staged st = s;
   st.fovc = d_fovc;
 
@@ -639,7 +651,8 @@ bool Context::prepare(const wsg_args &a, const Staged &s, bool gridding, void *v
   ScanOut h0{};
   h0.wmin_bits = 0x7ff0000000000000ull;
   ScanOut *d_scan = reinterpret_cast<ScanOut *>(b_small.ensure(4096));
-  CK(cudaMemcpyAsync(d_scan, &h0, sizeof(h0), cudaMemcpyHostToDevice, sst));
+  std::memcpy(hsm, &h0, sizeof h0);
+  CK(cudaMemcpyAsync(d_scan, hsm, sizeof(h0), cudaMemcpyHostToDevice, sst));
   // (off the main stream the caller zeroes the whole output itself)
   void *zero_out = scan_st ? nullptr : vis_out_dev;
   // the sort keys of the expected grid come out of the same pass: the fixed

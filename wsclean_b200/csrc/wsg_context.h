@@ -114,6 +114,11 @@ class Context {
   // a kernel: a copy-engine read-back would queue behind the previous call's
   // device-to-host copy of its output
   void *h_scan = nullptr, *h_scan_dev = nullptr;  // ScanOut
+  // pinned staging of the scan's small uploads (f/c, initial statistics): a
+  // pageable copy can wait behind a download in flight; reused once the
+  // previous call's scan stream was synchronized
+  void *h_small = nullptr;
+  size_t h_small_cap = 0;
   void finish_call(const wsg_args &a, Slot &sl, cudaStream_t last);
 
   int device = 0;
