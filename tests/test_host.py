@@ -131,3 +131,29 @@ def test_cpp_adapter_compiles(tmp_path):
     subprocess.run(["g++", "-std=c++17", "-c", "-I", host, "-I", os.path.join(ROOT, "include"),
                     os.path.join(host, "wgriddinggridder_b200.cpp"), "-o",
                     str(tmp_path / "adapter.o")], check=True)
+
+
+def test_launch_summary_takes_the_last_step(tmp_path, capsys):
+    """bench.py's launch summary of an ncu launch list: a step is two gridder
+    calls, each starting with its visibility scan (k_scan or k_scan_keys);
+    the scan's one-warp read-back kernel starts nothing."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    call = ["wsg::k_scan_keys<float2, float>(a)", "wsg::k_scan_readback(a)",
+            "wsg::k_records<float, float2, float>(a)", "wsg::k_spread<float, 8, 2, 8>(a)"]
+    names = ["wsg::k_scan<float2, float>(a)", "wsg::k_scan_readback(a)"] + call[2:] + call + call + call
+    lines = ['"ID","Kernel Name","Metric Name","Metric Unit","Metric Value"']
+    for i, n in enumerate(names):
+        us = 100.0 if "spread" in n else 10.0
+        lines.append(f'"{i}","void {n}","gpu__time_duration.sum","usecond","{us}"')
+    path = tmp_path / "launches.csv"
+    path.write_text("==PROF== banner line\n" + "\n".join(lines) + "\n")
+    bench.launch_summary(str(path), 1)
+    out = capsys.readouterr().out
+    # the last step: two calls of four launches
+    assert "over 8 launches in 1 step(s)" in out, out
+    row = next(l for l in out.splitlines() if l.startswith("wsg::k_scan_readback"))
+    assert row.split()[1] == "2"
+    assert "total 0.260 ms" in out
