@@ -1,6 +1,6 @@
 """Pipelined raw operators (wsg_ctx_set_async): a sequence of ms2dirty /
 dirty2ms calls on page-locked host buffers and on device tensors returns
-before the work is done, overlaps transfers with kernels through the two
+before the work is done, overlaps transfers with kernels through the three
 staging slots, and after synchronize() gives the synchronous results (to
 FP32 rounding: atomics reorder sums)."""
 import numpy as np
