@@ -123,25 +123,55 @@ int wsg_ms2dirty(wsg_ctx *ctx, const wsg_args *a, const void *vis, void *dirty,
 /* Replaces ducc0::dirty2ms (wgridder.h:1712-1729), the exact adjoint. */
 int wsg_dirty2ms(wsg_ctx *ctx, const wsg_args *a, const void *dirty, void *vis);
 
+/* Replace ducc0::ms2dirty_tuning / dirty2ms_tuning (wgridder.h:1781-1877),
+ * the calls behind WSClean's -gridder tuned-wgridder
+ * (wgriddinggridder_simple.cpp:59-63, :109-113): the same operators, with
+ * the work subdivided when the |w| statistics of the masked-in visibilities
+ * say it pays -- facets (each a smaller image with its own phase centre, so
+ * fewer w planes) for the visibilities at or above a |w| cut, the whole
+ * image for those below it.  The subdivision follows the reference's rule
+ * (get_tuning_parameters, wgridder.cc:144-278) and the results equal
+ * wsg_ms2dirty / wsg_dirty2ms within epsilon.  Odd image sizes are accepted,
+ * as the reference's tuned calls accept them (wgridder.h:1789-1801,
+ * :1829-1838).  The calls synchronise with the host between parts. */
+int wsg_ms2dirty_tuning(wsg_ctx *ctx, const wsg_args *a, const void *vis, void *dirty,
+                        int accumulate);
+int wsg_dirty2ms_tuning(wsg_ctx *ctx, const wsg_args *a, const void *dirty, void *vis);
+/* The subdivision of the last tuned call on ctx: nfx x nfy facets (0 x 0: the
+ * plain operator), their visibilities from |w| bin icut of 50 on, i.e. from
+ * |w| = wcut wavelengths (-1 without subdivision; icut 0: every visibility is
+ * faceted).  Extension of the reference interface (its verbosity report). */
+int wsg_get_tuning(const wsg_ctx *ctx, int *nfx, int *nfy, int *icut, double *wcut);
+/* Host-only: the subdivision the tuned calls choose for these arguments and
+ * |w| statistics -- hist[50]: counts of the masked-in visibilities in 50 equal
+ * |w| bins over [wmin, wmax] wavelengths, nvis_all = nrows x nchan. */
+int wsg_tuning_choice(const wsg_args *a, size_t nvis_all, double wmin, double wmax,
+                      const uint64_t *hist, int *nfx, int *nfy, int *icut);
+
 /* Allocation-free variant of wsg_ms2dirty, for callers that cannot allocate
- * device memory while they grid -- for example code recording a CUDA graph,
- * where cudaMalloc is not allowed, or a process whose device memory is owned
- * by another framework's pool.  It calls no cudaMalloc, cudaFree or
- * allocating library routine (no cuFFT plans; its own FFT kernels instead):
- * all scratch comes from one static device array of 96 MiB that every GPU
- * loading the library holds until the process exits.  This entry point has no
- * counterpart in the reference.
+ * device memory while they grid: a plugin inside a host application that
+ * reserved the whole device for its own memory pool at start-up (where a
+ * cudaMalloc fails, or takes memory the host has promised elsewhere), or a
+ * service that must run within a device-memory budget fixed when it started.
+ * It calls no cudaMalloc, cudaFree or allocating library routine (no cuFFT
+ * plans; its own FFT kernels instead): all scratch comes from one static
+ * device array of 96 MiB that every GPU loading the library holds until the
+ * process exits.  This entry point has no counterpart in the reference.
  *
  * Limits: mixed precision only; uvw, freq, vis, dirty (and wgt/mask when
  * given) must be device memory; the whole problem's scratch (about 40 bytes
  * per visibility plus the FP64 image plus at least one w plane of the band
  * grid and of the transformed columns) must fit in the 96 MiB, otherwise
- * WSG_ERR_INVALID with a message.  nv is a power of two here, so the grid
- * can differ from wsg_ms2dirty's; results agree within epsilon.
- * The first call on a device looks up the array's device address and should
- * come before any stream capture.  All calls share the array: calls that
- * overlap on the GPU race and must be serialised by the caller.  stream may
- * be NULL (the legacy default stream).  The image is overwritten. */
+ * WSG_ERR_INVALID with a message; nv is a power of two of at most 8192 (an
+ * image whose kernels all need a longer grid is rejected), so the grid can
+ * differ from wsg_ms2dirty's; results agree within epsilon.
+ * The first call in a CUDA context (once per device, again after a device
+ * reset) looks up the array's device address and should come before any
+ * stream capture.  The call synchronises its stream: it reads the visibility
+ * scan's statistics back to the host to plan the grid.  All calls share the
+ * array: calls that overlap on the GPU race and must be serialised by the
+ * caller.  stream may be NULL (the legacy default stream).  The image is
+ * overwritten. */
 int wsg_ms2dirty_noalloc(const wsg_args *a, const void *vis, void *dirty, void *stream);
 
 /* -------------------------------------- WGriddingGridder_Simple replacement */
@@ -154,7 +184,7 @@ typedef struct {
   size_t nthreads;            /* accepted for interface parity; unused */
   double epsilon;
   size_t verbosity;           /* 0..2 as in the reference */
-  int tuning;                 /* accepted; the GPU schedule is always used */
+  int tuning;                 /* nonzero: the tuned schedule (wsg_ms2dirty_tuning) */
   int precision;              /* WSG_PREC_MIXED (NumT=float) / WSG_PREC_FP64 (NumT=double) */
   int device;                 /* CUDA device, <0 = current */
 } wsg_gridder_params;

@@ -11,8 +11,7 @@ the timed CPU baseline.
   WSClean's argument pattern (wgridder/wgriddinggridder_simple.cpp:56-58).
 * ``dft_ms2dirty`` / ``dft_dirty2ms``: the FP64 direct Fourier transform
   (oracle/dft.c), WSClean's DirectMSGridder semantics in ducc0's convention.
-* ``wgridder_np``: a numpy restatement of the w-gridding algorithm for small
-  problems.
+* ``parse_report``: the grid parameters from ducc0's verbosity-1 report.
 """
 from __future__ import annotations
 

@@ -1,6 +1,11 @@
 """Parity on the geometries of the four other benchmark configurations (the
 headline bench runs config 2):
 
+* config 2 at full size (the headline workload): 8.1M visibilities, 4096^2
+  at 5", both directions in mixed precision (epsilon 1e-5) and in FP64
+  (epsilon 1e-12) against the reference w-gridder over the whole image and
+  all visibilities, against the FP64 DFT on 64 pixels and 10k visibilities,
+  and the adjoint (dot-product) test;
 * config 1 at full size: 2.9M complex128 visibilities, 1024^2 at 10",
   epsilon 1e-12, FP64 -- against the FP64 DFT and the reference w-gridder;
 * config 3 at full size: the chi^2 gradient at 2048^2 / 8" with Briggs
@@ -27,6 +32,76 @@ KW = dict(negate_v=True, divide_by_n=False, sigma_min=1.1, sigma_max=2.0)
 def G():
     from wsclean_b200 import gridder
     return gridder
+
+
+@pytest.fixture(scope="module")
+def config2_data():
+    from wsclean_b200 import synth
+    c = synth.config2()
+    uvw, freq, nx, px = c["uvw"], c["freq"], c["npix_x"], c["pixsize"]
+    rng = np.random.default_rng(22)
+    ix, iy, flux = synth.point_sky(c["nsrc"], nx, nx, rng)
+    vis = synth.predict_vis(uvw, freq, nx, nx, px, px, ix, iy, flux, device="cuda:0")
+    vis = vis + 0.1 * (rng.normal(size=vis.shape) + 1j * rng.normal(size=vis.shape))
+    model = synth.sky_image(nx, nx, ix, iy, flux)
+    return dict(uvw=uvw, freq=freq, nx=nx, px=px, vis=vis, model=model, rng=rng)
+
+
+# (precision, epsilon, tolerance vs the reference at the same epsilon,
+#  tolerance vs the DFT, adjoint tolerance)
+CONFIG2_FORMS = [("mixed", 1e-5, 2e-5, 1e-5, 1e-6), ("fp64", 1e-12, 1e-11, 1e-11, 1e-12)]
+
+
+@pytest.mark.parametrize("prec,eps,tol_ref,tol_dft,tol_adj", CONFIG2_FORMS)
+def test_config2_full(G, config2_data, prec, eps, tol_ref, tol_dft, tol_adj):
+    """The headline workload at full size, checked over the whole image and
+    every visibility against the reference w-gridder called as WSClean calls
+    it (wgriddinggridder_simple.cpp:56-58, :106-108), with the same epsilon
+    and the instance of the same width (<float,float> for the mixed form)."""
+    d2 = config2_data
+    uvw, freq, nx, px, model = d2["uvw"], d2["freq"], d2["nx"], d2["px"], d2["model"]
+    rng = np.random.default_rng(23)
+    dev = torch.device("cuda", 0)
+    cdt = np.complex64 if prec == "mixed" else np.complex128
+    fdt = np.float32 if prec == "mixed" else np.float64
+    vis = d2["vis"].astype(cdt)
+    tu, tf = torch.as_tensor(uvw, device=dev), torch.as_tensor(freq, device=dev)
+    tv = torch.as_tensor(vis, device=dev)
+    d = G.ms2dirty(tu, tf, tv, nx, nx, px, px, eps, precision=prec, dirty_dtype=np.float64,
+                   **KW).cpu().numpy()
+    pix = rng.integers(0, nx * nx, 64)
+    ref_pix = O.dft_ms2dirty(uvw, freq, vis, nx, nx, px, px, pixels=pix, negate_v=True,
+                             divide_by_n=False)
+    assert O.rel_rms(d.ravel()[pix], ref_pix) < tol_dft
+    tm = torch.as_tensor(model.astype(fdt), device=dev)
+    v = G.dirty2ms(tu, tf, tm, px, px, eps, precision=prec, vis_dtype=np.complex128,
+                   **KW).cpu().numpy()
+    sel = rng.choice(v.size, 10000, replace=False)
+    vref_sel = O.dft_dirty2ms(uvw, freq, model, px, px, negate_v=True, divide_by_n=False,
+                              select=sel)
+    assert O.rel_rms(v.ravel()[sel], vref_sel) < tol_dft
+    # adjointness on seeded random vectors: |<y, A x> - <A^H y, x>| / (|y| |A x|)
+    g = torch.Generator(device="cpu").manual_seed(5)
+    x = torch.randn((nx, nx), generator=g, dtype=torch.float64).to(dev)
+    y = (torch.randn(vis.shape, generator=g, dtype=torch.float64)
+         + 1j * torch.randn(vis.shape, generator=g, dtype=torch.float64)).to(dev)
+    Ax = G.dirty2ms(tu, tf, x.to(torch.float32 if prec == "mixed" else torch.float64), px, px,
+                    eps, precision=prec, vis_dtype=np.complex128, **KW)
+    Aty = G.ms2dirty(tu, tf, y.to(torch.complex64 if prec == "mixed" else torch.complex128),
+                     nx, nx, px, px, eps, precision=prec, dirty_dtype=np.float64, **KW)
+    if prec == "mixed":  # the operator saw the rounded inputs
+        x = x.to(torch.float32).double()
+        y = y.to(torch.complex64).to(torch.complex128)
+    a = torch.vdot(y.ravel(), Ax.ravel()).real.item()
+    b = torch.vdot(Aty.ravel().to(torch.complex128), x.ravel().to(torch.complex128)).real.item()
+    assert abs(a - b) / (y.norm().item() * Ax.norm().item()) < tol_adj
+    del x, y, Ax, Aty
+    if O.ref_available():
+        rp = "float" if prec == "mixed" else "double"
+        dr = O.ref_ms2dirty(uvw, freq, vis, nx, nx, px, px, eps, prec=rp)
+        assert O.rel_rms(d, dr.astype(np.float64)) < tol_ref
+        vr = O.ref_dirty2ms(uvw, freq, model.astype(fdt), px, px, eps, prec=rp, vis_dtype=cdt)
+        assert O.rel_rms(v, vr.astype(np.complex128)) < tol_ref
 
 
 def test_config1_fp64_full(G):

@@ -35,6 +35,7 @@ EXPORTED = [
     "wsg_stream_predict_begin", "wsg_stream_predict", "wsg_stream_get_stats",
     "wsg_weights_create", "wsg_weights_destroy", "wsg_weights_grid", "wsg_weights_finish",
     "wsg_weights_apply", "wsg_weights_get", "wsg_autotune", "wsg_ctx_set_async",
+    "wsg_ms2dirty_tuning", "wsg_dirty2ms_tuning", "wsg_get_tuning", "wsg_tuning_choice",
 ]
 
 c_size_t, c_double, c_int, c_void_p = ctypes.c_size_t, ctypes.c_double, ctypes.c_int, ctypes.c_void_p
@@ -165,6 +166,11 @@ def lib():
         L.wsg_weights_get.argtypes = [vp, vp, P(c_size_t), P(c_size_t), P(c_double)]
         L.wsg_autotune.argtypes = [vp, P(WsgArgs), vp, c_int, P(WsgStats)]
         L.wsg_ctx_set_async.argtypes = [vp, c_int]
+        L.wsg_ms2dirty_tuning.argtypes = [vp, P(WsgArgs), vp, vp, c_int]
+        L.wsg_dirty2ms_tuning.argtypes = [vp, P(WsgArgs), vp, vp]
+        L.wsg_get_tuning.argtypes = [vp, P(c_int), P(c_int), P(c_int), P(c_double)]
+        L.wsg_tuning_choice.argtypes = [P(WsgArgs), c_size_t, c_double, c_double,
+                                        P(ctypes.c_uint64), P(c_int), P(c_int), P(c_int)]
         L.wsg_last_error.restype = ctypes.c_char_p
         L.wsg_abi_version.restype = c_int
         for name in EXPORTED:

@@ -389,6 +389,7 @@ void choose_grid(GridPlan &g, double sigma_min, double sigma_max, int tile, bool
     if (pow2_v) {
       size_t p2 = 256;
       while (p2 < size_t(g.ny * k.sigma) + 2) p2 *= 2;
+      if (p2 > kPow2VMax) continue;  // beyond the shared-memory row FFT
       t.nv = p2;
     }
     set_band(t);
@@ -484,6 +485,130 @@ std::vector<std::pair<int, double>> rank_kernels(const GridPlan &g, double sigma
   for (size_t i = 0; i < all.size() && out.size() < n; ++i)
     out.emplace_back(std::get<1>(all[i]), std::get<2>(all[i]));
   return out;
+}
+
+// ------------------------------------------------- tuned schedule choice
+
+namespace {
+// n-1 range over a rectangle of (l, m), corners and axis crossings
+// (get_nminmax_rectangle, wgridder.cc:110-126)
+std::pair<double, double> nm1_range(double x0, double x1, double y0, double y1) {
+  std::vector<double> xs{x0, x1}, ys{y0, y1};
+  if (x0 * x1 < 0) xs.push_back(0.0);
+  if (y0 * y1 < 0) ys.push_back(0.0);
+  double lo = 1e300, hi = -1e300;
+  for (double x : xs)
+    for (double y : ys) {
+      const double r2 = x * x + y * y;
+      const double n = (r2 <= 1.0) ? std::sqrt(1.0 - r2) - 1.0 : -std::sqrt(r2 - 1.0) - 1.0;
+      lo = std::min(lo, n);
+      hi = std::max(hi, n);
+    }
+  return {lo, hi};
+}
+}  // namespace
+
+TuningChoice tuning_choice(size_t nx, size_t ny, double px, double py, double eps, bool do_w,
+                           double cx, double cy, size_t nvis_all, double wmin, double wmax,
+                           const uint64_t *hist) {
+  TuningChoice out;
+  out.wmin = wmin;
+  out.wmax = wmax;
+  if (!do_w || nx < 500 || ny < 500) return out;
+  size_t total = 0;
+  std::vector<size_t> acc(kTuningBins);
+  for (int i = 0; i < kTuningBins; ++i) acc[i] = (total += size_t(hist[i]));
+  if (total == 0 || !(wmax > wmin)) return out;
+  // the reference's CPU cost model, in seconds: support from epsilon,
+  // oversampling 1.5, a per-visibility gridding cost for its 4-wide SIMD
+  // kernels, a per-plane FFT cost scaled from a 2048^2 reference transform,
+  // and a per-call pass over all visibilities
+  const int W = std::max(3, std::min(16, int(2.0 - std::log10(eps))));
+  const double sigma = 1.5;
+  std::vector<double> wb(kTuningBins + 1);
+  for (int i = 0; i <= kTuningBins; ++i) wb[i] = wmin + i * (wmax - wmin) / kTuningBins;
+  const double xmin = cx - 0.5 * nx * px, ymin = cy - 0.5 * ny * py;
+  const double xmax = xmin + (nx - 1) * px, ymax = ymin + (ny - 1) * py;
+  const auto full = nm1_range(xmin, xmax, ymin, ymax);
+  const double dw = 1.0 / sigma / std::fabs(full.first - full.second);
+  const int nvec = (W + 3) / 4;
+  const double grid0 = 2.2e-10 * W * (W * nvec * 4 + (2 * nvec + 1) * (W + 3) * 4);
+  const double nu = sigma * nx, nv = sigma * ny;
+  const double ref = 2048.0;
+  const double fft0 = double(nx) / ref * nv / ref * (std::log(nu * nv) / std::log(ref * ref)) *
+                      0.0693 * 1.3;
+  const double overhead = 4e-9 * double(nvis_all);
+  const double planes_all = (wmax - wmin) / dw + W;
+  if (planes_all <= 2 * W || grid0 * total > 2 * fft0 * planes_all) return out;
+
+  double best = 1e300;
+  int bnfx = 0, bnfy = 0, bcut = 0;
+  for (int icut = 0; icut <= kTuningBins; ++icut) {
+    const double wcut = wb[icut];
+    const size_t nlo = icut == 0 ? 0 : acc[icut - 1];
+    const size_t nhi = total - nlo;
+    double cost = 1e300;
+    int cfx = 0, cfy = 0;
+    if (nhi > 0) {
+      for (int fx = 1; fx < 8; ++fx)
+        for (int fy = (fx == 1) ? 2 : 1; fy < 8; ++fy) {
+          double planes = 0;
+          for (int i = 0; i < fx; ++i)
+            for (int j = 0; j < fy; ++j) {
+              const auto r = nm1_range(xmin + i * (xmax - xmin) / fx, xmin + (i + 1) * (xmax - xmin) / fx,
+                                       ymin + j * (ymax - ymin) / fy, ymin + (j + 1) * (ymax - ymin) / fy);
+              const double fdw = 1.0 / sigma / std::fabs(r.first - r.second);
+              planes += (wmax - wcut) / fdw + W;
+            }
+          const double nf = double(fx * fy);
+          const double c = nf * double(nhi) * grid0 +
+                           fft0 * planes / nf * std::log(nu * nv / nf) / std::log(nu * nv) +
+                           nf * overhead;
+          if (c < cost) {
+            cost = c;
+            cfx = fx;
+            cfy = fy;
+          }
+        }
+    } else {
+      cost = 0;
+    }
+    if (icut != 0) {
+      // the reference discounts the low part's transform when nothing is
+      // above the cut (its FFT is then typically sparse)
+      const double fudge = nhi == 0 ? 0.75 : 1.0;
+      cost += fudge * fft0 * ((wcut - wmin) / dw + W) + grid0 * double(nlo) + overhead;
+    }
+    if (cost < best) {
+      best = cost;
+      bnfx = cfx;
+      bnfy = cfy;
+      bcut = icut;
+    }
+  }
+  if (bcut == kTuningBins) return out;  // no facets: the plain operator
+  out.nfx = bnfx;
+  out.nfy = bnfy;
+  out.icut = bcut;
+  return out;
+}
+
+Facet tuning_facet(size_t nx, size_t ny, int nfx, int nfy, int ifx, int ify, double px, double py,
+                   double cx, double cy) {
+  size_t is = (nx + nfx - 1) / nfx, js = (ny + nfy - 1) / nfy;
+  is += is % 2;
+  js += js % 2;
+  require(is <= nx && js <= ny, "bad facet step");
+  Facet f;
+  f.x0 = size_t(ifx) * is;
+  f.x1 = std::min(size_t(ifx + 1) * is, nx);
+  f.y0 = size_t(ify) * js;
+  f.y1 = std::min(size_t(ify + 1) * js, ny);
+  require(f.x0 + 32 <= f.x1 && f.x1 % 2 == 0, "bad facet x length");
+  require(f.y0 + 32 <= f.y1 && f.y1 % 2 == 0, "bad facet y length");
+  f.cx = cx + px * 0.5 * (double(f.x0 + f.x1) - double(nx));
+  f.cy = cy + py * 0.5 * (double(f.y0 + f.y1) - double(ny));
+  return f;
 }
 
 size_t plan_bytes(const GridPlan &g, size_t planes, bool gridding) {

@@ -147,6 +147,46 @@ int wsg_dirty2ms(wsg_ctx *ctx, const wsg_args *a, const void *dirty, void *vis) 
   });
 }
 
+int wsg_ms2dirty_tuning(wsg_ctx *ctx, const wsg_args *a, const void *vis, void *dirty,
+                        int accumulate) {
+  return guarded([&] {
+    wsg::require(ctx && a, "ctx and args are required");
+    ctx->ctx->ms2dirty_tuning(*a, vis, dirty, accumulate);
+  });
+}
+
+int wsg_dirty2ms_tuning(wsg_ctx *ctx, const wsg_args *a, const void *dirty, void *vis) {
+  return guarded([&] {
+    wsg::require(ctx && a, "ctx and args are required");
+    ctx->ctx->dirty2ms_tuning(*a, dirty, vis);
+  });
+}
+
+int wsg_get_tuning(const wsg_ctx *ctx, int *nfx, int *nfy, int *icut, double *wcut) {
+  return guarded([&] {
+    wsg::require(ctx && nfx && nfy && icut && wcut, "NULL argument");
+    const wsg::TuningChoice &t = ctx->ctx->last_tuning;
+    *nfx = t.nfx;
+    *nfy = t.nfy;
+    *icut = t.icut;
+    *wcut = t.split() ? t.wmin + t.icut * (t.wmax - t.wmin) / wsg::kTuningBins : -1.0;
+  });
+}
+
+int wsg_tuning_choice(const wsg_args *a, size_t nvis_all, double wmin, double wmax,
+                      const uint64_t *hist, int *nfx, int *nfy, int *icut) {
+  return guarded([&] {
+    wsg::require(a && hist && nfx && nfy && icut, "NULL argument");
+    const size_t nx = a->npix_x + (a->npix_x & 1), ny = a->npix_y + (a->npix_y & 1);
+    const wsg::TuningChoice t =
+        wsg::tuning_choice(nx, ny, a->pixsize_x, a->pixsize_y, a->epsilon, a->do_wgridding != 0,
+                           a->center_x, a->center_y, nvis_all, wmin, wmax, hist);
+    *nfx = t.nfx;
+    *nfy = t.nfy;
+    *icut = t.icut;
+  });
+}
+
 int wsg_get_stats(const wsg_ctx *ctx, wsg_stats *out) {
   return guarded([&] {
     wsg::require(ctx && out, "ctx and out are required");

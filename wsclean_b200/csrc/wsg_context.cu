@@ -191,7 +191,7 @@ std::vector<DevBuf *> Context::all_buffers() {
   return {&b_uvw, &b_fovc, &b_vis, &b_wgt, &b_mask, &b_keys_a, &b_keys_b, &b_vals_a,
           &b_vals_b, &b_cub, &b_rec, &b_chunks, &b_small, &b_band, &b_bandf, &b_bandd, &b_H,
           &b_img, &b_img2, &b_acc, &b_fftwork, &b_out, &corr_cache[0].buf, &corr_cache[1].buf,
-          &tw_cache[0].buf, &tw_cache[1].buf};
+          &tw_cache[0].buf, &tw_cache[1].buf, &b_tune, &b_tfovc, &b_mhi, &b_mlo, &b_pad};
 }
 
 void Context::invalidate_tables() {
@@ -793,6 +793,7 @@ ScreenArgs make_screen(const GridPlan &g, const double *d_cf, const ChebCorr &cc
   s.ny = int(g.ny);
   s.nu = int(g.nu);
   s.nv = int(g.nv);
+  s.ld = g.ny;
   s.px = g.px;
   s.py = g.py;
   s.x0 = g.lshift - 0.5 * g.nx * g.px;
@@ -987,7 +988,7 @@ size_t Context::choose_planes(const GridPlan &g, bool gridding) {
 
 template <typename R>
 bool Context::grid_core(const wsg_args &a, const Staged &s, double *img, bool accumulate,
-                        void *direct_out) {
+                        void *direct_out, size_t ld) {
   const bool dbl = sizeof(R) == 8;
   GridPlan gp;
   gp.nx = a.npix_x;
@@ -1002,11 +1003,15 @@ bool Context::grid_core(const wsg_args &a, const Staged &s, double *img, bool ac
   gp.divide_by_n = a.divide_by_n != 0;
   gp.lshift = a.center_x;
   gp.mshift = a.negate_v ? -a.center_y : a.center_y;
-  const size_t npix = a.npix_x * a.npix_y;
+  if (ld == 0) ld = a.npix_y;
+  // zeroes the FP64 image (a strided block when it is a facet)
+  auto clear_img = [&]() {
+    CK(cudaMemset2DAsync(img, ld * sizeof(double), 0, a.npix_y * sizeof(double), a.npix_x, stream));
+  };
 
   CK(cudaEventRecord(ev[0], stream));
   if (!prepare<R>(a, s, true, nullptr, gp)) {
-    if (!accumulate) CK(cudaMemsetAsync(img, 0, npix * sizeof(double), stream));
+    if (!accumulate) clear_img();
     record_stats(gp, true, 0);
     return false;
   }
@@ -1019,9 +1024,9 @@ bool Context::grid_core(const wsg_args &a, const Staged &s, double *img, bool ac
   mark("choose_planes");
   // one pass over all planes and nothing to accumulate: the w-screen sum
   // goes straight to the caller's image, else through the FP64 accumulator
-  const bool direct = direct_out && !accumulate && P >= gp.nplanes;
+  const bool direct = direct_out && !accumulate && P >= gp.nplanes && ld == a.npix_y;
   const int out_mode = direct ? (a.dirty_type == WSG_F64 ? 2 : 1) : 0;
-  if (!accumulate && !direct) CK(cudaMemsetAsync(img, 0, npix * sizeof(double), stream));
+  if (!accumulate && !direct) clear_img();
   const size_t cs = 2 * sizeof(R);
   const size_t nv = gp.nv;
   // the spread writes `band`; the v transform goes out of place to `bandf`,
@@ -1074,6 +1079,7 @@ bool Context::grid_core(const wsg_args &a, const Staged &s, double *img, bool ac
     ScreenArgs sa = make_screen(gp, cf_cur, cc, P);
     sa.pb0 = int(pb0);
     sa.npl = int(npl);
+    sa.ld = ld;
     dim3 sg((gp.nx + 31) / 32, (gp.ny + 31) / 32);
     k_screen_add<R><<<sg, 256, 0, stream>>>(sa, H, img, direct_out, out_mode);
     cuda_check(cudaGetLastError(), "k_screen_add launch");
@@ -1110,7 +1116,7 @@ bool Context::grid_core(const wsg_args &a, const Staged &s, double *img, bool ac
 
 template <typename R>
 void Context::degrid_core(const wsg_args &a, const Staged &s, const double *img, void *vis_out,
-                          const void *direct_in) {
+                          const void *direct_in, size_t ld, bool vis_acc) {
   const bool dbl = sizeof(R) == 8;
   GridPlan gp;
   gp.nx = a.npix_x;
@@ -1126,8 +1132,10 @@ void Context::degrid_core(const wsg_args &a, const Staged &s, const double *img,
   gp.lshift = a.center_x;
   gp.mshift = a.negate_v ? -a.center_y : a.center_y;
 
+  if (ld == 0) ld = a.npix_y;
+
   CK(cudaEventRecord(ev[0], stream));
-  if (!prepare<R>(a, s, false, vis_out, gp)) {
+  if (!prepare<R>(a, s, false, vis_acc ? nullptr : vis_out, gp)) {
     record_stats(gp, false, 0);
     return;
   }
@@ -1168,6 +1176,7 @@ void Context::degrid_core(const wsg_args &a, const Staged &s, const double *img,
   ga.sb = GridKernels<R>::SB;
   ga.vis_out = vis_out;
   ga.vis_double = a.vis_type == WSG_C128;
+  ga.vis_accumulate = vis_acc ? 1 : 0;
   const bool multi = P < gp.nplanes;
   const bool need_acc = multi || GridKernels<R>::groups(gp.kernel.W) > 1;
   ga.acc = need_acc ? b_acc.ensure(gp.nvis * cs) : nullptr;
@@ -1181,6 +1190,7 @@ void Context::degrid_core(const wsg_args &a, const Staged &s, const double *img,
     ScreenArgs sa = make_screen(gp, cf_cur, cc, P);
     sa.pb0 = int(pb0);
     sa.npl = int(npl);
+    sa.ld = ld;
     dim3 sg((gp.nx + 31) / 32, (gp.ny + 31) / 32);
     // the caller's image itself (FP32 or FP64) when given, else the FP64 copy
     const void *src = direct_in ? direct_in : static_cast<const void *>(img);
@@ -1224,8 +1234,8 @@ void Context::degrid_core(const wsg_args &a, const Staged &s, const double *img,
     }
   }
   if (need_acc) {
-    k_finalize<R><<<launch_blocks(gp.nvis, 256), 256, 0, stream>>>(int(gp.nvis), b_rec.p, ga.acc,
-                                                                  vis_out, ga.vis_double, 0);
+    k_finalize<R><<<launch_blocks(gp.nvis, 256), 256, 0, stream>>>(
+        int(gp.nvis), b_rec.p, ga.acc, vis_out, ga.vis_double, ga.vis_accumulate);
     cuda_check(cudaGetLastError(), "k_finalize launch");
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
   }
@@ -1346,7 +1356,8 @@ void Context::ms2dirty(const wsg_args &a, const void *vis, void *dirty, int accu
   CK(cudaEventRecord(ev_in, cpy));
   CK(cudaStreamWaitEvent(stream, ev_in, 0));
   // (stage_in returns device inputs unchanged: a new pointer means copied)
-  ScanPlacement place(*this, sl, s.uvw != a.uvw && s.vis != vis &&
+  // (a tuned call's parts scan masks made on the main stream: no early scan)
+  ScanPlacement place(*this, sl, !tuned_call && s.uvw != a.uvw && s.vis != vis &&
                                      (a.wgt == nullptr || s.wgt != a.wgt) &&
                                      (a.mask == nullptr || s.mask != a.mask));
   double *img = reinterpret_cast<double *>(b_img.ensure(npix * sizeof(double)));
@@ -1360,9 +1371,13 @@ void Context::ms2dirty(const wsg_args &a, const void *vis, void *dirty, int accu
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
   }
   void *dout = ddev ? dirty : sl.out.ensure(npix * dsz);
-  const bool direct = (a.precision == WSG_PREC_FP64)
-                          ? grid_core<double>(a, s, img, accumulate != 0, dout)
-                          : grid_core<float>(a, s, img, accumulate != 0, dout);
+  bool direct;
+  if (tuned_call)
+    direct = (a.precision == WSG_PREC_FP64) ? grid_tuned<double>(a, s, img, accumulate != 0, dout)
+                                            : grid_tuned<float>(a, s, img, accumulate != 0, dout);
+  else
+    direct = (a.precision == WSG_PREC_FP64) ? grid_core<double>(a, s, img, accumulate != 0, dout)
+                                            : grid_core<float>(a, s, img, accumulate != 0, dout);
   if (!direct) {  // convert/copy out of the FP64 accumulator
     int nb = launch_blocks(npix, 256);
     if (a.dirty_type == WSG_F64)
@@ -1399,7 +1414,8 @@ void Context::dirty2ms(const wsg_args &a, const void *dirty, void *vis) {
   const void *din = stage_in(dirty, npix * dsz, sl.out, cpy);
   CK(cudaEventRecord(ev_in, cpy));
   CK(cudaStreamWaitEvent(stream, ev_in, 0));
-  ScanPlacement place(*this, sl, s.uvw != a.uvw && (a.wgt == nullptr || s.wgt != a.wgt) &&
+  ScanPlacement place(*this, sl, !tuned_call && s.uvw != a.uvw &&
+                                     (a.wgt == nullptr || s.wgt != a.wgt) &&
                                      (a.mask == nullptr || s.mask != a.mask));
   // (the w-screen reads the model image in place: no FP64 copy)
   const bool vdev = is_device_pointer(vis);
@@ -1407,10 +1423,16 @@ void Context::dirty2ms(const wsg_args &a, const void *dirty, void *vis) {
   // inactive visibilities are zeroed; with no active ones at all the whole
   // output is zero
   CK(cudaMemsetAsync(vout, 0, vbytes, stream));
-  if (a.precision == WSG_PREC_FP64)
+  if (tuned_call) {
+    if (a.precision == WSG_PREC_FP64)
+      degrid_tuned<double>(a, s, nullptr, vout, din);
+    else
+      degrid_tuned<float>(a, s, nullptr, vout, din);
+  } else if (a.precision == WSG_PREC_FP64) {
     degrid_core<double>(a, s, nullptr, vout, din);
-  else
+  } else {
     degrid_core<float>(a, s, nullptr, vout, din);
+  }
   cudaStream_t last = stream;
   if (!vdev) {
     CK(cudaEventRecord(ev_done, stream));
@@ -1422,16 +1444,22 @@ void Context::dirty2ms(const wsg_args &a, const void *dirty, void *vis) {
 }
 
 void Context::degrid_from_image(const wsg_args &a, const Staged &s, const double *img, void *vis,
-                                size_t vbytes) {
+                                size_t vbytes, bool tuned) {
   const bool vdev = is_device_pointer(vis);
   void *vout = vdev ? vis : b_vis.ensure(vbytes);
   // inactive visibilities are zeroed by the scan; with no active ones at all
   // the whole output is zero
   CK(cudaMemsetAsync(vout, 0, vbytes, stream));
-  if (a.precision == WSG_PREC_FP64)
+  if (tuned) {
+    if (a.precision == WSG_PREC_FP64)
+      degrid_tuned<double>(a, s, img, vout, nullptr);
+    else
+      degrid_tuned<float>(a, s, img, vout, nullptr);
+  } else if (a.precision == WSG_PREC_FP64) {
     degrid_core<double>(a, s, img, vout);
-  else
+  } else {
     degrid_core<float>(a, s, img, vout);
+  }
   if (!vdev) CK(cudaMemcpyAsync(vis, vout, vbytes, cudaMemcpyDeviceToHost, stream));
   CK(cudaEventRecord(ev[6], stream));
   CK(cudaStreamSynchronize(stream));
@@ -1441,6 +1469,247 @@ void Context::degrid_from_image(const wsg_args &a, const Staged &s, const double
   stats.kernel_launches = g_kernel_launches.load();
   stats.nrows = a.nrows;
   stats.nchan = a.nchan;
+}
+
+// ------------------------------------------------------ tuned schedule
+//
+// ducc0's ms2dirty_tuning / dirty2ms_tuning (wgridder.h:1781-1877), which
+// WSClean calls for -gridder tuned-wgridder: the |w| histogram of the
+// masked-in visibilities decides (tuning_choice) whether to subdivide; if
+// so, the visibilities at or above the cut bin are gridded facet by facet,
+// each facet an image of its own with its own phase centre (and so its own,
+// smaller n-1 range and fewer w planes), written into its block of the
+// image, and those below the cut are gridded on the whole image and added.
+// Each part is one grid_core / degrid_core call on the device-resident
+// inputs with a mask selecting its visibilities.
+
+TuningChoice Context::tuning_for(const wsg_args &a, const Staged &s) {
+  const size_t nrows = a.nrows, nchan = a.nchan;
+  std::vector<double> freq(nchan), fovc(nchan);
+  if (is_device_pointer(a.freq))
+    CK(cudaMemcpy(freq.data(), a.freq, nchan * sizeof(double), cudaMemcpyDeviceToHost));
+  else
+    std::memcpy(freq.data(), a.freq, nchan * sizeof(double));
+  for (size_t c = 0; c < nchan; ++c) fovc[c] = freq[c] / kSpeedOfLight;
+  double *d_fovc = reinterpret_cast<double *>(b_tfovc.ensure(nchan * sizeof(double)));
+  CK(cudaMemcpyAsync(d_fovc, fovc.data(), nchan * sizeof(double), cudaMemcpyHostToDevice, stream));
+  auto *d = reinterpret_cast<unsigned long long *>(b_tune.ensure((3 + kTuningBins) * 8));
+  unsigned long long h[3 + kTuningBins] = {0x7ff0000000000000ull, 0, 0};
+  CK(cudaMemcpyAsync(d, h, sizeof h, cudaMemcpyHostToDevice, stream));
+  const int nb = std::min(launch_blocks(nrows, 256), num_sms * 8);
+  k_wrange<<<nb, 256, 0, stream>>>(nrows, int(nchan), s.uvw, d_fovc, s.mask, d);
+  cuda_check(cudaGetLastError(), "k_wrange launch");
+  g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+  CK(cudaMemcpyAsync(h, d, 3 * 8, cudaMemcpyDeviceToHost, stream));
+  CK(cudaStreamSynchronize(stream));
+  TuningChoice none;
+  if (h[2] == 0) return none;
+  double wmin, wmax;
+  std::memcpy(&wmin, &h[0], 8);
+  std::memcpy(&wmax, &h[1], 8);
+  none.wmin = wmin;
+  none.wmax = wmax;
+  if (!(wmax > wmin)) return none;
+  const double xdw = kTuningBins / (wmax - wmin);
+  k_whist<<<nb, 256, 0, stream>>>(nrows, int(nchan), s.uvw, d_fovc, s.mask, wmin, xdw, d + 3);
+  cuda_check(cudaGetLastError(), "k_whist launch");
+  g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+  CK(cudaMemcpyAsync(h + 3, d + 3, kTuningBins * 8, cudaMemcpyDeviceToHost, stream));
+  CK(cudaStreamSynchronize(stream));
+  std::vector<uint64_t> hist(h + 3, h + 3 + kTuningBins);
+  TuningChoice tc = tuning_choice(a.npix_x, a.npix_y, a.pixsize_x, a.pixsize_y, a.epsilon,
+                                  a.do_wgridding != 0, tune_center_set ? tune_center_x : a.center_x,
+                                  tune_center_set ? tune_center_y : a.center_y, nrows * nchan, wmin,
+                                  wmax, hist.data());
+  if (tc.split() && tc.icut > 0) {
+    uint8_t *hi = reinterpret_cast<uint8_t *>(b_mhi.ensure(nrows * nchan));
+    uint8_t *lo = reinterpret_cast<uint8_t *>(b_mlo.ensure(nrows * nchan));
+    k_wsplit<<<launch_blocks(nrows, 256), 256, 0, stream>>>(nrows, int(nchan), s.uvw, d_fovc,
+                                                            s.mask, wmin, xdw, tc.icut, hi, lo);
+    cuda_check(cudaGetLastError(), "k_wsplit launch");
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+  }
+  if (verbosity > 0) {
+    if (!tc.split())
+      std::printf("Tuning decision:\n  no subdivision\n");
+    else if (tc.icut == 0)
+      std::printf("Tuning decision:\n  subdividing into %dx%d facets.\n", tc.nfx, tc.nfy);
+    else
+      std::printf("Tuning decision:\n  subdividing w range at w=%g, subdividing high w part into "
+                  "%dx%d facets.\n", wmin + tc.icut * (wmax - wmin) / kTuningBins, tc.nfx, tc.nfy);
+    std::fflush(stdout);
+  }
+  return tc;
+}
+
+// The arguments of facet (i, j): its size and phase centre.  The facet's
+// pixels must land where they lie in the whole image.  Along y that depends
+// on negate_v: the gridder places pixel j at m = -center_y + (j - ny/2) py
+// when v is negated, so a facet above the middle needs its centre moved the
+// other way.  (The reference's faceting moves it the same way in both cases,
+// so with negate_v -- WSClean's call -- its tuned images have their facets
+// mirrored along y; the results here equal the plain operator's.)
+static wsg_args facet_args(const wsg_args &a, const TuningChoice &tc, int i, int j) {
+  const Facet f = tuning_facet(a.npix_x, a.npix_y, tc.nfx, tc.nfy, i, j, a.pixsize_x,
+                               a.pixsize_y, a.center_x, a.center_y);
+  wsg_args af = a;
+  af.npix_x = f.x1 - f.x0;
+  af.npix_y = f.y1 - f.y0;
+  af.center_x = f.cx;
+  af.center_y = a.negate_v ? 2.0 * a.center_y - f.cy : f.cy;
+  return af;
+}
+
+template <typename R>
+bool Context::grid_tuned(const wsg_args &a, const Staged &s, double *img, bool accumulate,
+                         void *direct_out) {
+  const TuningChoice tc = tuning_for(a, s);
+  last_tuning = tc;
+  if (!tc.split()) return grid_core<R>(a, s, img, accumulate, direct_out);
+  const size_t nx = a.npix_x, ny = a.npix_y;
+  if (!accumulate) CK(cudaMemsetAsync(img, 0, nx * ny * sizeof(double), stream));
+  const uint8_t *hi = tc.icut > 0 ? reinterpret_cast<const uint8_t *>(b_mhi.p) : s.mask;
+  for (int i = 0; i < tc.nfx; ++i)
+    for (int j = 0; j < tc.nfy; ++j) {
+      const Facet f = tuning_facet(nx, ny, tc.nfx, tc.nfy, i, j, a.pixsize_x, a.pixsize_y,
+                                   a.center_x, a.center_y);
+      wsg_args af = facet_args(a, tc, i, j);
+      af.mask = hi;
+      Staged sf = s;
+      sf.mask = hi;
+      grid_core<R>(af, sf, img + f.x0 * ny + f.y0, true, nullptr, ny);
+    }
+  if (tc.icut > 0) {
+    wsg_args al = a;
+    Staged sl = s;
+    al.mask = sl.mask = reinterpret_cast<const uint8_t *>(b_mlo.p);
+    grid_core<R>(al, sl, img, true, nullptr);
+  }
+  return false;
+}
+
+template <typename R>
+void Context::degrid_tuned(const wsg_args &a, const Staged &s, const double *img, void *vis_out,
+                           const void *direct_in) {
+  const TuningChoice tc = tuning_for(a, s);
+  last_tuning = tc;
+  if (!tc.split()) {
+    degrid_core<R>(a, s, img, vis_out, direct_in);
+    return;
+  }
+  // every part adds its visibilities (the caller zeroed vis_out)
+  const size_t nx = a.npix_x, ny = a.npix_y;
+  const size_t dsz = a.dirty_type == WSG_F64 ? 8 : 4;
+  const uint8_t *hi = tc.icut > 0 ? reinterpret_cast<const uint8_t *>(b_mhi.p) : s.mask;
+  for (int i = 0; i < tc.nfx; ++i)
+    for (int j = 0; j < tc.nfy; ++j) {
+      const Facet f = tuning_facet(nx, ny, tc.nfx, tc.nfy, i, j, a.pixsize_x, a.pixsize_y,
+                                   a.center_x, a.center_y);
+      wsg_args af = facet_args(a, tc, i, j);
+      af.mask = hi;
+      Staged sf = s;
+      sf.mask = hi;
+      const size_t off = f.x0 * ny + f.y0;
+      degrid_core<R>(af, sf, img ? img + off : nullptr, vis_out,
+                     direct_in ? static_cast<const char *>(direct_in) + off * dsz : nullptr, ny,
+                     true);
+    }
+  if (tc.icut > 0) {
+    wsg_args al = a;
+    Staged sl = s;
+    al.mask = sl.mask = reinterpret_cast<const uint8_t *>(b_mlo.p);
+    degrid_core<R>(al, sl, img, vis_out, direct_in, 0, true);
+  }
+}
+
+// Marks a raw operator call as tuned while alive; for a padded odd-size
+// image, also the centre the subdivision rule is given.
+struct TunedCall {
+  Context &cx;
+  explicit TunedCall(Context &c) : cx(c) { cx.tuned_call = true; }
+  TunedCall(Context &c, double cx_rule, double cy_rule) : cx(c) {
+    cx.tuned_call = true;
+    cx.tune_center_set = true;
+    cx.tune_center_x = cx_rule;
+    cx.tune_center_y = cy_rule;
+  }
+  ~TunedCall() {
+    cx.tuned_call = false;
+    cx.tune_center_set = false;
+  }
+};
+
+// The even image one pixel larger along each odd axis of a, centred so that
+// its pixel (i, j) lies where pixel (i, j) of a does: half a pixel further
+// along x, and along y in the direction pixels run (opposite with negate_v).
+static wsg_args padded_odd(const wsg_args &a) {
+  const size_t xodd = a.npix_x & 1, yodd = a.npix_y & 1;
+  wsg_args ap = a;
+  ap.npix_x += xodd;
+  ap.npix_y += yodd;
+  ap.center_x += 0.5 * a.pixsize_x * double(xodd);
+  ap.center_y += (a.negate_v ? -0.5 : 0.5) * a.pixsize_y * double(yodd);
+  return ap;
+}
+
+void Context::ms2dirty_tuning(const wsg_args &a, const void *vis, void *dirty, int accumulate) {
+  require(vis && dirty, "vis and dirty are required");
+  const size_t xodd = a.npix_x & 1, yodd = a.npix_y & 1;
+  if (!xodd && !yodd) {
+    TunedCall tc(*this);
+    ms2dirty(a, vis, dirty, accumulate);
+    return;
+  }
+  // odd sizes (the reference's tuned calls take them, wgridder.h:1789-1801):
+  // an image one pixel larger along each odd axis whose first npix_x x
+  // npix_y pixels lie where pixel (i, j) of the odd image lies,
+  // l = center_x + (i - npix_x/2) px (and likewise m), and are kept
+  require(a.npix_x > 0 && a.npix_y > 0, "empty image");
+  CK(cudaSetDevice(device));
+  const wsg_args ap = padded_odd(a);
+  const size_t dsz = a.dirty_type == WSG_F64 ? 8 : 4;
+  void *tmp = b_pad.ensure(ap.npix_x * ap.npix_y * dsz);
+  if (accumulate) {
+    CK(cudaMemsetAsync(tmp, 0, ap.npix_x * ap.npix_y * dsz, stream));
+    CK(cudaMemcpy2DAsync(tmp, ap.npix_y * dsz, dirty, a.npix_y * dsz, a.npix_y * dsz, a.npix_x,
+                         cudaMemcpyDefault, stream));
+  }
+  CK(cudaStreamSynchronize(stream));
+  {
+    // the reference's rule sees the padded image centred half a pixel
+    // further along both odd axes
+    TunedCall tc(*this, a.center_x + 0.5 * a.pixsize_x * double(xodd),
+                 a.center_y + 0.5 * a.pixsize_y * double(yodd));
+    ms2dirty(ap, vis, tmp, accumulate);
+  }
+  CK(cudaMemcpy2DAsync(dirty, a.npix_y * dsz, tmp, ap.npix_y * dsz, a.npix_y * dsz, a.npix_x,
+                       cudaMemcpyDefault, stream));
+  CK(cudaStreamSynchronize(stream));
+}
+
+void Context::dirty2ms_tuning(const wsg_args &a, const void *dirty, void *vis) {
+  require(vis && dirty, "vis and dirty are required");
+  const size_t xodd = a.npix_x & 1, yodd = a.npix_y & 1;
+  if (!xodd && !yodd) {
+    TunedCall tc(*this);
+    dirty2ms(a, dirty, vis);
+    return;
+  }
+  // odd sizes: the image zero-padded to the even image of ms2dirty_tuning,
+  // whose pixels lie at the same places, so that the pair stays adjoint (the
+  // reference pads here without moving the centre, wgridder.h:1829-1838,
+  // which puts the image half a pixel away from its gridding direction)
+  require(a.npix_x > 0 && a.npix_y > 0, "empty image");
+  CK(cudaSetDevice(device));
+  const wsg_args ap = padded_odd(a);
+  const size_t dsz = a.dirty_type == WSG_F64 ? 8 : 4;
+  void *tmp = b_pad.ensure(ap.npix_x * ap.npix_y * dsz);
+  CK(cudaMemsetAsync(tmp, 0, ap.npix_x * ap.npix_y * dsz, stream));
+  CK(cudaMemcpy2DAsync(tmp, ap.npix_y * dsz, dirty, a.npix_y * dsz, a.npix_y * dsz, a.npix_x,
+                       cudaMemcpyDefault, stream));
+  CK(cudaStreamSynchronize(stream));
+  TunedCall tc(*this, a.center_x, a.center_y);  // the centre the reference's rule sees
+  dirty2ms(ap, tmp, vis);
 }
 
 // ------------------------------------------------- reusable plans, batches
@@ -2651,10 +2920,17 @@ void Gridder::add_inversion_data(size_t nrows, size_t nchan, const double *uvw, 
   s.uvw = reinterpret_cast<const double *>(ctx.stage_in(uvw, nrows * 3 * sizeof(double), ctx.b_uvw));
   s.vis = ctx.stage_in(vis, nvis * 8, ctx.b_vis);
   double *img = reinterpret_cast<double *>(ctx.b_img2.p);
-  if (a.precision == WSG_PREC_FP64)
+  // -gridder tuned-wgridder: ms2dirty_tuning (wgriddinggridder_simple.cpp:59-63)
+  if (prm.tuning) {
+    if (a.precision == WSG_PREC_FP64)
+      ctx.grid_tuned<double>(a, s, img, true, nullptr);
+    else
+      ctx.grid_tuned<float>(a, s, img, true, nullptr);
+  } else if (a.precision == WSG_PREC_FP64) {
     ctx.grid_core<double>(a, s, img, true);
-  else
+  } else {
     ctx.grid_core<float>(a, s, img, true);
+  }
   CK(cudaStreamSynchronize(ctx.stream));
 }
 
@@ -2705,41 +2981,49 @@ void Gridder::predict_visibilities(size_t nrows, size_t nchan, const double *uvw
   CK(cudaSetDevice(ctx.device));
   Staged s;
   s.uvw = reinterpret_cast<const double *>(ctx.stage_in(uvw, nrows * 3 * sizeof(double), ctx.b_uvw));
-  ctx.degrid_from_image(a, s, reinterpret_cast<const double *>(ctx.b_img2.p), vis, nrows * nchan * 8);
+  // dirty2ms_tuning when tuned (wgriddinggridder_simple.cpp:109-113)
+  ctx.degrid_from_image(a, s, reinterpret_cast<const double *>(ctx.b_img2.p), vis, nrows * nchan * 8,
+                        prm.tuning != 0);
 }
 
 template bool Context::prepare<float>(const wsg_args &, const Staged &, bool, void *, GridPlan &);
 template bool Context::prepare<double>(const wsg_args &, const Staged &, bool, void *, GridPlan &);
-template bool Context::grid_core<float>(const wsg_args &, const Staged &, double *, bool, void *);
-template bool Context::grid_core<double>(const wsg_args &, const Staged &, double *, bool, void *);
+template bool Context::grid_core<float>(const wsg_args &, const Staged &, double *, bool, void *,
+                                        size_t);
+template bool Context::grid_core<double>(const wsg_args &, const Staged &, double *, bool, void *,
+                                         size_t);
 template void Context::degrid_core<float>(const wsg_args &, const Staged &, const double *, void *,
-                                          const void *);
+                                          const void *, size_t, bool);
 template void Context::degrid_core<double>(const wsg_args &, const Staged &, const double *, void *,
-                                           const void *);
+                                           const void *, size_t, bool);
 
 
 // ====================================================================
 // Allocation-free ms2dirty.
 //
-// Some callers cannot allocate device memory while they grid: code that runs
-// under a stream-ordered memory budget that must not grow, a host process that
-// has handed the whole device pool to another framework, or a pipeline being
-// recorded into a CUDA graph, where a cudaMalloc would be illegal.  For them
-// wsg_ms2dirty_noalloc runs the same mixed-precision pipeline as
-// wsg_ms2dirty but takes every scratch buffer (sort keys, visibility
-// records, chunk table, band grid, transformed columns, FP64 image, twiddle
-// and correction tables) from one file-scope device array of
-// kNoAllocScratchBytes, carves it up per call, and replaces cuFFT (whose plans
-// allocate) by the library's own shared-memory FFT, so nv is a power of two.
+// Some callers cannot allocate device memory while they grid: a plugin whose
+// host application reserved the whole device up front for its own memory pool
+// (a cudaMalloc there fails or steals from the host's budget), or code that
+// runs under a fixed device-memory budget that must not grow after start-up.
+// For them wsg_ms2dirty_noalloc runs the same mixed-precision pipeline as
+// wsg_ms2dirty but takes every scratch buffer (sort keys, visibility records,
+// chunk table, band grid, transformed columns, FP64 image, twiddle and
+// correction tables) from one file-scope device array of kNoAllocScratchBytes,
+// carves it up per call, and replaces cuFFT (whose plans allocate) by the
+// library's own shared-memory FFT, so nv is a power of two (at most 8192).
 // Every GPU that loads the library holds the array until the process exits.
 //
 // In host code the array's name is only a host-side stand-in, so its device
-// address is looked up once per device (cudaGetSymbolAddress, with that device
-// current) on the first call on the device; that first call should therefore
-// come before any stream capture.  All calls share the one array: calls that
-// overlap on the GPU (different streams, or different host threads on one
-// device) race on it and must be serialised by the caller.  Each call clears
-// what must start at zero (image, grids, counters) itself.
+// address is looked up (cudaGetSymbolAddress, with the device current) on the
+// first call in each CUDA context -- once per device, unless the device was
+// reset and a new context created, in which case the module is loaded again,
+// the array may move and the lookup is repeated.  That first call should come
+// before any stream capture.  The call synchronises its stream while it runs
+// (it reads the visibility scan's statistics back to plan the grid).  All
+// calls share the one array: calls that overlap on the GPU (different
+// streams, or different host threads on one device) race on it and must be
+// serialised by the caller.  Each call clears what must start at zero (image,
+// grids, counters) itself.
 // ====================================================================
 
 constexpr size_t kNoAllocScratchBytes = size_t(96) << 20;  // 96 MiB
@@ -2748,15 +3032,51 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 namespace {
 
 std::mutex g_noalloc_mu;
-std::map<int, unsigned char *> g_noalloc_ptr;  // device -> address of g_noalloc_scratch
+// (device, unique id of its current CUDA context) -> address of g_noalloc_scratch
+std::map<std::pair<int, unsigned long long>, unsigned char *> g_noalloc_ptr;
 
+// Unique id of the calling thread's current CUDA context (cuCtxGetId through
+// the runtime's driver entry point, so the library needs no link-time driver
+// dependency); 0 if the driver cannot tell, which keys the cache by device
+// alone.
+unsigned long long current_context_id() {
+  using GetCurrent = int (*)(void **);
+  using GetId = int (*)(void *, unsigned long long *);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<GetCurrent>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<GetId>(f);
+    cudaGetLastError();
+  });
+  void *ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current && get_id && get_current(&ctx) == 0 && ctx && get_id(ctx, &id) == 0) return id;
+  return 0;
+}
+
+// Device address of the scratch array in the current context of device dev
+// (dev is current).  Without a context id the address is looked up every time.
 unsigned char *noalloc_scratch(int dev) {
+  // cudaSetDevice initialises the device's primary context, so that the id
+  // below names the context the lookup and the kernels will use
+  cuda_check(cudaSetDevice(dev), "cudaSetDevice");
+  const unsigned long long id = current_context_id();
+  const auto key = std::make_pair(dev, id);
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  auto it = g_noalloc_ptr.find(dev);
-  if (it != g_noalloc_ptr.end()) return it->second;
+  auto it = g_noalloc_ptr.find(key);
+  if (id != 0 && it != g_noalloc_ptr.end()) return it->second;
   void *p = nullptr;
   cuda_check(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress(scratch)");
-  g_noalloc_ptr[dev] = reinterpret_cast<unsigned char *>(p);
+  if (id != 0) g_noalloc_ptr[key] = reinterpret_cast<unsigned char *>(p);
   return reinterpret_cast<unsigned char *>(p);
 }
 

@@ -80,16 +80,38 @@ class Context {
   // Grids into the FP64 accumulator img (+= with accumulate, else =), or --
   // when direct_out is given, nothing is accumulated and one pass covers all
   // planes -- writes the image of type a.dirty_type to direct_out and
-  // returns true.
+  // returns true.  ld: row stride of img (0: a.npix_y), for an image that is
+  // a facet of a larger one.
   bool grid_core(const wsg_args &a, const Staged &s, double *img, bool accumulate,
-                 void *direct_out = nullptr);
+                 void *direct_out = nullptr, size_t ld = 0);
   template <typename R>
   // Degrids the FP64 image img, or the caller's image direct_in (of type
-  // a.dirty_type) when given.
+  // a.dirty_type) when given; ld: their row stride (0: a.npix_y).  With
+  // vis_acc the visibilities are added to vis_out (inactive ones untouched)
+  // instead of overwriting it.
   void degrid_core(const wsg_args &a, const Staged &s, const double *img, void *vis_out,
-                   const void *direct_in = nullptr);
+                   const void *direct_in = nullptr, size_t ld = 0, bool vis_acc = false);
   void degrid_from_image(const wsg_args &a, const Staged &s, const double *img, void *vis,
-                         size_t vbytes);
+                         size_t vbytes, bool tuned = false);
+
+  // The tuned schedule (ducc0's ms2dirty_tuning / dirty2ms_tuning,
+  // wgridder.h:1781-1877): the subdivision of tuning_choice, each part run
+  // through grid_core / degrid_core into its facet of the image.  Odd image
+  // sizes are accepted as the reference's tuned calls accept them.
+  void ms2dirty_tuning(const wsg_args &a, const void *vis, void *dirty, int accumulate);
+  void dirty2ms_tuning(const wsg_args &a, const void *dirty, void *vis);
+  template <typename R>
+  bool grid_tuned(const wsg_args &a, const Staged &s, double *img, bool accumulate,
+                  void *direct_out);
+  template <typename R>
+  void degrid_tuned(const wsg_args &a, const Staged &s, const double *img, void *vis_out,
+                    const void *direct_in);
+  TuningChoice last_tuning;  // the subdivision of the last tuned call
+  bool tuned_call = false;   // ms2dirty / dirty2ms run the tuned schedule
+  // odd image sizes: the field centre the reference's subdivision rule sees
+  // for the padded image (it differs from the centre used for gridding)
+  bool tune_center_set = false;
+  double tune_center_x = 0, tune_center_y = 0;
 
   // Pipelined raw operators (wsg_ctx_set_async): wsg_ms2dirty / wsg_dirty2ms
   // stage their inputs through three slots on a copy stream and write host
@@ -161,6 +183,10 @@ class Context {
   void fft_exec(cufftHandle h, void *in, void *out, int dir, bool dbl);
   void record_stats(const GridPlan &g, bool gridding, size_t P);
   void check_device_error(const int *d_err);
+  // the |w| histogram of the masked-in visibilities and the subdivision it
+  // gives; for a w cut, the masks of the two parts in b_mhi / b_mlo
+  TuningChoice tuning_for(const wsg_args &a, const Staged &s);
+  DevBuf b_tune, b_tfovc, b_mhi, b_mlo, b_pad;
   void print_report(const GridPlan &g, bool gridding, size_t P);
   void mark(const char *what);
   void print_marks(const char *title);

@@ -1756,10 +1756,94 @@ __global__ void k_weights_apply(size_t nrows, int nchan, int npol, const double 
   }
 }
 
+// ------------------------------------------------- tuned schedule (w split)
+//
+// The |w| statistics behind the tuned schedule's choice of a w cut and
+// facets (get_winfo, wgridder.cc:28-89): the range of |w f/c| over the
+// masked-in visibilities, a histogram of NBIN equal bins over that range,
+// and the split of the mask into the visibilities below and at or above the
+// cut bin.  A visibility's bin is min(floor((|w f/c| - wmin) * xdw), NBIN-1)
+// with xdw = NBIN / (wmax - wmin), as the reference computes it.
+
+__global__ void k_wrange(size_t nrows, int nchan, const double *__restrict__ uvw,
+                         const double *__restrict__ fovc, const uint8_t *__restrict__ mask,
+                         unsigned long long *out /* [0] min bits, [1] max bits, [2] count */) {
+  double lo = 1e300, hi = 0;
+  unsigned long long cnt = 0;
+  for (size_t r = blockIdx.x * size_t(blockDim.x) + threadIdx.x; r < nrows;
+       r += size_t(gridDim.x) * blockDim.x) {
+    const double w = uvw[3 * r + 2];
+    for (int c = 0; c < nchan; ++c) {
+      if (mask && !mask[r * nchan + c]) continue;
+      const double aw = fabs(w * fovc[c]);
+      lo = fmin(lo, aw);
+      hi = fmax(hi, aw);
+      ++cnt;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+  }
+  if ((threadIdx.x & 31) == 0 && cnt > 0) {
+    atomicMin(&out[0], (unsigned long long)__double_as_longlong(lo));
+    atomicMax(&out[1], (unsigned long long)__double_as_longlong(hi));
+    atomicAdd(&out[2], cnt);
+  }
+}
+
+constexpr int kTuneBins = 50;
+
+__device__ __forceinline__ int w_bin(double aw, double wmin, double xdw) {
+  const double x = (aw - wmin) * xdw;
+  const unsigned long long b = (unsigned long long)x;  // x >= 0
+  return int(b < (unsigned long long)(kTuneBins - 1) ? b : (unsigned long long)(kTuneBins - 1));
+}
+
+__global__ void k_whist(size_t nrows, int nchan, const double *__restrict__ uvw,
+                        const double *__restrict__ fovc, const uint8_t *__restrict__ mask,
+                        double wmin, double xdw, unsigned long long *hist) {
+  __shared__ unsigned int h[kTuneBins];
+  for (int i = threadIdx.x; i < kTuneBins; i += blockDim.x) h[i] = 0;
+  __syncthreads();
+  for (size_t r = blockIdx.x * size_t(blockDim.x) + threadIdx.x; r < nrows;
+       r += size_t(gridDim.x) * blockDim.x) {
+    const double w = uvw[3 * r + 2];
+    for (int c = 0; c < nchan; ++c) {
+      if (mask && !mask[r * nchan + c]) continue;
+      atomicAdd(&h[w_bin(fabs(w * fovc[c]), wmin, xdw)], 1u);
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < kTuneBins; i += blockDim.x)
+    if (h[i]) atomicAdd(&hist[i], (unsigned long long)h[i]);
+}
+
+// hi[k] = mask_k and bin >= icut; lo[k] = mask_k and bin < icut
+__global__ void k_wsplit(size_t nrows, int nchan, const double *__restrict__ uvw,
+                         const double *__restrict__ fovc, const uint8_t *__restrict__ mask,
+                         double wmin, double xdw, int icut, uint8_t *__restrict__ hi,
+                         uint8_t *__restrict__ lo) {
+  for (size_t r = blockIdx.x * size_t(blockDim.x) + threadIdx.x; r < nrows;
+       r += size_t(gridDim.x) * blockDim.x) {
+    const double w = uvw[3 * r + 2];
+    for (int c = 0; c < nchan; ++c) {
+      const size_t k = r * nchan + c;
+      const bool in = !mask || mask[k];
+      const bool up = in && w_bin(fabs(w * fovc[c]), wmin, xdw) >= icut;
+      hi[k] = up ? 1 : 0;
+      lo[k] = (in && !up) ? 1 : 0;
+    }
+  }
+}
+
 // ------------------------------------------------------------- screens
 
 struct ScreenArgs {
   int nx, ny, nu, nv;
+  size_t ld;                // row stride of the x-major image (ny, or the full
+                            // image's ny for a facet inside a larger image)
   double px, py, x0, y0;
   double nshift, dw, wmin;
   int do_w, divide_by_n;
@@ -1871,7 +1955,7 @@ __global__ void __launch_bounds__(256) k_screen_add(ScreenArgs s, const void *Hv
   for (int k = 0; k < 4; ++k) {
     const int ii = i0 + ty + 8 * k, jj = j0 + tx;
     if (ii < s.nx && jj < s.ny) {
-      const size_t o = size_t(ii) * s.ny + jj;
+      const size_t o = size_t(ii) * s.ld + jj;
       const double x = tile[tx][ty + 8 * k];
       if (out_mode == 0)
         img[o] += x;
@@ -1897,7 +1981,7 @@ __global__ void __launch_bounds__(256) k_screen_put(ScreenArgs s, const void *im
     const int ii = i0 + ty + 8 * k, jj = j0 + tx;
     double x = 0.0;
     if (ii < s.nx && jj < s.ny) {
-      const size_t o = size_t(ii) * s.ny + jj;
+      const size_t o = size_t(ii) * s.ld + jj;
       x = in_f32 ? double(reinterpret_cast<const float *>(img)[o])
                  : reinterpret_cast<const double *>(img)[o];
     }

@@ -139,8 +139,11 @@ struct GridPlan {
 // Parameter choice (the analogue of ducc0 Params::getNuNv, wgridder.h:1503-1576,
 // and the w-plane placement of countRanges, wgridder.h:690-699).  The cost
 // model is this implementation's own, calibrated for the B200 kernels.
-// pow2_v: restrict nv to a power of two (for the FFT along v by the
-// library's own shared-memory kernel instead of cuFFT).
+// pow2_v: restrict nv to a power of two no larger than kPow2VMax (for the FFT
+// along v by the library's own shared-memory kernel instead of cuFFT, whose
+// lengths run from 256 to 8192); kernels that would need a longer nv are
+// skipped.
+constexpr size_t kPow2VMax = 8192;
 void choose_grid(GridPlan &g, double sigma_min, double sigma_max, int tile, bool pow2_v = false);
 
 // The n cheapest kernels (W, sigma) for these inputs by the cost model of
@@ -151,6 +154,35 @@ std::vector<std::pair<int, double>> rank_kernels(const GridPlan &g, double sigma
 // Shared memory of a spread / interpolation CTA for tile T and support W.
 constexpr size_t kMaxSmemPerBlock = 227 * 1024;
 size_t tile_smem_bytes(int T, int W, bool fp32);
+
+// The tuned schedule's subdivision (ducc0's ms2dirty_tuning / dirty2ms_tuning,
+// wgridder.h:1781-1877, with the choice of get_tuning_parameters,
+// wgridder.cc:144-278): either no subdivision, or nfx x nfy facets (each
+// gridded with its own phase centre) of the visibilities whose |w| bin is at
+// least icut, plus -- when icut > 0 -- the visibilities below the cut gridded
+// on the whole image.  The rule is the reference's, restated, so that a tuned
+// call subdivides the way the reference does; the results equal the plain
+// operator's within epsilon whatever the subdivision.
+struct TuningChoice {
+  int nfx = 0, nfy = 0;   // 0: no facets
+  int icut = 0;           // first |w| bin of the faceted part (0: all of them)
+  double wmin = 0, wmax = 0;
+  bool split() const { return nfx > 0; }
+};
+constexpr int kTuningBins = 50;
+// hist: visibility counts of the kTuningBins |w| bins over [wmin, wmax]
+// (masked-in visibilities only), nvis_all = nrows * nchan.
+TuningChoice tuning_choice(size_t npix_x, size_t npix_y, double pixsize_x, double pixsize_y,
+                           double epsilon, bool do_w, double center_x, double center_y,
+                           size_t nvis_all, double wmin, double wmax, const uint64_t *hist);
+// Facet (ifx, ify) of an nfx x nfy subdivision (get_facet_data,
+// wgridder.cc:92-108): pixel range [x0, x1) x [y0, y1) and phase centre.
+struct Facet {
+  size_t x0, y0, x1, y1;
+  double cx, cy;
+};
+Facet tuning_facet(size_t npix_x, size_t npix_y, int nfx, int nfy, int ifx, int ify,
+                   double pixsize_x, double pixsize_y, double center_x, double center_y);
 
 // Nominal device bytes for one pass with `planes` planes resident.
 size_t plan_bytes(const GridPlan &g, size_t planes, bool gridding);

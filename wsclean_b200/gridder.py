@@ -116,6 +116,11 @@ class Context:
         L.check(L.lib().wsg_get_stats(self._h, ctypes.byref(s)))
         return s.as_dict()
 
+    def last_tuning(self):
+        """Subdivision of the last tuned call: dict(nfx, nfy, icut, wcut);
+        nfx == 0 when the plain operator ran (wsg_get_tuning)."""
+        return _tuning_of(self._h)
+
     def _args(self, uvw, freq, nrows, nchan, wgt, mask, npix_x, npix_y, pixsize_x, pixsize_y,
               epsilon, do_wgridding, negate_v, divide_by_n, sigma_min, sigma_max, center_x,
               center_y, precision, vis_type, dirty_type, keep):
@@ -151,7 +156,10 @@ class Context:
     def ms2dirty(self, uvw, freq, vis, npix_x, npix_y, pixsize_x, pixsize_y, epsilon,
                  do_wgridding=True, wgt=None, mask=None, negate_v=False, divide_by_n=True,
                  sigma_min=1.1, sigma_max=2.6, center_x=0.0, center_y=0.0,
-                 precision="mixed", dirty=None, accumulate=False, dirty_dtype=None):
+                 precision="mixed", dirty=None, accumulate=False, dirty_dtype=None,
+                 tuning=False):
+        """ducc0::ms2dirty (tuning=True: ms2dirty_tuning, the subdivided
+        schedule of -gridder tuned-wgridder; odd image sizes allowed)."""
         keep = []
         v, vp, vdt, vcuda = _prep(vis)
         if vdt not in _NP_C:
@@ -173,7 +181,8 @@ class Context:
                        epsilon, do_wgridding, negate_v, divide_by_n, sigma_min, sigma_max,
                        center_x, center_y, precision, _NP_C[vdt], _NP_F[ddt], keep)
         self._bind_stream(v, d, *keep)
-        L.check(L.lib().wsg_ms2dirty(self._h, ctypes.byref(a), vp, dp, int(bool(accumulate))))
+        fn = L.lib().wsg_ms2dirty_tuning if tuning else L.lib().wsg_ms2dirty
+        L.check(fn(self._h, ctypes.byref(a), vp, dp, int(bool(accumulate))))
         if getattr(self, "_async", False):
             self._pending = (getattr(self, "_pending", []) + [(keep, d)])[-4:]
         return d
@@ -205,7 +214,8 @@ class Context:
     def dirty2ms(self, uvw, freq, dirty, pixsize_x, pixsize_y, epsilon, do_wgridding=True,
                  wgt=None, mask=None, negate_v=False, divide_by_n=True, sigma_min=1.1,
                  sigma_max=2.6, center_x=0.0, center_y=0.0, precision="mixed",
-                 vis=None, vis_dtype=np.complex64):
+                 vis=None, vis_dtype=np.complex64, tuning=False):
+        """ducc0::dirty2ms (tuning=True: dirty2ms_tuning)."""
         keep = []
         d, dp, ddt, dcuda = _prep(dirty)
         if ddt not in _NP_F:
@@ -225,10 +235,18 @@ class Context:
                        epsilon, do_wgridding, negate_v, divide_by_n, sigma_min, sigma_max,
                        center_x, center_y, precision, _NP_C[vdt], _NP_F[ddt], keep)
         self._bind_stream(d, v, *keep)
-        L.check(L.lib().wsg_dirty2ms(self._h, ctypes.byref(a), dp, vp))
+        fn = L.lib().wsg_dirty2ms_tuning if tuning else L.lib().wsg_dirty2ms
+        L.check(fn(self._h, ctypes.byref(a), dp, vp))
         if getattr(self, "_async", False):
             self._pending = (getattr(self, "_pending", []) + [(keep, v)])[-4:]
         return v
+
+
+def _tuning_of(ctx_handle):
+    nfx, nfy, icut, wcut = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+    L.check(L.lib().wsg_get_tuning(ctx_handle, ctypes.byref(nfx), ctypes.byref(nfy),
+                                   ctypes.byref(icut), ctypes.byref(wcut)))
+    return dict(nfx=nfx.value, nfy=nfy.value, icut=icut.value, wcut=wcut.value)
 
 
 def _precision(p):
@@ -347,6 +365,10 @@ class WGriddingGridder:
         s = L.WsgStats()
         L.check(L.lib().wsg_get_stats(L.lib().wsg_gridder_ctx(self._h), ctypes.byref(s)))
         return s.as_dict()
+
+    def last_tuning(self):
+        """Subdivision of the last tuned call (gridders made with tuning=True)."""
+        return _tuning_of(L.lib().wsg_gridder_ctx(self._h))
 
 
 def plan_grid(npix_x, npix_y, pixsize_x, pixsize_y, epsilon, nvis, wmin, wmax, umax, vmax=None,
