@@ -41,12 +41,40 @@ sys.path.insert(0, HERE)
 METRIC = "Mvis/s ms2dirty+dirty2ms @4096²: FP32-mixed vs FP64 GPU, rel err vs FP64 DFT"
 UNIT = "Mvis/s"
 EPS_MIXED, EPS_FP64 = 1e-5, 1e-12
-# Grid chosen by the reference (ducc0) for this workload, from its verbosity-1
-# report (oracle/_ref run on the same seeded data): mixed eps 1e-5 -> 7392^2 x
-# 14 planes; FP64 eps 1e-12 -> 7392^2 x 22 planes.  Used only for the
-# algorithmic-bytes roofline so that it does not depend on this library's
-# own (smaller) grid choice.
-DUCC_GRID = {"mixed": (7392, 7392, 14), "fp64": (7392, 7392, 22)}
+# WSClean's call pattern of the reference w-gridder (wgriddinggridder_simple.cpp:56-58)
+CALL = "negate_v, no divide_by_n, sigma 1.1..2.0"
+GRIDS_PATH = os.path.join(HERE, "tests", "golden", "ducc_grids.json")
+
+
+def ducc_grids():
+    """The grids the reference (ducc0) chooses for the benchmark workloads,
+    from its verbosity-1 report on the same seeded data
+    (tests/golden/make_ducc_grids.py).  The roofline charges their
+    algorithmic bytes, so that it does not depend on this library's own
+    (smaller, band-pruned) grid choice."""
+    with open(GRIDS_PATH) as fh:
+        return json.load(fh)
+
+
+def grid_tuple(g):
+    return (int(g["nu"]), int(g["nv"]), int(g["nplanes"]))
+
+
+def peak_hbm():
+    path = os.path.join(HERE, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def roofline(bytes_per_step, ms_per_step, kernel):
+    """HBM roofline of a workload: algorithmic bytes (the reference's grid,
+    the build plan's formula) over the measured time."""
+    peak, src = peak_hbm()
+    achieved = bytes_per_step / (ms_per_step / 1e3) / 1e9
+    return {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": src, "bytes_per_step": int(bytes_per_step)}
 
 
 def parse_args():
@@ -61,6 +89,9 @@ def parse_args():
                     help="do not sample nvidia-smi during the timed region")
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the config-4 batched-facets measurement")
+    ap.add_argument("--legs", default="1,3,4,5",
+                    help="the other configurations to measure after the headline "
+                         "(comma list of 1, 3, 4, 5; empty for none)")
     ap.add_argument("--timed-only", action="store_true",
                     help="stop after the timed region (for profiler launch lists)")
     ap.add_argument("--scale", type=float, default=1.0,
@@ -219,6 +250,13 @@ def dist_setup(args):
     return world, rank, local, pg
 
 
+def config2_dict(nvis, nx, world):
+    """The workload description both arms print (the same dict)."""
+    return {"workload": "config-2 adjoint pair: 8.1M vis, 4096^2 @ 5\", eps 1e-5",
+            "nvis": nvis, "npix": nx, "call": CALL, "parallelism": f"replicas x{world}",
+            "l2": "inputs and grids larger than L2 (uvw 194 MB, grids GBs)"}
+
+
 def run_reference(args, world, rank):
     """The reference's CPU w-gridder (compiled ducc0) on the same workload."""
     if rank != 0:
@@ -257,9 +295,8 @@ def run_reference(args, world, rank):
         "steps": len(ts), "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(ts),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded Earth-rotation observation, 200 point sources)",
-        "config": {"workload": "config-2 adjoint pair: 8.1M vis, 4096^2 @ 5\", eps 1e-5",
-                   "nvis": nvis, "npix": nx, "instance": "ducc0 <float,float>",
-                   "wsclean_args": "negate_v, no divide_by_n, sigma 1.1..2.0"},
+        "config": config2_dict(nvis, nx, world),
+        "instance": "ducc0 <float,float>",
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
                          "sample": "full workload per step (one ms2dirty + one dirty2ms)"},
@@ -268,12 +305,134 @@ def run_reference(args, world, rank):
     print(json.dumps(out))
 
 
+KW = dict(negate_v=True, divide_by_n=False, sigma_min=1.1, sigma_max=2.0)
+KW_REF = dict(KW, nthreads=0)
+
+
+def device_timed(torch, dev, fns, steps, warmup):
+    """Mean device time (ms) of each synchronous library call in fns, by CUDA
+    events on torch's current stream (the calls are ordered on it)."""
+    st = torch.cuda.current_stream(dev)
+    for _ in range(warmup):
+        for f in fns:
+            f()
+    torch.cuda.synchronize(dev)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(fns) + 1)]
+    tot = [0.0] * len(fns)
+    for _ in range(steps):
+        ev[0].record(st)
+        for i, f in enumerate(fns):
+            f()
+            ev[i + 1].record(st)
+        torch.cuda.synchronize(dev)
+        for i in range(len(fns)):
+            tot[i] += ev[i].elapsed_time(ev[i + 1])
+    return [t / steps for t in tot]
+
+
+def cpu_pair(uvw, freq, vis, model, nx, px, eps, prec, wgt=None, sample=""):
+    """The reference's CPU w-gridder (oracle/_ref, all host threads) on one
+    ms2dirty + dirty2ms, with its grid choice from the verbosity report."""
+    import oracle as O
+    if not O.ref_available():
+        return None, None
+    t0 = time.perf_counter()
+    _, rep = O.ref_ms2dirty(uvw, freq, vis, nx, nx, px, px, eps, prec=prec, wgt=wgt,
+                            return_report=True, **KW_REF)
+    t1 = time.perf_counter()
+    O.ref_dirty2ms(uvw, freq, model, px, px, eps, prec=prec, wgt=wgt, vis_dtype=vis.dtype, **KW_REF)
+    t2 = time.perf_counter()
+    nvis = vis.size
+    return ({"value": nvis / (t2 - t0) / 1e6, "unit": UNIT, "cores": os.cpu_count(),
+             "kind": "reference", "ms2dirty_mvis_s": nvis / (t1 - t0) / 1e6,
+             "dirty2ms_mvis_s": nvis / (t2 - t1) / 1e6,
+             "sample": sample or "full workload, one ms2dirty + one dirty2ms"},
+            O.parse_report(rep)[0])
+
+
+def leg_config1(torch, dev, ctx, grids, with_cpu):
+    """Config 1: plain FP64 (complex128) pair at epsilon 1e-12, 1024^2 at 10",
+    2.9M visibilities -- the form of WSClean's own CPU path."""
+    from wsclean_b200 import synth
+    c = synth.config1()
+    uvw, freq, nx, px = c["uvw"], c["freq"], c["npix_x"], c["pixsize"]
+    rng = np.random.default_rng(1)
+    ix, iy, flux = synth.point_sky(c["nsrc"], nx, nx, rng)
+    vis = synth.predict_vis(uvw, freq, nx, nx, px, px, ix, iy, flux, device=dev)
+    vis = vis + 0.1 * (rng.normal(size=vis.shape) + 1j * rng.normal(size=vis.shape))
+    model = synth.sky_image(nx, nx, ix, iy, flux)
+    nrows, nvis = uvw.shape[0], vis.size
+    tu, tf = torch.as_tensor(uvw, device=dev), torch.as_tensor(freq, device=dev)
+    tv, tm = torch.as_tensor(vis, device=dev), torch.as_tensor(model, device=dev)
+    d = torch.zeros((nx, nx), dtype=torch.float64, device=dev)
+    o = torch.zeros(vis.shape, dtype=torch.complex128, device=dev)
+    eps = 1e-12
+    t1, t2 = device_timed(torch, dev, [
+        lambda: ctx.ms2dirty(tu, tf, tv, nx, nx, px, px, eps, precision="fp64", dirty=d, **KW),
+        lambda: ctx.dirty2ms(tu, tf, tm, px, px, eps, precision="fp64", vis=o, **KW)], 5, 2)
+    st = ctx.stats()
+    pix = rng.integers(0, nx * nx, 16)
+    acc = {"ms2dirty_rel_rms_vs_dft":
+           rel_rms(d.cpu().numpy().ravel()[pix], dft_pixels(uvw, freq, vis, nx, nx, px, px, pix,
+                                                            torch, dev))}
+    cpu, g = cpu_pair(uvw, freq, vis, model, nx, px, eps, "double") if with_cpu else (None, None)
+    g = g or grids["config1"]["fp64"]
+    B = 2 * algorithmic_bytes(nvis, nrows, nx, nx, grid_tuple(g), 16, 16)
+    return {"workload": "config 1: 64 antennas within 3 km, 360 x 10 s, 4 channels, 2.9M complex128 "
+                        "visibilities, 1024^2 at 10\", FP64 at eps 1e-12",
+            "nvis": nvis, "ms2dirty_mvis_s": nvis / t1 / 1e3, "dirty2ms_mvis_s": nvis / t2 / 1e3,
+            "value": nvis / (t1 + t2) / 1e3, "ms_per_step": t1 + t2,
+            "grid": {"nu": st["nu"], "nv": st["nv"], "nplanes": st["nplanes"], "W": st["supp"]},
+            "reference_grid": g, "roofline": roofline(B, t1 + t2, "FP64 pair"),
+            "accuracy": acc, "cpu_baseline": cpu}
+
+
+def leg_config3(torch, dev, ctx, grids, with_cpu):
+    """Config 3: the chi^2-gradient pair (one dirty2ms of the model, one
+    ms2dirty of the weighted residuals) at 2048^2 / 8" on the config-2 array,
+    Briggs robust-0 times U[0.5, 2] noise weights, mixed at eps 1e-5."""
+    from wsclean_b200 import synth
+    c = synth.config3()
+    uvw, freq, nx, px = c["uvw"], c["freq"], c["npix_x"], c["pixsize"]
+    rng = np.random.default_rng(3)
+    ix, iy, flux = synth.point_sky(c["nsrc"], nx, nx, rng)
+    vis = synth.predict_vis(uvw, freq, nx, nx, px, px, ix, iy, flux, device=dev)
+    noise = rng.uniform(0.5, 2.0, vis.shape)
+    w = (noise * synth.briggs_weights(uvw, freq, nx, nx, px, px, robust=0.0,
+                                      noise_weights=noise)).astype(np.float32)
+    model = synth.sky_image(nx, nx, ix, iy, flux)
+    model = (model * (1 + 0.05 * rng.normal(size=model.shape))).astype(np.float32)
+    nrows, nvis = uvw.shape[0], vis.size
+    tu, tf = torch.as_tensor(uvw, device=dev), torch.as_tensor(freq, device=dev)
+    tv = torch.as_tensor(vis.astype(np.complex64), device=dev)
+    tw, tm = torch.as_tensor(w, device=dev), torch.as_tensor(model, device=dev)
+    d = torch.zeros((nx, nx), dtype=torch.float32, device=dev)
+    o = torch.zeros(vis.shape, dtype=torch.complex64, device=dev)
+    eps = 1e-5
+    t2, t1 = device_timed(torch, dev, [
+        lambda: ctx.dirty2ms(tu, tf, tm, px, px, eps, wgt=tw, vis=o, **KW),
+        lambda: ctx.ms2dirty(tu, tf, tv, nx, nx, px, px, eps, wgt=tw, dirty=d, **KW)], 10, 3)
+    st = ctx.stats()
+    cpu, g = (cpu_pair(uvw, freq, vis.astype(np.complex64), model, nx, px, eps, "float", wgt=w)
+              if with_cpu else (None, None))
+    g = g or grids["config3"]["mixed"]
+    B = 2 * algorithmic_bytes(nvis, nrows, nx, nx, grid_tuple(g), 8, 8) + 2 * nvis * 4
+    return {"workload": "config 3: chi^2 gradient pair, config-2 array (8.1M vis) at 2048^2 / 8\", "
+                        "Briggs(0) x U[0.5,2] weights, mixed at eps 1e-5",
+            "nvis": nvis, "ms2dirty_mvis_s": nvis / t1 / 1e3, "dirty2ms_mvis_s": nvis / t2 / 1e3,
+            "value": nvis / (t1 + t2) / 1e3, "ms_per_step": t1 + t2,
+            "grid": {"nu": st["nu"], "nv": st["nv"], "nplanes": st["nplanes"], "W": st["supp"]},
+            "reference_grid": g, "roofline": roofline(B, t1 + t2, "mixed pair with weights"),
+            "cpu_baseline": cpu}
+
+
 def run_batched(dev, torch, ctx, args):
     """Config 4: 16 Voronoi facets x 8 output channels (8 of 64 input
     channels each) = 128 jobs over the same rows, gridded and degridded
     through one reusable plan (one persistent spread / interpolation launch
     per call, replayed as a CUDA graph), against the plain FP64 form run job
-    by job (timed on the first 16 jobs and scaled to all 128)."""
+    by job over all 128 jobs, at the mixed form's epsilon (1e-5, the same
+    stated accuracy) and at 1e-12."""
     from wsclean_b200 import synth
     from wsclean_b200 import gridder as G
     c = synth.config4()
@@ -282,7 +441,7 @@ def run_batched(dev, torch, ctx, args):
     jobs = [dict(npix_x=f["nx"], npix_y=f["ny"], center_x=f["dx"] * px, center_y=f["dy"] * px,
                  chan_begin=8 * oc, chan_end=8 * oc + 8)
             for oc in range(8) for f in synth.facets4()]
-    kw = dict(negate_v=True, divide_by_n=False, sigma_min=1.1, sigma_max=2.0)
+    kw = KW
     g = torch.Generator(device=dev).manual_seed(7)
     vis = torch.complex(torch.randn(nrows, 64, device=dev, generator=g),
                         torch.randn(nrows, 64, device=dev, generator=g))
@@ -315,33 +474,180 @@ def run_batched(dev, torch, ctx, args):
     W = plan.stats(0)["supp"]
     plan.close()
     del dirty, pred, models
-    # plain FP64 form, job by job
+    # plain FP64 form, job by job over all 128 jobs (a first pass creates the
+    # FFT plans of each facet size and is not timed)
     vis64 = vis.to(torch.complex128)
     del vis
     tu = torch.as_tensor(uvw, device=dev)
     tf = torch.as_tensor(freq, device=dev)
-    sub = jobs[:16]
-    t64 = 0.0
-    for rep in range(2):   # the first pass creates the FFT plans of each facet size
-        torch.cuda.synchronize(dev)
-        t0 = time.perf_counter()
-        for j in sub:
-            c0, c1 = j["chan_begin"], j["chan_end"]
-            ctx.ms2dirty(tu, tf[c0:c1], vis64[:, c0:c1].contiguous(), j["npix_x"], j["npix_y"],
-                         px, px, EPS_FP64, precision="fp64", center_x=j["center_x"],
-                         center_y=j["center_y"], dirty_dtype=np.float64, **kw)
-        torch.cuda.synchronize(dev)
-        t64 = (time.perf_counter() - t0) / len(sub) * len(jobs) * 1e3
+    chans = [vis64[:, 8 * oc:8 * oc + 8].contiguous() for oc in range(8)]
     del vis64
+
+    def per_job(eps, timed_jobs):
+        for rep in range(2):
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            for j in (timed_jobs if rep else timed_jobs[:16]):
+                c0, c1 = j["chan_begin"], j["chan_end"]
+                ctx.ms2dirty(tu, tf[c0:c1], chans[c0 // 8], j["npix_x"], j["npix_y"], px, px, eps,
+                             precision="fp64", center_x=j["center_x"], center_y=j["center_y"],
+                             dirty_dtype=np.float64, **kw)
+            torch.cuda.synchronize(dev)
+            t = (time.perf_counter() - t0) * 1e3
+        return t
+
+    t64 = per_job(EPS_FP64, jobs)
+    t64e = per_job(EPS_MIXED, jobs)
+    del chans
+    cycles = 10
     return {"workload": "config 4: 96 antennas within 10 km, 360 x 10 s, 64 channels 120-180 MHz; "
                         "16 Voronoi facets (512^2..2048^2, phase centre at the box centre) x 8 "
                         "output channels = 128 jobs",
             "rows": nrows, "job_visibilities": jv, "plan_build_s": t_build, "W": W,
             "mixed_ms2dirty_ms": tg, "mixed_dirty2ms_ms": td,
             "mixed_ms2dirty_mvis_s": jv / tg / 1e3, "mixed_dirty2ms_mvis_s": jv / td / 1e3,
+            "mixed_pair_mvis_s": jv / (tg + td) / 1e3,
+            "mixed_pair_mvis_s_with_build_over_%d_cycles" % cycles:
+                jv / (tg + td + t_build * 1e3 / cycles) / 1e3,
             "fp64_per_job_ms2dirty_ms": t64, "fp64_per_job_ms2dirty_mvis_s": jv / t64 / 1e3,
+            "fp64_per_job_eps_1e-5_ms2dirty_ms": t64e,
+            "fp64_per_job_eps_1e-5_ms2dirty_mvis_s": jv / t64e / 1e3,
             "mixed_batched_over_fp64_per_job": t64 / tg,
-            "fp64_timing": "16 of 128 jobs timed (warm FFT plans), scaled to 128"}
+            "mixed_batched_over_fp64_per_job_same_eps": t64e / tg,
+            "fp64_timing": "all 128 jobs timed (warm FFT plans), wall clock with a device sync "
+                           "on both sides; the mixed plan time excludes its build (reported "
+                           "beside it, and amortised over %d major cycles)" % cycles}
+
+
+def leg_config5(torch, dev, ctx, grids, with_cpu, args):
+    """Config 5: 522M visibilities (256 antennas, 1000 x 8 s, 16 channels)
+    at 8192^2 / 2", streamed from page-locked host memory in 256 MiB chunks
+    through wsg_stream_*: dirty2ms of the sky model (2000 point sources and 5
+    Gaussians) chunk by chunk, then ms2dirty of those visibilities.  Also the
+    same with the chunks resident in HBM (no host copies), the plain
+    host-to-device copy time of the data, the tuned schedule against the
+    plain one on a 2% time subsample, and the reference on 30% of the data."""
+    from wsclean_b200 import synth
+    from wsclean_b200 import gridder as G
+    c = synth.config5()
+    uvw, freq, nx, px = c["uvw"], c["freq"], c["npix_x"], c["pixsize"]
+    nrows, nchan = uvw.shape[0], len(freq)
+    nvis = nrows * nchan
+    rng = np.random.default_rng(5)
+    ix, iy, flux = synth.point_sky(c["nsrc"], nx, nx, rng)
+    model = synth.sky_image(nx, nx, ix, iy, flux) + synth.gaussian_blobs(nx, nx, c["ngauss"], rng)
+    model32 = model.astype(np.float32)
+    rows = (256 << 20) // (24 + 8 * nchan)
+    bounds = list(range(0, nrows, rows)) + [nrows]
+    parts = list(zip(bounds[:-1], bounds[1:]))
+    h_uvw = torch.as_tensor(uvw).pin_memory()
+    h_vis = torch.empty((nrows, nchan), dtype=torch.complex64).pin_memory()
+    h_model = torch.as_tensor(model32).pin_memory()
+    h_dirty = torch.empty((nx, nx), dtype=torch.float32).pin_memory()
+    ext = G.data_extent(uvw, freq)
+    out = {"workload": "config 5: 256 antennas (log-radial to 20 km), 1000 x 8 s, 16 channels "
+                       "140-190 MHz, 522M complex64 visibilities, 8192^2 at 2\", |w| up to 40% "
+                       "of max|uv|, mixed at eps 1e-5, streamed in 256 MiB chunks",
+           "nvis": nvis, "chunks": len(parts)}
+    s = G.Stream(freq, nx, nx, px, px, EPS_MIXED, ext, nvis=nvis, context=ctx, **KW)
+    try:
+        def d2m(src_uvw, dst_vis):
+            s.predict_begin(h_model)
+            for a, b in parts:
+                s.predict(src_uvw[a:b], vis=dst_vis[a:b])
+
+        def m2d(src_uvw, src_vis, dst):
+            for a, b in parts:
+                s.add(src_uvw[a:b], src_vis[a:b])
+            s.finish(dst)
+
+        def wall(f):
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            f()
+            torch.cuda.synchronize(dev)
+            return (time.perf_counter() - t0) * 1e3
+
+        # warm-up on the first chunks (buffers, FFT plans), then one full pass
+        s.predict_begin(h_model)
+        s.predict(h_uvw[:parts[0][1]], vis=h_vis[:parts[0][1]])
+        for a, b in parts[:2]:
+            s.add(h_uvw[a:b], h_vis[a:b])
+        s.finish(h_dirty)
+        t_d2m = wall(lambda: d2m(h_uvw, h_vis))
+        t_m2d = wall(lambda: m2d(h_uvw, h_vis, h_dirty))
+        st = s.stats()
+        # accuracy: dirty2ms on 20k visibilities (1250 rows x 16 channels)
+        # against the FP64 DFT of the model's pixels (torch, on the GPU)
+        sel_rows = rng.choice(nrows, 1250, replace=False)
+        nz = np.flatnonzero(model)
+        vref = synth.predict_vis(uvw[sel_rows], freq, nx, nx, px, px, nz // nx, nz % nx,
+                                 model.ravel()[nz], device=dev)
+        out["accuracy"] = {"dirty2ms_rel_rms_vs_dft_20k": rel_rms(h_vis.numpy()[sel_rows], vref)}
+        pix = np.concatenate([rng.choice(nz, 4, replace=False), rng.integers(0, nx * nx, 4)])
+        out["accuracy"]["ms2dirty_rel_rms_vs_dft_8px"] = rel_rms(
+            h_dirty.numpy().ravel()[pix],
+            dft_pixels(uvw, freq, h_vis.numpy(), nx, nx, px, px, pix, torch, dev))
+        # the same passes with the data resident in HBM
+        d_uvw = h_uvw.to(dev)
+        d_vis = h_vis.to(dev)
+        d_dirty = torch.empty((nx, nx), dtype=torch.float32, device=dev)
+        d_out = torch.empty_like(d_vis)
+        r_d2m = wall(lambda: d2m(d_uvw, d_out))
+        r_m2d = wall(lambda: m2d(d_uvw, d_vis, d_dirty))
+        del d_out, d_dirty
+        # plain copies of what the streamed passes move to the device
+        t_h2d = wall(lambda: [d_vis[a:b].copy_(h_vis[a:b], non_blocking=True) for a, b in parts]
+                     + [d_uvw[a:b].copy_(h_uvw[a:b], non_blocking=True) for a, b in parts])
+        del d_uvw, d_vis
+    finally:
+        s.close()
+    torch.cuda.empty_cache()
+    g = grids["config5"]["mixed"]
+    B = 2 * algorithmic_bytes(nvis, nrows, nx, nx, grid_tuple(g), 8, 8)
+    h2d = 2 * h_uvw.numel() * 8 + h_vis.numel() * 8 + h_model.numel() * 4
+    d2h = h_vis.numel() * 8 + h_dirty.numel() * 4
+    out.update({
+        "ms2dirty_mvis_s": nvis / t_m2d / 1e3, "dirty2ms_mvis_s": nvis / t_d2m / 1e3,
+        "value": nvis / (t_m2d + t_d2m) / 1e3, "ms_per_step": t_m2d + t_d2m,
+        "resident_ms2dirty_mvis_s": nvis / r_m2d / 1e3, "resident_dirty2ms_mvis_s": nvis / r_d2m / 1e3,
+        "resident_value": nvis / (r_m2d + r_d2m) / 1e3,
+        "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+        "h2d_copy_alone_ms": t_h2d,
+        "h2d_hidden_fraction": max(0.0, min(1.0, (r_m2d + t_h2d - t_m2d) / t_h2d)),
+        "grid": {"nu": st["nu"], "nv": st["nv"], "nplanes": st["nplanes"], "W": st["supp"],
+                 "u_band_rows": st["band_rows"]},
+        "reference_grid": g, "roofline": roofline(B, t_m2d + t_d2m, "streamed pair"),
+        "timing": "wall clock around each full pass (every call returns once its results are in "
+                  "place), device synchronised on both sides"})
+    # the reference on the first 30% of the timesteps (its FFT work is fixed
+    # and its gridding work follows the visibilities: a small sample would
+    # understate its rate at full size)
+    cpu = None
+    if with_cpu:
+        r30 = int(0.3 * nrows) // 32640 * 32640
+        cpu, _ = cpu_pair(uvw[:r30], freq, h_vis.numpy()[:r30], model32, nx, px, EPS_MIXED,
+                          "float", sample="first 300 of 1000 timesteps (156.7M visibilities) of "
+                                          "the same data, one ms2dirty + one dirty2ms of ducc0 "
+                                          "<float,float>")
+    del h_vis, h_uvw
+    # tuned against plain on a 2% time subsample
+    sub = synth.config5(scale=0.02)
+    su, sf = sub["uvw"], sub["freq"]
+    sv = (rng.normal(size=(len(su), nchan)) + 1j * rng.normal(size=(len(su), nchan))).astype(np.complex64)
+    tu, tf, tv = (torch.as_tensor(su, device=dev), torch.as_tensor(sf, device=dev),
+                  torch.as_tensor(sv, device=dev))
+    dd = torch.empty((nx, nx), dtype=torch.float32, device=dev)
+    tp, tt = device_timed(torch, dev, [
+        lambda: ctx.ms2dirty(tu, tf, tv, nx, nx, px, px, EPS_MIXED, dirty=dd, **KW),
+        lambda: ctx.ms2dirty(tu, tf, tv, nx, nx, px, px, EPS_MIXED, dirty=dd, tuning=True, **KW)],
+        2, 1)
+    out["tuned_vs_plain_2pct"] = {"nvis": sv.size, "plain_ms2dirty_ms": tp, "tuned_ms2dirty_ms": tt,
+                                  "tuned_subdivision": ctx.last_tuning()}
+    del tu, tf, tv, dd
+    ctx.release_buffers()
+    out["cpu_baseline"] = cpu
+    return out
 
 
 def dft_pixels(uvw, freq, vis, nx, ny, px, py, pix, torch, dev):
@@ -569,45 +875,51 @@ def run_ours(args, world, rank, local, pg):
     h2d = 2 * h_uvw.numel() * 8 + h_vis.numel() * 8 + h_model.numel() * 4 + 2 * nchan * 8
     d2h = h_dirty.numel() * 4 + h_out.numel() * 8
 
-    # ---- config 4: batched facets x output channels through one plan
-    batched = None
-    if not args.no_batch:
+    # ---- CPU baseline (reference, rank 0, N=1), with the reference's grid
+    # choice for the roofline from its verbosity report
+    grids = ducc_grids()
+    cpu, ref_grid = None, None
+    with_cpu = rank == 0 and world == 1 and not args.no_cpu_baseline
+    if with_cpu:
         try:
-            batched = run_batched(dev, torch, ctx, args)
-        except Exception as e:  # reported, not fatal
-            batched = {"error": str(e)}
-        torch.cuda.empty_cache()
-
-    # ---- roofline of the pipeline (algorithmic bytes, the reference's grid)
-    B = (algorithmic_bytes(nvis, nrows, nx, nx, DUCC_GRID["mixed"], 8, 8) * 2)
-    achieved = B / (ms_per_step / 1e3) / 1e9
-    peaks_path = os.path.join(HERE, "MEASURED_PEAKS.json")
-    peak, peak_src = 6650.0, "fallback"
-    if os.path.exists(peaks_path):
-        with open(peaks_path) as fh:
-            peak, peak_src = float(json.load(fh)["hbm_gbs"]), "measured"
-
-    # ---- CPU baseline (reference, rank 0, N=1)
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        try:
-            import oracle as O
-            if O.ref_available():
-                cores = os.cpu_count()
-                vis32 = forms["mixed"]["vis"].cpu().numpy()
-                m32 = forms["mixed"]["model"].cpu().numpy()
-                rk = dict(prec="float", negate_v=True, divide_by_n=False, sigma_min=1.1,
-                          sigma_max=2.0, nthreads=cores)
-                t0 = time.perf_counter()
-                O.ref_ms2dirty(uvw, freq, vis32, nx, nx, px, px, EPS_MIXED, **rk)
-                O.ref_dirty2ms(uvw, freq, m32, px, px, EPS_MIXED, **rk)
-                tc = time.perf_counter() - t0
-                cpu = {"value": nvis / tc / 1e6, "unit": UNIT, "cores": cores, "kind": "reference",
-                       "sample": "full workload, one ms2dirty + one dirty2ms, ducc0 <float,float> "
-                                 "at eps 1e-5 with WSClean's arguments"}
+            cpu, ref_grid = cpu_pair(
+                uvw, freq, forms["mixed"]["vis"].cpu().numpy(), forms["mixed"]["model"].cpu().numpy(),
+                nx, px, EPS_MIXED, "float",
+                sample="full workload, one ms2dirty + one dirty2ms, ducc0 <float,float> at eps "
+                       "1e-5 with WSClean's arguments")
         except Exception as e:  # reported, not fatal
             cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"failed: {e}"}
+    ref_grid = ref_grid or grids["config2"]["mixed"]
+
+    # ---- roofline of the pipeline (algorithmic bytes, the reference's grid)
+    B = algorithmic_bytes(nvis, nrows, nx, nx, grid_tuple(ref_grid), 8, 8) * 2
+    rl = roofline(B, ms_per_step, "ms2dirty+dirty2ms pipeline")
+    rl["traffic"] = profiled_traffic()
+    rl["reference_grid"] = ref_grid
+
+    # ---- the other configurations (rank 0 only: they are single-GPU legs)
+    legs = {}
+    want = set(x.strip() for x in args.legs.split(",") if x.strip())
+    if args.no_batch:
+        want.discard("4")
+    del forms, h_vis, h_out, h_model, h_dirty, d_uvw, d_freq
+    ctx.release_buffers()
+    torch.cuda.empty_cache()
+    if rank == 0:
+        for name, fn in (("1", lambda: leg_config1(torch, dev, ctx, grids, with_cpu)),
+                         ("3", lambda: leg_config3(torch, dev, ctx, grids, with_cpu)),
+                         ("4", lambda: run_batched(dev, torch, ctx, args)),
+                         ("5", lambda: leg_config5(torch, dev, ctx, grids, with_cpu, args))):
+            if name not in want:
+                continue
+            try:
+                legs["config" + name] = fn()
+            except Exception as e:  # reported, not fatal
+                legs["config" + name] = {"error": f"{type(e).__name__}: {e}"}
+            ctx.release_buffers()
+            gc.collect()
+            torch.cuda.empty_cache()
 
     if rank == 0:
         out = {
@@ -615,10 +927,8 @@ def run_ours(args, world, rank, local, pg):
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 coords/phase/accumulate)",
             "data": "synthetic (seeded Earth-rotation observation, 200 point sources)",
-            "config": {"workload": "config-2 adjoint pair: 8.1M vis, 4096^2 @ 5\", eps 1e-5",
-                       "nvis": nvis, "npix": nx, "parallelism": f"replicas x{world}",
-                       "l2": "inputs and grids larger than L2 (uvw 194 MB, grids GBs)",
-                       "grid": grid_info},
+            "config": config2_dict(nvis, nx, world),
+            "grid": grid_info,
             "ms2dirty_mvis_s": world * nvis * args.steps / (t_ms / 1e3) / 1e6,
             "dirty2ms_mvis_s": world * nvis * args.steps / (t_dm / 1e3) / 1e6,
             "fp64": fp64,
@@ -631,13 +941,9 @@ def run_ours(args, world, rank, local, pg):
                     "d2h_bytes_per_step": int(d2h),
                     "mode": "pipelined calls (wsg_ctx_set_async), pinned host buffers",
                     "synchronous_calls_value": e2e_sync},
-            "roofline": {"bound": "hbm", "kernel": "ms2dirty+dirty2ms pipeline",
-                         "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": profiled_traffic(),
-                         "peak_source": peak_src,
-                         "bytes_per_step": B},
+            "roofline": rl,
             "cpu_baseline": cpu,
-            "batched_facets": batched,
+            "configs": legs,
             "clocks": clocks,
             "gpu_launches": launches,
         }

@@ -339,13 +339,16 @@ typedef struct wsg_stream wsg_stream;
 int wsg_stream_create(wsg_ctx *ctx, const wsg_args *a, double wmin, double wmax, double umax,
                       double vmax, size_t nvis, wsg_stream **out);
 int wsg_stream_destroy(wsg_stream *s);
-/* Adds nrows rows (uvw nrows x 3, vis nrows x nchan, wgt/mask or NULL). */
+/* Adds nrows rows (uvw nrows x 3, vis nrows x nchan, wgt/mask or NULL).
+ * After a prediction (wsg_stream_predict_begin) the first add starts a new
+ * gridding on a cleared grid, as a major cycle's Invert follows its Predict. */
 int wsg_stream_add(wsg_stream *s, size_t nrows, const double *uvw, const void *vis,
                    const void *wgt, const uint8_t *mask);
 /* Transforms the accumulated grid into dirty (or adds it when accumulate);
  * the stream is then empty again. */
 int wsg_stream_finish(wsg_stream *s, void *dirty, int accumulate);
-/* Loads a model image for prediction. */
+/* Loads a model image for prediction (rows added since the last
+ * wsg_stream_finish are discarded). */
 int wsg_stream_predict_begin(wsg_stream *s, const void *dirty);
 /* Predicts nrows rows into vis (nrows x nchan of vis_type). */
 int wsg_stream_predict(wsg_stream *s, size_t nrows, const double *uvw, void *vis,

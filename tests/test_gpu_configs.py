@@ -17,7 +17,10 @@ headline bench runs config 2):
   over a quarter of the observation;
 * config 5: the 8192^2 / 2" wide-field geometry with |w| up to 40% of
   max|uv| on a 2% time subsample (10.4M visibilities), against the DFT on
-  64 pixels and on a 20k-visibility subsample."""
+  64 pixels and on a 20k-visibility subsample; and at full size (522M
+  visibilities) streamed from page-locked host memory in 256 MiB chunks,
+  predicted from the sky model (2000 point sources and 5 Gaussians) and
+  gridded back, against the DFT on 20k visibilities and on image pixels."""
 import numpy as np
 import pytest
 import torch
@@ -224,3 +227,54 @@ def test_config5_widefield_subsample(G):
     sel = rng.choice(nvis, 20000, replace=False)
     vref = O.dft_dirty2ms(uvw, freq, model, px, px, negate_v=True, divide_by_n=False, select=sel)
     assert O.rel_rms(v.cpu().numpy().ravel()[sel], vref) < 1e-5
+
+
+def _config5_full():
+    """The full config-5 observation in page-locked host memory, the sky
+    model, and the row chunks of 256 MiB of uvw + visibilities each."""
+    from wsclean_b200 import synth
+    c = synth.config5()
+    uvw, freq, nx, px = c["uvw"], c["freq"], c["npix_x"], c["pixsize"]
+    rng = np.random.default_rng(5)
+    ix, iy, flux = synth.point_sky(c["nsrc"], nx, nx, rng)
+    model = synth.sky_image(nx, nx, ix, iy, flux) + synth.gaussian_blobs(nx, nx, c["ngauss"], rng)
+    nchan = len(freq)
+    rows = (256 << 20) // (24 + 8 * nchan)
+    bounds = list(range(0, len(uvw), rows)) + [len(uvw)]
+    return c, uvw, freq, nx, px, model, rng, list(zip(bounds[:-1], bounds[1:]))
+
+
+def test_config5_full_streamed(G):
+    c, uvw, freq, nx, px, model, rng, parts = _config5_full()
+    nrows, nchan = uvw.shape[0], len(freq)
+    assert nrows * nchan == 522_240_000
+    h_uvw = torch.as_tensor(uvw).pin_memory()
+    h_vis = torch.empty((nrows, nchan), dtype=torch.complex64).pin_memory()
+    ext = G.data_extent(uvw, freq)
+    with G.Stream(freq, nx, nx, px, px, 1e-5, ext, nvis=nrows * nchan, dirty_dtype=np.float64,
+                  **KW) as s:
+        # dirty2ms: the visibilities of the sky model, chunk by chunk
+        s.predict_begin(model)
+        for a, b in parts:
+            s.predict(h_uvw[a:b], vis=h_vis[a:b])
+        sel = rng.choice(nrows * nchan, 20000, replace=False)
+        vref = O.dft_dirty2ms(uvw, freq, model, px, px, negate_v=True, divide_by_n=False,
+                              select=sel)
+        vis = h_vis.numpy()
+        assert O.rel_rms(vis.ravel()[sel], vref) < 1e-5
+        # ms2dirty of those visibilities, streamed back in the same chunks
+        for a, b in parts:
+            s.add(h_uvw[a:b], h_vis[a:b])
+        d = s.finish()
+        st = s.stats()
+    assert st["nplanes"] > 8
+    # FP64 DFT of all 522M visibilities at 16 pixels (8 on sources), summed
+    # over row blocks (the transform is linear in the visibilities)
+    src = np.flatnonzero(model.ravel())
+    pix = np.concatenate([rng.choice(src, 8, replace=False), rng.integers(0, nx * nx, 8)])
+    ref = np.zeros(len(pix))
+    step = 4_000_000
+    for r0 in range(0, nrows, step):
+        ref += O.dft_ms2dirty(uvw[r0:r0 + step], freq, vis[r0:r0 + step], nx, nx, px, px,
+                              pixels=pix, negate_v=True, divide_by_n=False)
+    assert O.rel_rms(d.ravel()[pix], ref) < 1e-5

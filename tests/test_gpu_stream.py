@@ -114,3 +114,26 @@ def test_stream_rejects_chunk_outside_extent():
         s.add(uvw[:500], vis[:500])
         with pytest.raises(L.InvalidArgument):
             s.add(wide, vis[500:])
+
+
+def test_stream_predict_then_grid(cfg5):
+    """A major cycle on one stream: predict the model, then grid the
+    predicted visibilities (the first add after a prediction clears the
+    grid); the image equals the single-call ms2dirty of the same data."""
+    from wsclean_b200 import gridder as G
+    from wsclean_b200 import synth
+    c, _ = cfg5
+    uvw, freq, nx, px = c["uvw"], c["freq"], c["npix_x"], c["pixsize"]
+    rng = np.random.default_rng(6)
+    ix, iy, flux = synth.point_sky(50, nx, nx, rng)
+    model = synth.sky_image(nx, nx, ix, iy, flux)
+    ext = G.data_extent(uvw, freq)
+    parts = chunks(len(uvw), 3)
+    with G.Stream(freq, nx, nx, px, px, 1e-5, ext, dirty_dtype=np.float64, **KW) as s:
+        s.predict_begin(model)
+        vis = np.concatenate([s.predict(uvw[a:b]) for a, b in parts])
+        for a, b in parts:
+            s.add(uvw[a:b], vis[a:b])
+        d = s.finish()
+    ref = G.ms2dirty(uvw, freq, vis, nx, nx, px, px, 1e-5, dirty_dtype=np.float64, **KW)
+    assert O.rel_rms(d, ref) < 5e-6

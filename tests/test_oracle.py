@@ -102,3 +102,26 @@ def test_imageweights_restatement_matches_briggs_helper():
     helper = synth.briggs_weights(uvw, freq, nx, nx, px, px, robust=0.0,
                                   noise_weights=noise.astype(np.float32))
     np.testing.assert_allclose(iw, helper, rtol=1e-6)
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="compiled reference not built")
+def test_recorded_reference_grids_config2():
+    """The benchmark's roofline charges the grid the reference chooses for
+    the headline workload, recorded in tests/golden/ducc_grids.json by
+    tests/golden/make_ducc_grids.py: the reference chooses it again here."""
+    import json
+    import os
+    from wsclean_b200 import synth
+    rec = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "ducc_grids.json")))
+    c = synth.config2()
+    rng = np.random.default_rng(2)
+    v = (rng.normal(size=(len(c["uvw"]), 1)) + 1j * rng.normal(size=(len(c["uvw"]), 1)))
+    kw = dict(negate_v=True, divide_by_n=False, sigma_min=1.1, sigma_max=2.0, return_report=True)
+    for form, prec, eps, dt in (("mixed", "float", 1e-5, np.complex64),
+                                ("fp64", "double", 1e-12, np.complex128)):
+        _, rep = O.ref_ms2dirty(c["uvw"], c["freq"], v.astype(dt), c["npix_x"], c["npix_x"],
+                                c["pixsize"], c["pixsize"], eps, prec=prec, **kw)
+        g = O.parse_report(rep)[0]
+        r = rec["config2"][form]
+        assert (g["nu"], g["nv"], g["nplanes"], g["supp"]) == (r["nu"], r["nv"], r["nplanes"],
+                                                             r["supp"]), form

@@ -887,9 +887,11 @@ ChebCorr Context::upload_corrections(const GridPlan &g) {
 // [k2][t] for t < M/16; and the per-slot factors exp(+2 pi i (M/16 q - neg M)
 // k2 / nu), [k2][q][neg].  Angles are reduced exactly in integers before the
 // FP64 sin/cos.
+static size_t col_table_entries(size_t M, size_t K) { return M + K * (M / 16) + 32 * K; }
+
 static std::vector<double> col_twiddle_table(size_t M, size_t nu, size_t K) {
   const size_t TPF = M / 16;
-  std::vector<double> h(2 * (M + K * TPF + 32 * K), 0.0);
+  std::vector<double> h(2 * col_table_entries(M, K), 0.0);
   auto put = [&](size_t idx, long long num, long long den) {
     long long r = num % den;
     if (r < 0) r += den;
@@ -1900,7 +1902,7 @@ void Plan::build(const std::vector<wsg_job> &js) {
     CK(cudaMemcpy(cf_host.data() + pj.cf_off, cx_.cf_cur, ncf * sizeof(double),
                   cudaMemcpyDeviceToHost));
     const size_t M = size_t(1) << gp.logM;
-    const size_t ntw = (M + size_t(gp.K) * (M / 16) + 32 * size_t(gp.K)) * cs;
+    const size_t ntw = col_table_entries(M, size_t(gp.K)) * cs;
     pj.tw_off = tw_host.size();
     tw_host.resize(align256(tw_host.size() + ntw));
     CK(cudaMemcpy(tw_host.data() + pj.tw_off, twd, ntw, cudaMemcpyDeviceToHost));
@@ -2293,7 +2295,7 @@ StreamGridder::StreamGridder(Context &cx, const wsg_args &a, double wmin, double
   cf_.ensure(ncf * sizeof(double));
   CK(cudaMemcpy(cf_.p, cx_.cf_cur, ncf * sizeof(double), cudaMemcpyDeviceToDevice));
   const size_t M = size_t(1) << g.logM;
-  const size_t ntw = (M + size_t(g.K) * (M / 16) + 32 * size_t(g.K)) * cs;
+  const size_t ntw = col_table_entries(M, size_t(g.K)) * cs;
   tw_.ensure(ntw);
   CK(cudaMemcpy(tw_.p, twd, ntw, cudaMemcpyDeviceToDevice));
   CF(cufftCreate(&fft_));
@@ -2411,10 +2413,13 @@ void StreamGridder::add_t(const Staged &s, size_t nrows) {
 
 void StreamGridder::add(size_t nrows, const double *uvw, const void *vis, const void *wgt,
                         const uint8_t *mask) {
-  require(mode_ == 1, "add() after predict_begin(): finish the image first");
   require(uvw && vis, "uvw and vis are required");
   if (nrows == 0) return;
   CK(cudaSetDevice(cx_.device));
+  if (mode_ == 2) {  // after prediction (a major cycle's Predict, then Invert)
+    CK(cudaMemsetAsync(band_.p, 0, band_.n, cx_.stream));
+    mode_ = 1;
+  }
   Slot &sl = slots_[k_++ & 1];
   Staged s = stage(sl, nrows, uvw, vis, wgt, mask);
   if (dbl_)
