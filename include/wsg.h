@@ -320,11 +320,14 @@ int wsg_ctx_synchronize(wsg_ctx *ctx);
 /* Streaming gridding of data larger than one call -- WSClean's chunked
  * AddInversionData / PredictVisibilities loop (wgridder/wgriddingmsgridder.cpp:80-193)
  * -- with the w-stack of the whole observation resident on the GPU: the grid
- * is planned once from the declared data extent, every chunk of rows is
- * copied in (pinned double buffers on a copy stream, so the next chunk's
- * transfer overlaps this chunk's sort and spread) and spread into the same
- * grid, and the FFTs, w-screens and correction run once, in
- * wsg_stream_finish.  Prediction runs the transpose: the model image is
+ * is planned once from the declared data extent; the chunks of rows passed
+ * to wsg_stream_add are copied into device batches of about a third of the
+ * expected visibilities (nvis) and each batch is sorted and spread into the
+ * same grid (so that a tile of the grid collects the records of many chunks
+ * before it is flushed; two batches alternate, so the copies into one
+ * overlap the spread of the other); the FFTs, w-screens and correction run
+ * once, in wsg_stream_finish.  wsg_stream_add returns once its chunk has
+ * been copied (the caller's buffers are free again).  Prediction runs the transpose: the model image is
  * transformed once (wsg_stream_predict_begin) and each chunk is interpolated.
  * Extension of the reference interface, which re-plans and re-transforms per
  * chunk.

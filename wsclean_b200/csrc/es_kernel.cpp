@@ -460,10 +460,21 @@ void choose_grid(GridPlan &g, double sigma_min, double sigma_max, int tile, bool
   g.nwmin = g.do_w ? int(g.nplanes) - W + 1 : 1;
   uint64_t nbins = uint64_t(g.ntu) * g.ntv * g.nwmin;
   int bin_bits = ceil_log2(nbins);
-  require(bin_bits <= 30, "too many (tile, w-plane) bins for 31-bit sort keys");
-  int tbits = ceil_log2(uint64_t(tile));
-  g.lbits = std::min(tbits, (30 - bin_bits) / 2);
+  require(bin_bits <= 30, "too many (tile, w-plane) bins for the sort keys");
+  // the full in-tile position keeps the records of a bin in footprint order
+  // (the spread accumulates in registers while the footprint repeats); when
+  // it does not fit 31 bits beside the bin, the keys are 64-bit
+  g.bin_bits = bin_bits;
+  g.lbits = ceil_log2(uint64_t(tile));
   g.key_bits = bin_bits + 2 * g.lbits;
+  g.wide_keys = g.key_bits > 31;
+}
+
+void limit_key_bits(GridPlan &g, int max_bits) {
+  if (g.key_bits <= max_bits) return;
+  g.lbits = std::max(0, std::min(g.lbits, (max_bits - 1 - g.bin_bits) / 2));
+  g.key_bits = g.bin_bits + 2 * g.lbits;
+  g.wide_keys = g.key_bits > 31;
 }
 
 std::vector<std::pair<int, double>> rank_kernels(const GridPlan &g, double sigma_min,

@@ -308,7 +308,8 @@ DevGeom make_geom(const GridPlan &g) {
   int tb = 0;
   while ((1 << tb) < g.T) ++tb;
   d.qshift = tb - g.lbits;
-  d.inactive_key = 1u << g.key_bits;
+  d.wide = g.wide_keys ? 1 : 0;
+  d.inactive_key = 1ull << g.key_bits;
   d.Lu = int(g.Lu);
   d.band_rows = int(g.band_rows);
   d.band_full = g.band_full;
@@ -555,14 +556,14 @@ void launch_scan(Context &cx, const wsg_args &a, const Staged &s, bool gridding,
   g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
-template <typename TW, typename TV>
+template <typename TW, typename TV, typename K>
 void launch_keys(Context &cx, const wsg_args &a, const Staged &s, bool gridding, const DevGeom &g,
-                 uint32_t *keys, uint32_t *vals) {
+                 K *keys, uint32_t *vals) {
   int nb = launch_blocks(a.nrows, 256);
-  k_keys<TV, TW><<<nb, 256, 0, cx.stream>>>(a.nrows, int(a.nchan), s.uvw, s.fovc,
-                                            reinterpret_cast<const TV *>(s.vis),
-                                            reinterpret_cast<const TW *>(s.wgt), s.mask,
-                                            gridding ? 1 : 0, g, keys, vals);
+  k_keys<TV, TW, K><<<nb, 256, 0, cx.stream>>>(a.nrows, int(a.nchan), s.uvw, s.fovc,
+                                               reinterpret_cast<const TV *>(s.vis),
+                                               reinterpret_cast<const TW *>(s.wgt), s.mask,
+                                               gridding ? 1 : 0, g, keys, vals);
   cuda_check(cudaGetLastError(), "k_keys launch");
   g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
@@ -663,17 +664,25 @@ bool Context::prepare(const wsg_args &a, const Staged &s, bool gridding, void *v
     spec = make_geom(gp);
   else if (have_spec)
     std::memcpy(&spec, spec_geom.data(), sizeof spec);
-  uint32_t *ka = reinterpret_cast<uint32_t *>(b_keys_a.ensure(nvis_tot * 4));
+  // keys are 4 or 8 bytes (the expected grid's width; sized for the wider)
+  void *ka = b_keys_a.ensure(nvis_tot * 8);
   uint32_t *va = reinterpret_cast<uint32_t *>(b_vals_a.ensure(nvis_tot * 4));
   with_types(a, [&](auto *tw, auto *tv) {
     using TW = std::remove_pointer_t<decltype(tw)>;
     using TV = std::remove_pointer_t<decltype(tv)>;
     if (have_spec) {
       const int nb = std::min(launch_blocks(a.nrows, 256), num_sms * 8);
-      k_scan_keys<TV, TW><<<nb, 256, 0, sst>>>(
-          a.nrows, int(a.nchan), st.uvw, st.fovc, reinterpret_cast<const TV *>(st.vis),
-          reinterpret_cast<const TW *>(st.wgt), st.mask, gridding ? 1 : 0,
-          a.negate_v ? -1.0 : 1.0, d_scan, reinterpret_cast<TV *>(zero_out), spec, ka, va);
+      auto go = [&](auto *kp) {
+        using K = std::remove_pointer_t<decltype(kp)>;
+        k_scan_keys<TV, TW, K><<<nb, 256, 0, sst>>>(
+            a.nrows, int(a.nchan), st.uvw, st.fovc, reinterpret_cast<const TV *>(st.vis),
+            reinterpret_cast<const TW *>(st.wgt), st.mask, gridding ? 1 : 0,
+            a.negate_v ? -1.0 : 1.0, d_scan, reinterpret_cast<TV *>(zero_out), spec, kp, va);
+      };
+      if (spec.wide)
+        go(reinterpret_cast<unsigned long long *>(ka));
+      else
+        go(reinterpret_cast<uint32_t *>(ka));
       cuda_check(cudaGetLastError(), "k_scan_keys launch");
       g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     } else {
@@ -749,20 +758,30 @@ bool Context::prepare(const wsg_args &a, const Staged &s, bool gridding, void *v
   mark("choose_grid");
 
   // keys (unless the scan wrote them for this grid) + sort
-  uint32_t *kb = reinterpret_cast<uint32_t *>(b_keys_b.ensure(nvis_tot * 4));
+  void *kb = b_keys_b.ensure(nvis_tot * 8);
   uint32_t *vb = reinterpret_cast<uint32_t *>(b_vals_b.ensure(nvis_tot * 4));
-  if (!keyed) {
-    with_types(a, [&](auto *tw, auto *tv) {
-      using TW = std::remove_pointer_t<decltype(tw)>;
-      using TV = std::remove_pointer_t<decltype(tv)>;
-      launch_keys<TW, TV>(*this, a, st, gridding, g, ka, va);
-    });
-  }
-  size_t tmp = 0;
-  int end_bit = gp.key_bits + 1;
-  CK(cub::DeviceRadixSort::SortPairs(nullptr, tmp, ka, kb, va, vb, int(nvis_tot), 0, end_bit, stream));
-  void *dtmp = b_cub.ensure(tmp);
-  CK(cub::DeviceRadixSort::SortPairs(dtmp, tmp, ka, kb, va, vb, int(nvis_tot), 0, end_bit, stream));
+  const int end_bit = gp.key_bits + 1;
+  auto keys_and_sort = [&](auto *kap, auto *kbp) {
+    using K = std::remove_pointer_t<decltype(kap)>;
+    if (!keyed) {
+      with_types(a, [&](auto *tw, auto *tv) {
+        using TW = std::remove_pointer_t<decltype(tw)>;
+        using TV = std::remove_pointer_t<decltype(tv)>;
+        launch_keys<TW, TV, K>(*this, a, st, gridding, g, kap, va);
+      });
+    }
+    size_t tmp = 0;
+    CK(cub::DeviceRadixSort::SortPairs(nullptr, tmp, kap, kbp, va, vb, int(nvis_tot), 0, end_bit,
+                                       stream));
+    void *dtmp = b_cub.ensure(tmp);
+    CK(cub::DeviceRadixSort::SortPairs(dtmp, tmp, kap, kbp, va, vb, int(nvis_tot), 0, end_bit,
+                                       stream));
+  };
+  if (gp.wide_keys)
+    keys_and_sort(reinterpret_cast<unsigned long long *>(ka),
+                  reinterpret_cast<unsigned long long *>(kb));
+  else
+    keys_and_sort(reinterpret_cast<uint32_t *>(ka), reinterpret_cast<uint32_t *>(kb));
 
   // records
   void *rec = b_rec.ensure(gp.nvis * sizeof(typename RecOf<R>::type));
@@ -775,12 +794,19 @@ bool Context::prepare(const wsg_args &a, const Staged &s, bool gridding, void *v
   // chunk boundaries
   int *chunks = reinterpret_cast<int *>(b_chunks.ensure((gp.nvis + 1) * sizeof(int)));
   int *d_nch = reinterpret_cast<int *>(reinterpret_cast<char *>(b_small.p) + 1024);
-  ChunkStartPred pred{kb, 2 * gp.lbits, chunk_size};
-  thrust::counting_iterator<int> it(0);
-  tmp = 0;
-  CK(cub::DeviceSelect::If(nullptr, tmp, it, chunks, d_nch, int(gp.nvis), pred, stream));
-  dtmp = b_cub.ensure(std::max(tmp, b_cub.n));
-  CK(cub::DeviceSelect::If(dtmp, tmp, it, chunks, d_nch, int(gp.nvis), pred, stream));
+  auto select = [&](auto *kbp) {
+    using K = std::remove_pointer_t<decltype(kbp)>;
+    ChunkStartPred<K> pred{kbp, 2 * gp.lbits, chunk_size};
+    thrust::counting_iterator<int> it(0);
+    size_t tmp = 0;
+    CK(cub::DeviceSelect::If(nullptr, tmp, it, chunks, d_nch, int(gp.nvis), pred, stream));
+    void *dtmp = b_cub.ensure(std::max(tmp, b_cub.n));
+    CK(cub::DeviceSelect::If(dtmp, tmp, it, chunks, d_nch, int(gp.nvis), pred, stream));
+  };
+  if (gp.wide_keys)
+    select(reinterpret_cast<unsigned long long *>(kb));
+  else
+    select(reinterpret_cast<uint32_t *>(kb));
   mark("sort+records-submit");
   return true;
 }
@@ -2311,6 +2337,24 @@ StreamGridder::StreamGridder(Context &cx, const wsg_args &a, double wmin, double
     CK(cudaEventCreateWithFlags(&sl.copied, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
   }
+  for (auto &b : batch_) {
+    CK(cudaEventCreateWithFlags(&b.filled, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&b.spread, cudaEventDisableTiming));
+  }
+  // a batch holds a third of the expected visibilities (so that the copies
+  // of one overlap the spread of another), at least 32M, within 2^31 - 1
+  // and with its inputs in at most 1/16 of the device memory
+  {
+    size_t freeb = 0, total = 0;
+    CK(cudaMemGetInfo(&freeb, &total));
+    const size_t row_bytes = 24 + a.nchan * ((a.vis_type == WSG_C128 ? 16 : 8) +
+                                             (a.wgt_type == WSG_F64 ? 8 : 4) + 1);
+    size_t vis = std::max<size_t>(size_t(32) << 20, (nvis ? nvis : 0) / 3);
+    vis = std::min(vis, (size_t(1) << 31) - 1);
+    size_t rows = vis / a.nchan;
+    rows = std::min(rows, (total / 16) / row_bytes);
+    batch_rows_ = std::max<size_t>(rows, 1);
+  }
   CK(cudaMemsetAsync(band_.p, 0, band_.n, cx_.stream));
   mode_ = 1;
 }
@@ -2328,8 +2372,14 @@ StreamGridder::~StreamGridder() {
     for (DevBuf *b : {&sl.uvw, &sl.vis, &sl.wgt, &sl.mask}) b->release();
     for (PinnedBuf *b : {&sl.h_uvw, &sl.h_vis, &sl.h_wgt, &sl.h_mask}) b->release();
   }
+  for (auto &b : batch_) {
+    if (b.filled) cudaEventDestroy(b.filled);
+    if (b.spread) cudaEventDestroy(b.spread);
+    for (DevBuf *d : {&b.uvw, &b.vis, &b.wgt, &b.mask}) d->release();
+  }
   if (fft_) cufftDestroy(fft_);
-  for (DevBuf *b : {&band_, &H_, &img_, &cf_, &tw_, &fftwork_, &vout_}) b->release();
+  for (DevBuf *b : {&band_, &H_, &img_, &cf_, &tw_, &fftwork_, &vout_, &fovc_, &scan_d_}) b->release();
+  scan_h_.release();
 }
 
 // Planes per pass of the final transforms (the u-transformed rows of a pass
@@ -2411,6 +2461,95 @@ void StreamGridder::add_t(const Staged &s, size_t nrows) {
                            make_kernel<R>(g.poly));
 }
 
+// Enqueues a copy of bytes from src (device, page-locked or pageable host
+// memory) to the device buffer dst on the copy stream; pageable memory goes
+// through the page-locked buffer pin (the caller synchronises the copy
+// stream before pin is reused).
+void StreamGridder::copy_into(void *dst, const void *src, size_t bytes, PinnedBuf &pin) {
+  cudaPointerAttributes at;
+  cudaMemoryType t = cudaMemoryTypeUnregistered;
+  if (cudaPointerGetAttributes(&at, src) == cudaSuccess)
+    t = at.type;
+  else
+    cudaGetLastError();
+  if (t == cudaMemoryTypeDevice || t == cudaMemoryTypeManaged || t == cudaMemoryTypeHost) {
+    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, copy_));
+    return;
+  }
+  std::memcpy(pin.ensure(bytes), src, bytes);
+  CK(cudaMemcpyAsync(dst, pin.p, bytes, cudaMemcpyHostToDevice, copy_));
+}
+
+// Rejects a chunk (device copies on the copy stream) with an active
+// visibility outside the declared extent, as prepare() does for the fixed
+// grid: the chunk's visibility scan runs on the copy stream right after its
+// copies, so the check does not wait for the spread of an earlier batch.
+void StreamGridder::check_extent(const Staged &s, size_t nrows) {
+  const size_t nchan = a_.nchan;
+  if (fovc_.n == 0) {
+    std::vector<double> f(nchan);
+    for (size_t c = 0; c < nchan; ++c) f[c] = freq_[c] / kSpeedOfLight;
+    CK(cudaMemcpy(fovc_.ensure(nchan * sizeof(double)), f.data(), nchan * sizeof(double),
+                  cudaMemcpyHostToDevice));
+  }
+  ScanOut *d = reinterpret_cast<ScanOut *>(scan_d_.ensure(sizeof(ScanOut)));
+  ScanOut *h = reinterpret_cast<ScanOut *>(scan_h_.ensure(sizeof(ScanOut)));
+  *h = ScanOut{};
+  h->wmin_bits = 0x7ff0000000000000ull;
+  CK(cudaMemcpyAsync(d, h, sizeof(ScanOut), cudaMemcpyHostToDevice, copy_));
+  wsg_args ac = a_;
+  ac.nrows = nrows;
+  ac.wgt = s.wgt;
+  with_types(ac, [&](auto *tw, auto *tv) {
+    using TW = std::remove_pointer_t<decltype(tw)>;
+    using TV = std::remove_pointer_t<decltype(tv)>;
+    const int nb = std::min(launch_blocks(nrows, 256), cx_.num_sms * 8);
+    k_scan<TV, TW><<<nb, 256, 0, copy_>>>(nrows, int(nchan), s.uvw,
+                                          reinterpret_cast<const double *>(fovc_.p),
+                                          reinterpret_cast<const TV *>(s.vis),
+                                          reinterpret_cast<const TW *>(s.wgt), s.mask, 1,
+                                          a_.negate_v ? -1.0 : 1.0, d, (TV *)nullptr);
+  });
+  cuda_check(cudaGetLastError(), "k_scan launch");
+  g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+  CK(cudaMemcpyAsync(h, d, sizeof(ScanOut), cudaMemcpyDeviceToHost, copy_));
+  CK(cudaStreamSynchronize(copy_));
+  if (h->nvis == 0) return;
+  auto bits2d = [](unsigned long long b) {
+    double x;
+    std::memcpy(&x, &b, 8);
+    return x;
+  };
+  const GridPlan &g = gp_;
+  auto within = [](double x, double lim) { return x <= lim * (1.0 + 1e-12) + 1e-9; };
+  require(bits2d(h->wmin_bits) >= g.wmin_d * (1.0 - 1e-12) - 1e-9 &&
+              within(bits2d(h->wmax_bits), g.wmax_d),
+          "a chunk's |w| range lies outside the extent declared for the stream");
+  require(within(bits2d(h->umax_bits), g.umax) && within(bits2d(h->vmax_bits), g.vmax),
+          "a chunk's |u| or |v| exceeds the extent declared for the stream");
+}
+
+// Sorts and spreads the current batch (after its copies) and switches to
+// the other one.
+void StreamGridder::flush_batch() {
+  Batch &b = batch_[bcur_];
+  if (b.rows == 0) return;
+  CK(cudaEventRecord(b.filled, copy_));
+  CK(cudaStreamWaitEvent(cx_.stream, b.filled, 0));
+  Staged s;
+  s.uvw = reinterpret_cast<const double *>(b.uvw.p);
+  s.vis = b.vis.p;
+  s.wgt = b.has_wgt ? b.wgt.p : nullptr;
+  s.mask = b.has_mask ? reinterpret_cast<const uint8_t *>(b.mask.p) : nullptr;
+  if (dbl_)
+    add_t<double>(s, b.rows);
+  else
+    add_t<float>(s, b.rows);
+  CK(cudaEventRecord(b.spread, cx_.stream));
+  b.rows = 0;
+  bcur_ ^= 1;
+}
+
 void StreamGridder::add(size_t nrows, const double *uvw, const void *vis, const void *wgt,
                         const uint8_t *mask) {
   require(uvw && vis, "uvw and vis are required");
@@ -2418,15 +2557,54 @@ void StreamGridder::add(size_t nrows, const double *uvw, const void *vis, const 
   CK(cudaSetDevice(cx_.device));
   if (mode_ == 2) {  // after prediction (a major cycle's Predict, then Invert)
     CK(cudaMemsetAsync(band_.p, 0, band_.n, cx_.stream));
+    for (auto &b : batch_) b.rows = 0;
     mode_ = 1;
   }
-  Slot &sl = slots_[k_++ & 1];
-  Staged s = stage(sl, nrows, uvw, vis, wgt, mask);
-  if (dbl_)
-    add_t<double>(s, nrows);
-  else
-    add_t<float>(s, nrows);
-  CK(cudaEventRecord(sl.done, cx_.stream));
+  if (nrows > batch_rows_) {  // a chunk larger than a batch is spread alone
+    flush_batch();
+    Slot &sl = slots_[k_++ & 1];
+    Staged s = stage(sl, nrows, uvw, vis, wgt, mask);
+    if (dbl_)
+      add_t<double>(s, nrows);
+    else
+      add_t<float>(s, nrows);
+    CK(cudaEventRecord(sl.done, cx_.stream));
+    return;
+  }
+  Batch *b = &batch_[bcur_];
+  if (b->rows > 0 && (b->rows + nrows > batch_rows_ || (wgt != nullptr) != b->has_wgt ||
+                      (mask != nullptr) != b->has_mask)) {
+    flush_batch();
+    b = &batch_[bcur_];
+  }
+  const size_t nchan = a_.nchan;
+  const size_t vsz = a_.vis_type == WSG_C128 ? 16 : 8, wsz = a_.wgt_type == WSG_F64 ? 8 : 4;
+  if (b->rows == 0) {  // the batch's previous spread has read its buffers
+    CK(cudaEventSynchronize(b->spread));
+    b->has_wgt = wgt != nullptr;
+    b->has_mask = mask != nullptr;
+    b->uvw.ensure(batch_rows_ * 3 * sizeof(double));
+    b->vis.ensure(batch_rows_ * nchan * vsz);
+    if (b->has_wgt) b->wgt.ensure(batch_rows_ * nchan * wsz);
+    if (b->has_mask) b->mask.ensure(batch_rows_ * nchan);
+  }
+  // the caller's buffers are free again when add() returns: the copies
+  // (not the spread of an earlier batch, which runs meanwhile) are waited for
+  Slot &sl = slots_[0];
+  const size_t r0 = b->rows;
+  copy_into(static_cast<char *>(b->uvw.p) + r0 * 3 * sizeof(double), uvw, nrows * 3 * sizeof(double),
+            sl.h_uvw);
+  copy_into(static_cast<char *>(b->vis.p) + r0 * nchan * vsz, vis, nrows * nchan * vsz, sl.h_vis);
+  if (wgt)
+    copy_into(static_cast<char *>(b->wgt.p) + r0 * nchan * wsz, wgt, nrows * nchan * wsz, sl.h_wgt);
+  if (mask) copy_into(static_cast<char *>(b->mask.p) + r0 * nchan, mask, nrows * nchan, sl.h_mask);
+  Staged s;
+  s.uvw = reinterpret_cast<const double *>(static_cast<char *>(b->uvw.p) + r0 * 3 * sizeof(double));
+  s.vis = static_cast<char *>(b->vis.p) + r0 * nchan * vsz;
+  s.wgt = wgt ? static_cast<char *>(b->wgt.p) + r0 * nchan * wsz : nullptr;
+  s.mask = mask ? reinterpret_cast<const uint8_t *>(b->mask.p) + r0 * nchan : nullptr;
+  check_extent(s, nrows);  // waits for the copies; a rejected chunk is not kept
+  b->rows += nrows;
 }
 
 template <typename R>
@@ -2484,6 +2662,7 @@ void StreamGridder::finish(void *dirty, int accumulate) {
   require(mode_ == 1, "finish() without a gridding stream");
   require(dirty != nullptr, "dirty is required");
   CK(cudaSetDevice(cx_.device));
+  flush_batch();
   if (dbl_)
     finish_t<double>(dirty, accumulate);
   else
@@ -2521,6 +2700,7 @@ void StreamGridder::predict_begin_t(const double *img) {
 void StreamGridder::predict_begin(const void *dirty) {
   require(dirty != nullptr, "dirty is required");
   CK(cudaSetDevice(cx_.device));
+  for (auto &b : batch_) b.rows = 0;  // rows added since the last finish are discarded
   const size_t npix = gp_.nx * gp_.ny, dsz = a_.dirty_type == WSG_F64 ? 8 : 4;
   const void *din = cx_.stage_in(dirty, npix * dsz, cx_.b_out);
   double *img = reinterpret_cast<double *>(img_.p);
@@ -3234,6 +3414,7 @@ void ms2dirty_noalloc(const wsg_args &a, const void *vis, void *dirty, cudaStrea
     gp.umax = bits2d(hs.umax_bits);
     gp.vmax = bits2d(hs.vmax_bits);
     choose_grid(gp, a.sigma_min, a.sigma_max, 16, /*pow2_v=*/true);
+    limit_key_bits(gp, 31);  // this path sorts 32-bit keys
     int logMv = 0;
     while ((size_t(1) << logMv) < gp.nv) ++logMv;
     const DevGeom g = make_geom(gp);
@@ -3246,7 +3427,7 @@ void ms2dirty_noalloc(const wsg_args &a, const void *vis, void *dirty, cudaStrea
     with_types(a, [&](auto *tw, auto *tv) {
       using TW = std::remove_pointer_t<decltype(tw)>;
       using TV = std::remove_pointer_t<decltype(tv)>;
-      k_keys<TV, TW><<<launch_blocks(a.nrows, 256), 256, 0, stream>>>(
+      k_keys<TV, TW, uint32_t><<<launch_blocks(a.nrows, 256), 256, 0, stream>>>(
           a.nrows, int(a.nchan), st.uvw, st.fovc, reinterpret_cast<const TV *>(st.vis),
           reinterpret_cast<const TW *>(st.wgt), st.mask, 1, g, ka, va);
     });
@@ -3268,7 +3449,7 @@ void ms2dirty_noalloc(const wsg_args &a, const void *vis, void *dirty, cudaStrea
     });
     cuda_check(cudaGetLastError(), "k_records launch");
     int *chunks = reinterpret_cast<int *>(ar.take((gp.nvis + 1) * sizeof(int)));
-    ChunkStartPred pred{kb, 2 * gp.lbits, 1024};
+    ChunkStartPred<uint32_t> pred{kb, 2 * gp.lbits, 1024};
     thrust::counting_iterator<int> it(0);
     tmp = 0;
     cuda_check(cub::DeviceSelect::If(nullptr, tmp, it, chunks, d_nch, int(gp.nvis), pred, stream),

@@ -338,6 +338,27 @@ class StreamGridder {
   Staged stage(Slot &sl, size_t nrows, const double *uvw, const void *vis, const void *wgt,
                const uint8_t *mask);
   size_t plane_batch() const;
+  // Gridding batches: the chunks passed to add() are gathered on the device
+  // and sorted and spread together, so that a (tile, w-plane) bin holds the
+  // records of many chunks and its tile is flushed to the grid once for all
+  // of them; two batches alternate, so that the copies into one overlap the
+  // spread of the other.
+  struct Batch {
+    DevBuf uvw, vis, wgt, mask;
+    size_t rows = 0;
+    bool has_wgt = false, has_mask = false;
+    cudaEvent_t filled = nullptr, spread = nullptr;
+  };
+  Batch batch_[2];
+  int bcur_ = 0;
+  size_t batch_rows_ = 0;
+  // the extent check of a chunk at add(): f/c on the device, the scan's
+  // statistics and their page-locked read-back
+  DevBuf fovc_, scan_d_;
+  PinnedBuf scan_h_;
+  void check_extent(const Staged &s, size_t nrows);
+  void copy_into(void *dst, const void *src, size_t bytes, PinnedBuf &pin);
+  void flush_batch();
 
   Context &cx_;
   wsg_args a_;

@@ -47,7 +47,8 @@ struct DevGeom {
   double lshift, mshift, nshift, vfac;
   int shifting;
   int T, ntu, ntv, nwmin, lbits, qshift;  // qshift: in-tile bits dropped per axis
-  uint32_t inactive_key;
+  int wide;                               // 64-bit sort keys
+  unsigned long long inactive_key;
   int Lu, band_rows, band_full;
 };
 
@@ -160,14 +161,18 @@ __device__ __forceinline__ void vis_pixel(const DevGeom &g, double u, double v,
   }
 }
 
-__device__ __forceinline__ uint32_t bin_key(const DevGeom &g, const VisPix &p) {
+// Sort key of a visibility: its (tile, minplane) bin, then its position in
+// the tile (quantised to lbits per axis), in 32 or -- when the bins and the
+// full in-tile position need more than 31 bits -- 64 bits.
+template <typename K>
+__device__ __forceinline__ K bin_key(const DevGeom &g, const VisPix &p) {
   int a = p.iu0 + g.nsafe, b = p.iv0 + g.nsafe;
   uint32_t tu = uint32_t(a / g.T), tv = uint32_t(b / g.T);
   uint32_t lu = uint32_t(a % g.T), lv = uint32_t(b % g.T);
   uint32_t bin = (tu * uint32_t(g.ntv) + tv) * uint32_t(g.nwmin) + uint32_t(p.iw);
   // in-tile position, quantised to lbits per axis (T <= 32)
   uint32_t q = ((lu >> g.qshift) << g.lbits) | (lv >> g.qshift);
-  return (bin << (2 * g.lbits)) | q;
+  return (K(bin) << (2 * g.lbits)) | K(q);
 }
 
 
@@ -184,13 +189,13 @@ __device__ __forceinline__ T warp_sum(T v) {
 // visibilities (scanData, wgridder.h:1578-1618); with KEYS, also the sort
 // key of every visibility for the grid geometry g, as k_keys writes it (the
 // caller checks afterwards that the planned geometry is g).
-template <typename TV, typename TW, bool KEYS>
+template <typename TV, typename TW, bool KEYS, typename K = uint32_t>
 __device__ __forceinline__ void scan_rows(size_t nrows, int nchan, const double *__restrict__ uvw,
                                           const double *__restrict__ fovc,
                                           const TV *__restrict__ vis, const TW *__restrict__ wgt,
                                           const uint8_t *__restrict__ mask, int gridding,
                                           double vfac, ScanOut *out, TV *__restrict__ vis_out,
-                                          const DevGeom &g, uint32_t *__restrict__ keys,
+                                          const DevGeom &g, K *__restrict__ keys,
                                           uint32_t *__restrict__ vals) {
   double lwmin = 1e300, lwmax = 0, lumax = 0, lvmax = 0;
   unsigned long long cnt = 0;
@@ -210,7 +215,7 @@ __device__ __forceinline__ void scan_rows(size_t nrows, int nchan, const double 
         act = (!wgt || wgt[k] != 0) && (!mask || mask[k] != 0);
         if (!act && vis_out) vis_out[k] = TV{0, 0};
       }
-      uint32_t key = KEYS ? g.inactive_key : 0u;
+      K key = KEYS ? K(g.inactive_key) : K(0);
       if (act) {
         double f = fovc[c];
         double aw = fabs(w * f);
@@ -222,7 +227,7 @@ __device__ __forceinline__ void scan_rows(size_t nrows, int nchan, const double 
         if constexpr (KEYS) {
           VisPix p;
           vis_pixel(g, u * f, v * f, w * f, p);
-          key = bin_key(g, p);
+          key = bin_key<K>(g, p);
         }
       }
       if constexpr (KEYS) {
@@ -255,29 +260,29 @@ __global__ void k_scan(size_t nrows, int nchan, const double *__restrict__ uvw,
                        int gridding, double vfac, ScanOut *out, TV *__restrict__ vis_out) {
   const DevGeom g{};
   scan_rows<TV, TW, false>(nrows, nchan, uvw, fovc, vis, wgt, mask, gridding, vfac, out, vis_out,
-                           g, nullptr, nullptr);
+                           g, (uint32_t *)nullptr, nullptr);
 }
 
 // The scan with the keys of an expected geometry: when consecutive calls
 // plan the same grid (the usual case: the same image and data extent), the
 // separate pass of k_keys over uvw and the visibilities is not needed.
-template <typename TV, typename TW>
+template <typename TV, typename TW, typename K>
 __global__ void k_scan_keys(size_t nrows, int nchan, const double *__restrict__ uvw,
                             const double *__restrict__ fovc, const TV *__restrict__ vis,
                             const TW *__restrict__ wgt, const uint8_t *__restrict__ mask,
                             int gridding, double vfac, ScanOut *out, TV *__restrict__ vis_out,
-                            DevGeom g, uint32_t *__restrict__ keys, uint32_t *__restrict__ vals) {
-  scan_rows<TV, TW, true>(nrows, nchan, uvw, fovc, vis, wgt, mask, gridding, vfac, out, vis_out,
-                          g, keys, vals);
+                            DevGeom g, K *__restrict__ keys, uint32_t *__restrict__ vals) {
+  scan_rows<TV, TW, true, K>(nrows, nchan, uvw, fovc, vis, wgt, mask, gridding, vfac, out,
+                             vis_out, g, keys, vals);
 }
 
 // --------------------------------------------------------------- k_keys
 
-template <typename TV, typename TW>
+template <typename TV, typename TW, typename K>
 __global__ void k_keys(size_t nrows, int nchan, const double *__restrict__ uvw,
                        const double *__restrict__ fovc, const TV *__restrict__ vis,
                        const TW *__restrict__ wgt, const uint8_t *__restrict__ mask,
-                       int gridding, DevGeom g, uint32_t *__restrict__ keys,
+                       int gridding, DevGeom g, K *__restrict__ keys,
                        uint32_t *__restrict__ vals) {
   for (size_t r = blockIdx.x * size_t(blockDim.x) + threadIdx.x; r < nrows;
        r += size_t(gridDim.x) * blockDim.x) {
@@ -294,12 +299,12 @@ __global__ void k_keys(size_t nrows, int nchan, const double *__restrict__ uvw,
       } else {
         act = (!wgt || wgt[k] != 0) && (!mask || mask[k] != 0);
       }
-      uint32_t key = g.inactive_key;
+      K key = K(g.inactive_key);
       if (act) {
         double f = fovc[c];
         VisPix p;
         vis_pixel(g, u * f, v * f, w * f, p);
-        key = bin_key(g, p);
+        key = bin_key<K>(g, p);
       }
       keys[k] = key;
       vals[k] = uint32_t(k);
@@ -379,8 +384,9 @@ __global__ void k_plan_chunks(int n, const int *__restrict__ in, int *__restrict
 
 // A chunk starts where the (tile, minplane) bin changes or at a multiple of
 // the chunk size; chunks therefore never cross bins.
+template <typename K>
 struct ChunkStartPred {
-  const uint32_t *keys;
+  const K *keys;
   int shift;
   int chunk;
   __host__ __device__ bool operator()(const int &i) const {

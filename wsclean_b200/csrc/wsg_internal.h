@@ -125,7 +125,9 @@ struct GridPlan {
   int T = 16;
   int ntu = 0, ntv = 0, nwmin = 1;
   int lbits = 0;      // sort bits per axis for the position inside a tile
-  int key_bits = 0;   // total key bits (<= 31)
+  int bin_bits = 0;   // sort bits of the (tile, minplane) bin
+  int key_bits = 0;   // total key bits
+  bool wide_keys = false;  // key_bits > 31: 64-bit sort keys
   // batch plans: every job uses the kernel (W, sigma) of the first one
   int force_W = 0;
   double force_sigma = 0;
@@ -145,6 +147,10 @@ struct GridPlan {
 // skipped.
 constexpr size_t kPow2VMax = 8192;
 void choose_grid(GridPlan &g, double sigma_min, double sigma_max, int tile, bool pow2_v = false);
+
+// Caps the sort key at max_bits by quantising the in-tile position (for
+// callers that sort 32-bit keys only).
+void limit_key_bits(GridPlan &g, int max_bits);
 
 // The n cheapest kernels (W, sigma) for these inputs by the cost model of
 // choose_grid, cheapest first (the autotuner times them).
