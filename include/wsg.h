@@ -389,6 +389,18 @@ int wsg_weights_apply(wsg_weights *w, size_t nrows, size_t nchan, size_t npol, c
 /* The grid (width x height/2 doubles, index x + y*width; NULL to skip), its
  * size and the sum of gridded weights. */
 int wsg_weights_get(wsg_weights *w, double *grid, size_t *width, size_t *height, double *total);
+/* Folds the imaging weights of w (finished by wsg_weights_finish, on the
+ * stream's device) into every later wsg_stream_add: each visibility is
+ * gridded with weight x imaging weight of its uv cell -- the product that
+ * MSGridderBase::readAndWeightVisibilities forms on the host
+ * (gridding/msgridderbase.cpp:583-590,640-659) -- looked up while the
+ * device scans the batch and builds its records, so no weighted copy of the
+ * weights is made or uploaded; a visibility outside the weight grid is
+ * inactive.  The product is rounded to float for float weights, as
+ * wsg_weights_apply stores it.  Predictions are not weighted.  w must stay
+ * alive while set; NULL turns the lookup off.  Extension of the reference
+ * interface. */
+int wsg_stream_set_imaging_weights(wsg_stream *s, const wsg_weights *w);
 
 #ifdef __cplusplus
 }

@@ -79,3 +79,45 @@ def test_weights_polarisations_and_briggs_into_gridding(data):
     dft = O.dft_ms2dirty(uvw, freq, vis, 256, 256, 4 * px, 4 * px, wgt=wi.astype(np.float64),
                          pixels=pix, negate_v=True, divide_by_n=False)
     assert O.rel_rms(d.ravel()[pix], dft) < 1e-5
+
+
+def test_stream_fuses_imaging_weights(data):
+    """A stream with imaging weights set grids every visibility with weight x
+    imaging weight looked up on the device (the product WSClean's
+    readAndWeightVisibilities forms, msgridderbase.cpp:583-590,640-659),
+    equal to gridding the weights that wsg_weights_apply returns, and to the
+    FP64 DFT with those weights; cells outside the weight grid (a weight grid
+    of a quarter of the image's extent in uv) drop their visibilities."""
+    from wsclean_b200 import gridder as G
+    from wsclean_b200.gridder import ImageWeights
+    import oracle as O
+    c, w = data
+    uvw, freq, nx, px = c["uvw"], c["freq"], c["npix_x"], c["pixsize"]
+    kw = dict(negate_v=True, divide_by_n=False, sigma_min=1.1, sigma_max=2.0)
+    rng = np.random.default_rng(9)
+    vis = (rng.normal(size=w.shape) + 1j * rng.normal(size=w.shape)).astype(np.complex64)
+    ext = G.data_extent(uvw, freq)
+    parts = [(0, len(uvw) // 3), (len(uvw) // 3, len(uvw))]
+    for scale in (1.0, 0.25):   # 0.25: a coarser weight grid that misses the outer uv cells
+        with ImageWeights("briggs", 0.0, nx, nx, px / scale, px / scale) as iw:
+            iw.grid(uvw, freq, w)
+            iw.finish()
+            weff = iw.apply(uvw, freq, w)
+            with G.Stream(freq, nx, nx, px, px, 1e-5, ext, nvis=vis.size, dirty_dtype=np.float64,
+                          **kw) as s:
+                s.set_imaging_weights(iw)
+                for a, b in parts:
+                    s.add(uvw[a:b], vis[a:b], wgt=w[a:b])
+                fused = s.finish()
+            with G.Stream(freq, nx, nx, px, px, 1e-5, ext, nvis=vis.size, dirty_dtype=np.float64,
+                          **kw) as s:
+                for a, b in parts:
+                    s.add(uvw[a:b], vis[a:b], wgt=weff[a:b])
+                unfused = s.finish()
+        if scale < 1.0:
+            assert (weff == 0).sum() > (w == 0).sum()   # some cells fell outside
+        assert O.rel_rms(fused, unfused) < 1e-6
+        pix = rng.integers(0, nx * nx, 32)
+        dft = O.dft_ms2dirty(uvw, freq, vis, nx, nx, px, px, wgt=weff.astype(np.float64),
+                             pixels=pix, negate_v=True, divide_by_n=False)
+        assert O.rel_rms(fused.ravel()[pix], dft) < 1e-5

@@ -36,6 +36,7 @@ EXPORTED = [
     "wsg_weights_create", "wsg_weights_destroy", "wsg_weights_grid", "wsg_weights_finish",
     "wsg_weights_apply", "wsg_weights_get", "wsg_autotune", "wsg_ctx_set_async",
     "wsg_ms2dirty_tuning", "wsg_dirty2ms_tuning", "wsg_get_tuning", "wsg_tuning_choice",
+    "wsg_stream_set_imaging_weights",
 ]
 
 c_size_t, c_double, c_int, c_void_p = ctypes.c_size_t, ctypes.c_double, ctypes.c_int, ctypes.c_void_p
@@ -157,6 +158,7 @@ def lib():
         L.wsg_stream_predict_begin.argtypes = [vp, vp]
         L.wsg_stream_predict.argtypes = [vp, c_size_t, vp, vp, vp, vp]
         L.wsg_stream_get_stats.argtypes = [vp, P(WsgStats)]
+        L.wsg_stream_set_imaging_weights.argtypes = [vp, vp]
         L.wsg_weights_create.argtypes = [vp, c_int, c_double, c_size_t, c_size_t, c_double,
                                          c_double, c_int, c_double, P(vp)]
         L.wsg_weights_destroy.argtypes = [vp]

@@ -442,6 +442,13 @@ int wsg_weights_create(wsg_ctx *ctx, int mode, double briggs_robust, size_t widt
   });
 }
 
+int wsg_stream_set_imaging_weights(wsg_stream *s, const wsg_weights *w) {
+  return guarded([&] {
+    wsg::require(s != nullptr, "stream is NULL");
+    s->impl->set_imaging_weights(w ? w->impl.get() : nullptr);
+  });
+}
+
 int wsg_weights_destroy(wsg_weights *w) {
   return guarded([&] {
     if (!w) return;

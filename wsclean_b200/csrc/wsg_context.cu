@@ -140,7 +140,7 @@ Context::Context(int dev) {
   CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
   CK(cudaStreamCreateWithPriority(&cpy, cudaStreamNonBlocking, prio_hi));
   CK(cudaStreamCreateWithFlags(&d2h, cudaStreamNonBlocking));
-  for (cudaEvent_t *e : {&ev_start, &ev_in, &ev_done, &ev_scan})
+  for (cudaEvent_t *e : {&ev_start, &ev_in, &ev_done, &ev_scan, &ev_keys})
     CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
   CK(cudaHostAlloc(&h_scan, sizeof(ScanOut), cudaHostAllocMapped));
   CK(cudaHostGetDevicePointer(&h_scan_dev, h_scan, 0));
@@ -176,7 +176,7 @@ Context::~Context() {
       cudaStreamSynchronize(st);
       cudaStreamDestroy(st);
     }
-  for (cudaEvent_t e : {ev_start, ev_in, ev_done, ev_scan})
+  for (cudaEvent_t e : {ev_start, ev_in, ev_done, ev_scan, ev_keys})
     if (e) cudaEventDestroy(e);
   for (auto &sl : slots)
     if (sl.free_ev) cudaEventDestroy(sl.free_ev);
@@ -488,6 +488,27 @@ struct GridKernels {
 // Whether `extra` bytes of shared memory fit beside a CTA's `base` bytes
 // without lowering the CTAs an SM holds (228 KB a SM, 227 KB a CTA, 1 KB
 // reserved a CTA).
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the
+// library has no link-time driver dependency); nullptr if unavailable.
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                   const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                   const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(f);
+    cudaGetLastError();
+  });
+  return fn;
+}
+
 bool twist_tables_fit(size_t base, size_t extra) {
   constexpr size_t kSM = 228 * 1024, kCTA = 227 * 1024, kRes = 1024;
   if (base + extra > kCTA) return false;
@@ -497,10 +518,58 @@ bool twist_tables_fit(size_t base, size_t extra) {
 // Pruned u-transform kernels, dispatched over log2(M).
 template <typename R>
 struct ColKernels {
+  // The band-to-image transform with the band columns staged by the tensor
+  // memory accelerator (k_ucol_bwd_tma), when its boxes can be used: a box
+  // row of NB columns is a multiple of 16 bytes, column groups start on a
+  // 16-byte boundary and do not straddle the wrap of the v axis.  Returns
+  // false when not used.
   template <int LOGM>
-  static void run1(bool bwd, const ColArgs &a, int npl, cudaStream_t st) {
+  static bool run_tma(const ColArgs &a, int npl, cudaStream_t st, int *err) {
+    constexpr int M = 1 << LOGM;
+    using Cfg = TmaCfg<R, M>;
+    constexpr int NB = Cfg::NB;
+    EncodeTiledFn enc = encode_tiled();
+    if (!err || !enc || env_int("WSG_UCOL_TMA", 1) == 0) return false;
+    if (NB * 2 * int(sizeof(R)) % 16 != 0 || (a.ny / 2) % NB != 0) return false;
+    if (sizeof(R) == 4 && ((a.nv - a.ny / 2) % 2) != 0) return false;
+    CUtensorMap map;
+    const cuuint64_t dims[2] = {cuuint64_t(2) * cuuint64_t(npl) * cuuint64_t(a.nv),
+                                cuuint64_t(a.band_rows)};
+    const cuuint64_t strides[1] = {cuuint64_t(a.P) * cuuint64_t(a.nv) * 2 * sizeof(R)};
+    const cuuint32_t box[2] = {cuuint32_t(2 * NB), cuuint32_t(Cfg::BR)};
+    const cuuint32_t estr[2] = {1, 1};
+    if (enc(&map, sizeof(R) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+            2, const_cast<void *>(a.band), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return false;
+    const size_t smem = Cfg::stage_bytes() +
+                        (size_t(NB) * FftBuf<M>::value + M) * 2 * sizeof(R) + 128;
+    auto *kern = k_ucol_bwd_tma<R, LOGM>;
+    smem_attr(kern, smem);
+    static int per_sm = -1;  // resident CTAs per SM (one instantiation, one answer)
+    if (per_sm < 0) {
+      int n = 0;
+      cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, ColCfg<R, M>::THREADS,
+                                                               smem),
+                 "occupancy");
+      per_sm = std::max(n, 1);
+    }
+    int dev = 0, nsm = 148;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    cuda_check(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev), "attribute");
+    const long long nitems = (long long)((a.ny + NB - 1) / NB) * npl;
+    const int grid = int(std::min<long long>(nitems, (long long)nsm * per_sm));
+    kern<<<grid, ColCfg<R, M>::THREADS, smem, st>>>(a, map, npl, err);
+    cuda_check(cudaGetLastError(), "k_ucol_bwd_tma launch");
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+    return true;
+  }
+  template <int LOGM>
+  static void run1(bool bwd, const ColArgs &a, int npl, cudaStream_t st, int *err) {
     constexpr int M = 1 << LOGM;
     using Cfg = ColCfg<R, M>;
+    if (bwd && run_tma<LOGM>(a, npl, st, err)) return;
     const size_t smem = ColSmem2<R, M>::bytes();
     dim3 grid((a.ny + Cfg::NB - 1) / Cfg::NB, npl);
     if (bwd) {
@@ -521,16 +590,19 @@ struct ColKernels {
     cuda_check(cudaGetLastError(), bwd ? "k_ucol_bwd launch" : "k_ucol_fwd launch");
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
   }
-  static void run(int logM, bool bwd, const ColArgs &a, int npl, cudaStream_t st) {
+  // err: the device error word (bit 2: a staged copy did not complete), or
+  // nullptr to stay with the plain loads
+  static void run(int logM, bool bwd, const ColArgs &a, int npl, cudaStream_t st,
+                  int *err = nullptr) {
     switch (logM) {
-      case 8: run1<8>(bwd, a, npl, st); break;
-      case 9: run1<9>(bwd, a, npl, st); break;
-      case 10: run1<10>(bwd, a, npl, st); break;
-      case 11: run1<11>(bwd, a, npl, st); break;
-      case 12: run1<12>(bwd, a, npl, st); break;
+      case 8: run1<8>(bwd, a, npl, st, err); break;
+      case 9: run1<9>(bwd, a, npl, st, err); break;
+      case 10: run1<10>(bwd, a, npl, st, err); break;
+      case 11: run1<11>(bwd, a, npl, st, err); break;
+      case 12: run1<12>(bwd, a, npl, st, err); break;
       case 13:
         if constexpr (sizeof(R) == 4) {
-          run1<13>(bwd, a, npl, st);
+          run1<13>(bwd, a, npl, st, err);
           break;
         }
         [[fallthrough]];
@@ -551,7 +623,7 @@ void launch_scan(Context &cx, const wsg_args &a, const Staged &s, bool gridding,
   k_scan<TV, TW><<<nb, 256, 0, st>>>(
       a.nrows, int(a.nchan), s.uvw, s.fovc, reinterpret_cast<const TV *>(s.vis),
       reinterpret_cast<const TW *>(s.wgt), s.mask, gridding ? 1 : 0, a.negate_v ? -1.0 : 1.0,
-      d_out, vis_out);
+      d_out, vis_out, s.iw);
   cuda_check(cudaGetLastError(), "k_scan launch");
   g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
@@ -563,21 +635,28 @@ void launch_keys(Context &cx, const wsg_args &a, const Staged &s, bool gridding,
   k_keys<TV, TW, K><<<nb, 256, 0, cx.stream>>>(a.nrows, int(a.nchan), s.uvw, s.fovc,
                                                reinterpret_cast<const TV *>(s.vis),
                                                reinterpret_cast<const TW *>(s.wgt), s.mask,
-                                               gridding ? 1 : 0, g, keys, vals);
+                                               gridding ? 1 : 0, g, keys, vals, s.iw);
   cuda_check(cudaGetLastError(), "k_keys launch");
   g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
+// Records of the nvis active visibilities in sorted order: the sorted
+// positions pos (scratch of nvis_tot entries) from the sort's permutation
+// sidx, then the records built in visibility order and scattered to them
+// (the inactive visibilities sorted last and are skipped).
 template <typename R, typename TW, typename TV>
-void launch_records(Context &cx, size_t nvis, const wsg_args &a, const Staged &s, bool gridding,
-                    const DevGeom &g, const uint32_t *sidx, void *rec) {
-  int nb = launch_blocks(nvis, 256);
-  k_records<R, TV, TW><<<nb, 256, 0, cx.stream>>>(
-      nvis, int(a.nchan), sidx, s.uvw, s.fovc, reinterpret_cast<const TV *>(s.vis),
+void launch_records(size_t nvis, const wsg_args &a, const Staged &s, bool gridding,
+                    const DevGeom &g, const uint32_t *sidx, uint32_t *pos, void *rec,
+                    cudaStream_t st) {
+  const size_t nvis_tot = a.nrows * a.nchan;
+  k_rank<<<launch_blocks(nvis_tot, 256), 256, 0, st>>>(nvis_tot, sidx, pos);
+  cuda_check(cudaGetLastError(), "k_rank launch");
+  k_records<R, TV, TW><<<launch_blocks(nvis_tot, 256), 256, 0, st>>>(
+      nvis_tot, nvis, int(a.nchan), pos, s.uvw, s.fovc, reinterpret_cast<const TV *>(s.vis),
       reinterpret_cast<const TW *>(s.wgt), gridding ? 1 : 0, g,
-      reinterpret_cast<typename RecOf<R>::type *>(rec));
+      reinterpret_cast<typename RecOf<R>::type *>(rec), s.iw);
   cuda_check(cudaGetLastError(), "k_records launch");
-  g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+  g_kernel_launches.fetch_add(2, std::memory_order_relaxed);
 }
 
 // type-dispatch helpers over (weight type, vis type)
@@ -667,6 +746,9 @@ bool Context::prepare(const wsg_args &a, const Staged &s, bool gridding, void *v
   // keys are 4 or 8 bytes (the expected grid's width; sized for the wider)
   void *ka = b_keys_a.ensure(nvis_tot * 8);
   uint32_t *va = reinterpret_cast<uint32_t *>(b_vals_a.ensure(nvis_tot * 4));
+  // off the main stream, the scan must not overwrite the keys and indices
+  // that the previous call's sort and records may still be reading there
+  if (sst != stream) CK(cudaStreamWaitEvent(sst, ev_keys, 0));
   with_types(a, [&](auto *tw, auto *tv) {
     using TW = std::remove_pointer_t<decltype(tw)>;
     using TV = std::remove_pointer_t<decltype(tv)>;
@@ -677,7 +759,8 @@ bool Context::prepare(const wsg_args &a, const Staged &s, bool gridding, void *v
         k_scan_keys<TV, TW, K><<<nb, 256, 0, sst>>>(
             a.nrows, int(a.nchan), st.uvw, st.fovc, reinterpret_cast<const TV *>(st.vis),
             reinterpret_cast<const TW *>(st.wgt), st.mask, gridding ? 1 : 0,
-            a.negate_v ? -1.0 : 1.0, d_scan, reinterpret_cast<TV *>(zero_out), spec, kp, va);
+            a.negate_v ? -1.0 : 1.0, d_scan, reinterpret_cast<TV *>(zero_out), spec, kp, va,
+            st.iw);
       };
       if (spec.wide)
         go(reinterpret_cast<unsigned long long *>(ka));
@@ -788,7 +871,8 @@ bool Context::prepare(const wsg_args &a, const Staged &s, bool gridding, void *v
   with_types(a, [&](auto *tw, auto *tv) {
     using TW = std::remove_pointer_t<decltype(tw)>;
     using TV = std::remove_pointer_t<decltype(tv)>;
-    launch_records<R, TW, TV>(*this, gp.nvis, a, st, gridding, g, vb, rec);
+    // (the unsorted indices va are free after the sort: they hold the ranks)
+    launch_records<R, TW, TV>(gp.nvis, a, st, gridding, g, vb, va, rec, stream);
   });
 
   // chunk boundaries
@@ -807,6 +891,7 @@ bool Context::prepare(const wsg_args &a, const Staged &s, bool gridding, void *v
     select(reinterpret_cast<unsigned long long *>(kb));
   else
     select(reinterpret_cast<uint32_t *>(kb));
+  CK(cudaEventRecord(ev_keys, stream));
   mark("sort+records-submit");
   return true;
 }
@@ -1102,7 +1187,7 @@ bool Context::grid_core(const wsg_args &a, const Staged &s, double *img, bool ac
       fft_exec(h, band, bandf, dir, dbl);
     }
     // pruned transform along u: band rows of the image columns -> image rows
-    ColKernels<R>::run(gp.logM, true, ca, int(npl), stream);
+    ColKernels<R>::run(gp.logM, true, ca, int(npl), stream, d_err);
     CK(cudaEventRecord(ev[4], stream));
     ScreenArgs sa = make_screen(gp, cf_cur, cc, P);
     sa.pb0 = int(pb0);
@@ -1288,6 +1373,7 @@ void Context::check_device_error(const int *d_err) {
   int h = 0;
   CK(cudaMemcpyAsync(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost, stream));
   CK(cudaStreamSynchronize(stream));
+  if (h & 2) throw std::runtime_error("internal error: a staged copy into shared memory did not complete");
   if (h) throw std::runtime_error("internal error: a visibility record fell outside its tile");
 }
 
@@ -2031,7 +2117,7 @@ void Plan::enqueue_grid(const void *vis, void *const *dirty, int accumulate) {
       CF(cufftExecC2C(pj.fft, reinterpret_cast<cufftComplex *>(band),
                       reinterpret_cast<cufftComplex *>(band), CUFFT_INVERSE));
     ColArgs ca = make_col(gp, gp.nplanes, static_cast<char *>(tw_.p) + pj.tw_off, band, H_.p);
-    ColKernels<R>::run(gp.logM, true, ca, int(gp.nplanes), st);
+    ColKernels<R>::run(gp.logM, true, ca, int(gp.nplanes), st, d_err);
     if (accumulate) {
       if (a_.dirty_type == WSG_F64)
         k_load_image<double><<<nb, 256, 0, st>>>(npix, (const double *)dirty[j], img, 0);
@@ -2378,7 +2464,8 @@ StreamGridder::~StreamGridder() {
     for (DevBuf *d : {&b.uvw, &b.vis, &b.wgt, &b.mask}) d->release();
   }
   if (fft_) cufftDestroy(fft_);
-  for (DevBuf *b : {&band_, &H_, &img_, &cf_, &tw_, &fftwork_, &vout_, &fovc_, &scan_d_}) b->release();
+  for (DevBuf *b : {&band_, &H_, &img_, &cf_, &tw_, &fftwork_, &vout_, &fovc_, &scan_d_, &lambda_})
+    b->release();
   scan_h_.release();
 }
 
@@ -2442,7 +2529,10 @@ void StreamGridder::add_t(const Staged &s, size_t nrows) {
   int *counter = reinterpret_cast<int *>(reinterpret_cast<char *>(cx_.b_small.p) + 2048);
   int *d_nch = reinterpret_cast<int *>(reinterpret_cast<char *>(cx_.b_small.p) + 1024);
   int *d_err = reinterpret_cast<int *>(reinterpret_cast<char *>(cx_.b_small.p) + 3072);
-  CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
+  if (!err_armed_) {  // read back and cleared by finish()
+    CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
+    err_armed_ = true;
+  }
   CK(cudaMemsetAsync(counter, 0, sizeof(int), st));
   GridArgs ga{};
   ga.err = d_err;
@@ -2508,7 +2598,7 @@ void StreamGridder::check_extent(const Staged &s, size_t nrows) {
                                           reinterpret_cast<const double *>(fovc_.p),
                                           reinterpret_cast<const TV *>(s.vis),
                                           reinterpret_cast<const TW *>(s.wgt), s.mask, 1,
-                                          a_.negate_v ? -1.0 : 1.0, d, (TV *)nullptr);
+                                          a_.negate_v ? -1.0 : 1.0, d, (TV *)nullptr, s.iw);
   });
   cuda_check(cudaGetLastError(), "k_scan launch");
   g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
@@ -2529,6 +2619,28 @@ void StreamGridder::check_extent(const Staged &s, size_t nrows) {
           "a chunk's |u| or |v| exceeds the extent declared for the stream");
 }
 
+// WSClean multiplies each visibility's weight by the imaging weight of its
+// uv cell before gridding (MSGridderBase::readAndWeightVisibilities,
+// gridding/msgridderbase.cpp:583-590,640-659).  Here the lookup happens in
+// the scan and record kernels of each batch, from the finished grid of w.
+void StreamGridder::set_imaging_weights(const ImageWeightsGpu *w) {
+  if (!w) {
+    iw_ = ImgW{};
+    return;
+  }
+  require(w->finished(), "the imaging weights must be finished (wsg_weights_finish)");
+  require(w->device() == cx_.device, "the imaging weights live on another device");
+  flush_batch();  // rows added so far keep the weights they were added with
+  std::vector<double> l(freq_.size());
+  for (size_t c = 0; c < l.size(); ++c) l[c] = kSpeedOfLight / freq_[c];
+  CK(cudaStreamSynchronize(cx_.stream));  // an earlier table may still be read
+  double *d = reinterpret_cast<double *>(lambda_.ensure(l.size() * sizeof(double)));
+  CK(cudaMemcpy(d, l.data(), l.size() * sizeof(double), cudaMemcpyHostToDevice));
+  iw_.grid = w->grid_ptr();
+  iw_.lambda = d;
+  iw_.g = w->geometry();
+}
+
 // Sorts and spreads the current batch (after its copies) and switches to
 // the other one.
 void StreamGridder::flush_batch() {
@@ -2541,6 +2653,7 @@ void StreamGridder::flush_batch() {
   s.vis = b.vis.p;
   s.wgt = b.has_wgt ? b.wgt.p : nullptr;
   s.mask = b.has_mask ? reinterpret_cast<const uint8_t *>(b.mask.p) : nullptr;
+  s.iw = iw_;
   if (dbl_)
     add_t<double>(s, b.rows);
   else
@@ -2564,6 +2677,7 @@ void StreamGridder::add(size_t nrows, const double *uvw, const void *vis, const 
     flush_batch();
     Slot &sl = slots_[k_++ & 1];
     Staged s = stage(sl, nrows, uvw, vis, wgt, mask);
+    s.iw = iw_;
     if (dbl_)
       add_t<double>(s, nrows);
     else
@@ -2603,6 +2717,7 @@ void StreamGridder::add(size_t nrows, const double *uvw, const void *vis, const 
   s.vis = static_cast<char *>(b->vis.p) + r0 * nchan * vsz;
   s.wgt = wgt ? static_cast<char *>(b->wgt.p) + r0 * nchan * wsz : nullptr;
   s.mask = mask ? reinterpret_cast<const uint8_t *>(b->mask.p) + r0 * nchan : nullptr;
+  s.iw = iw_;
   check_extent(s, nrows);  // waits for the copies; a rejected chunk is not kept
   b->rows += nrows;
 }
@@ -2635,11 +2750,16 @@ void StreamGridder::finish_t(void *dirty, int accumulate) {
     CF(cufftExecC2C(fft_, reinterpret_cast<cufftComplex *>(band_.p),
                     reinterpret_cast<cufftComplex *>(band_.p), CUFFT_INVERSE));
   const size_t P = std::max<size_t>(1, H_.n / (npix * cs));
+  int *d_err = reinterpret_cast<int *>(reinterpret_cast<char *>(cx_.b_small.p) + 3072);
+  if (!err_armed_) {
+    CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
+    err_armed_ = true;
+  }
   for (size_t p0 = 0; p0 < g.nplanes; p0 += P) {
     const size_t np = std::min(P, g.nplanes - p0);
     // the band layout is [row][plane][nv]: a pass starts p0 planes into each row
     ColArgs ca = make_col(g, g.nplanes, tw_.p, static_cast<char *>(band_.p) + p0 * g.nv * cs, H_.p);
-    ColKernels<R>::run(g.logM, true, ca, int(np), st);
+    ColKernels<R>::run(g.logM, true, ca, int(np), st, d_err);
     ScreenArgs sa = make_screen(g, reinterpret_cast<const double *>(cf_.p), cc_, np);
     sa.pb0 = int(p0);
     sa.npl = int(np);
@@ -2655,7 +2775,8 @@ void StreamGridder::finish_t(void *dirty, int accumulate) {
   cuda_check(cudaGetLastError(), "k_store_image launch");
   if (!ddev) CK(cudaMemcpyAsync(dirty, dout, npix * dsz, cudaMemcpyDeviceToHost, st));
   CK(cudaMemsetAsync(band_.p, 0, band_.n, st));
-  CK(cudaStreamSynchronize(st));
+  err_armed_ = false;
+  cx_.check_device_error(d_err);  // synchronises the stream
 }
 
 void StreamGridder::finish(void *dirty, int accumulate) {
@@ -3379,7 +3500,8 @@ void ms2dirty_noalloc(const wsg_args &a, const void *vis, void *dirty, cudaStrea
       k_scan<TV, TW><<<nb, 256, 0, stream>>>(a.nrows, int(a.nchan), st.uvw, st.fovc,
                                              reinterpret_cast<const TV *>(st.vis),
                                              reinterpret_cast<const TW *>(st.wgt), st.mask, 1,
-                                             a.negate_v ? -1.0 : 1.0, d_scan, (TV *)nullptr);
+                                             a.negate_v ? -1.0 : 1.0, d_scan, (TV *)nullptr,
+                                             ImgW{});
     });
     cuda_check(cudaGetLastError(), "k_scan launch");
   }
@@ -3429,7 +3551,7 @@ void ms2dirty_noalloc(const wsg_args &a, const void *vis, void *dirty, cudaStrea
       using TV = std::remove_pointer_t<decltype(tv)>;
       k_keys<TV, TW, uint32_t><<<launch_blocks(a.nrows, 256), 256, 0, stream>>>(
           a.nrows, int(a.nchan), st.uvw, st.fovc, reinterpret_cast<const TV *>(st.vis),
-          reinterpret_cast<const TW *>(st.wgt), st.mask, 1, g, ka, va);
+          reinterpret_cast<const TW *>(st.wgt), st.mask, 1, g, ka, va, ImgW{});
     });
     cuda_check(cudaGetLastError(), "k_keys launch");
     size_t tmp = 0;
@@ -3443,11 +3565,8 @@ void ms2dirty_noalloc(const wsg_args &a, const void *vis, void *dirty, cudaStrea
     with_types(a, [&](auto *tw, auto *tv) {
       using TW = std::remove_pointer_t<decltype(tw)>;
       using TV = std::remove_pointer_t<decltype(tv)>;
-      k_records<float, TV, TW><<<launch_blocks(gp.nvis, 256), 256, 0, stream>>>(
-          gp.nvis, int(a.nchan), vb, st.uvw, st.fovc, reinterpret_cast<const TV *>(st.vis),
-          reinterpret_cast<const TW *>(st.wgt), 1, g, reinterpret_cast<RecF *>(rec));
+      launch_records<float, TW, TV>(gp.nvis, a, st, true, g, vb, va, rec, stream);
     });
-    cuda_check(cudaGetLastError(), "k_records launch");
     int *chunks = reinterpret_cast<int *>(ar.take((gp.nvis + 1) * sizeof(int)));
     ChunkStartPred<uint32_t> pred{kb, 2 * gp.lbits, 1024};
     thrust::counting_iterator<int> it(0);
@@ -3509,7 +3628,7 @@ void ms2dirty_noalloc(const wsg_args &a, const void *vis, void *dirty, cudaStrea
       ga.pb1 = int(pb0 + npl);
       GridKernels<float>::dispatch(gp.kernel.W, true, nsm, smem, stream, ga, g, kc);
       row_fft_f(logMv, band, (long long)(gp.band_rows * P), d_twv, +1, stream);
-      ColKernels<float>::run(gp.logM, true, ca, int(npl), stream);
+      ColKernels<float>::run(gp.logM, true, ca, int(npl), stream, d_err);
       ScreenArgs sa = make_screen(gp, d_cf, cc, P);
       sa.pb0 = int(pb0);
       sa.npl = int(npl);
@@ -3521,6 +3640,8 @@ void ms2dirty_noalloc(const wsg_args &a, const void *vis, void *dirty, cudaStrea
     int herr = 0;
     cuda_check(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, stream), "err D2H");
     cuda_check(cudaStreamSynchronize(stream), "sync");
+    if (herr & 2)
+      throw std::runtime_error("internal error: a staged copy into shared memory did not complete");
     if (herr) throw std::runtime_error("internal error: a visibility record fell outside its tile");
   }
   const int nb = launch_blocks(npix, 256);

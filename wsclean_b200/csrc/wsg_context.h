@@ -47,13 +47,15 @@ struct TuneChoice {
 bool tuned_choice(const wsg_args &a, size_t nvis, TuneChoice &out);
 void store_tuned(const wsg_args &a, size_t nvis, const TuneChoice &c);
 
-// Device pointers of one call's inputs.
+// Device pointers of one call's inputs (and the imaging weights to fold
+// into the visibility weights while gridding them).
 struct Staged {
   const double *uvw = nullptr;
   const double *fovc = nullptr;
   const void *vis = nullptr;
   const void *wgt = nullptr;
   const uint8_t *mask = nullptr;
+  ImgW iw;
 };
 
 class Context {
@@ -128,6 +130,10 @@ class Context {
   size_t slot_k = 0;
   cudaStream_t cpy = nullptr, d2h = nullptr;
   cudaEvent_t ev_start = nullptr, ev_in = nullptr, ev_done = nullptr, ev_scan = nullptr;
+  // the last use of the sort buffers (keys, indices, ranks) by the previous
+  // prepare(): a scan on the copy stream, which writes the next call's keys,
+  // waits for it
+  cudaEvent_t ev_keys = nullptr;
   // where prepare() scans (nullptr: the main stream) and puts f/c
   cudaStream_t scan_st = nullptr;
   DevBuf *fovc_buf = nullptr;
@@ -320,6 +326,8 @@ class StreamGridder {
   void predict_begin(const void *dirty);
   void predict(size_t nrows, const double *uvw, void *vis, const void *wgt, const uint8_t *mask);
   void stats(wsg_stats &out) const;
+  // Imaging weights folded into every later add (nullptr: none).
+  void set_imaging_weights(const class ImageWeightsGpu *w);
 
  private:
   struct Slot {
@@ -354,8 +362,10 @@ class StreamGridder {
   size_t batch_rows_ = 0;
   // the extent check of a chunk at add(): f/c on the device, the scan's
   // statistics and their page-locked read-back
-  DevBuf fovc_, scan_d_;
+  DevBuf fovc_, scan_d_, lambda_;
   PinnedBuf scan_h_;
+  ImgW iw_;
+  bool err_armed_ = false;  // the device error word was cleared for this gridding
   void check_extent(const Staged &s, size_t nrows);
   void copy_into(void *dst, const void *src, size_t bytes, PinnedBuf &pin);
   void flush_batch();
@@ -386,6 +396,11 @@ class ImageWeightsGpu {
   void apply(size_t nrows, size_t nchan, size_t npol, const double *uvw, const double *freq,
              const float *in, float *out);
   void get(double *grid, size_t *width, size_t *height, double *total);
+  // the finished grid, for lookups while visibilities are gridded
+  bool finished() const { return finished_; }
+  const double *grid_ptr() const { return reinterpret_cast<const double *>(grid_.p); }
+  WeightGrid geometry() const { return WeightGrid{int(W_), int(H_), psx_, psy_}; }
+  int device() const { return cx_.device; }
 
  private:
   const double *lambdas(size_t nchan, const double *freq);

@@ -21,6 +21,7 @@
 //               correction, added into the FP64 image         (grid2dirty_post2 :428-484, apply_global_corrections :1348-1400)
 #pragma once
 
+#include <cuda.h>  // CUtensorMap (the type only; no driver-API calls here)
 #include <cuda_runtime.h>
 #include <cstdint>
 
@@ -176,6 +177,33 @@ __device__ __forceinline__ K bin_key(const DevGeom &g, const VisPix &p) {
 }
 
 
+
+__device__ __forceinline__ bool weight_cell(const WeightGrid &g, double u, double v, int &x,
+                                            int &y) {
+  if (v < 0.0) {
+    u = -u;
+    v = -v;
+  }
+  x = int(floor(u * double(g.W) * g.psx + double(g.W / 2)));
+  y = int(floor(v * double(g.H) * g.psy));
+  return x >= 0 && x < g.W && y < g.H / 2;
+}
+
+// The visibility weight w (1 when there are none) times the imaging weight
+// of row r, channel c (raw uvw: v not negated).
+template <typename TW>
+__device__ __forceinline__ double weighted(const ImgW &iw, const double *__restrict__ uvw, size_t r,
+                                           int c, double w) {
+  if (!iw.grid) return w;
+  int x, y;
+  const double lam = iw.lambda[c];
+  const double f = weight_cell(iw.g, uvw[3 * r] / lam, uvw[3 * r + 1] / lam, x, y)
+                       ? iw.grid[size_t(x) + size_t(y) * iw.g.W]
+                       : 0.0;
+  const double p = w * f;
+  return sizeof(TW) == 4 ? double(float(p)) : p;
+}
+
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll
@@ -196,7 +224,7 @@ __device__ __forceinline__ void scan_rows(size_t nrows, int nchan, const double 
                                           const uint8_t *__restrict__ mask, int gridding,
                                           double vfac, ScanOut *out, TV *__restrict__ vis_out,
                                           const DevGeom &g, K *__restrict__ keys,
-                                          uint32_t *__restrict__ vals) {
+                                          uint32_t *__restrict__ vals, const ImgW &iw) {
   double lwmin = 1e300, lwmax = 0, lumax = 0, lvmax = 0;
   unsigned long long cnt = 0;
   for (size_t r = blockIdx.x * size_t(blockDim.x) + threadIdx.x; r < nrows;
@@ -208,7 +236,10 @@ __device__ __forceinline__ void scan_rows(size_t nrows, int nchan, const double 
       if (gridding) {
         TV x = vis[k];
         auto n = x.x * x.x + x.y * x.y;
-        if (wgt) n *= wgt[k];
+        if (iw.grid)
+          n *= decltype(n)(weighted<TW>(iw, uvw, r, c, wgt ? double(wgt[k]) : 1.0));
+        else if (wgt)
+          n *= wgt[k];
         if (mask) n *= mask[k];
         act = (n != 0);
       } else {
@@ -257,10 +288,11 @@ template <typename TV, typename TW>
 __global__ void k_scan(size_t nrows, int nchan, const double *__restrict__ uvw,
                        const double *__restrict__ fovc, const TV *__restrict__ vis,
                        const TW *__restrict__ wgt, const uint8_t *__restrict__ mask,
-                       int gridding, double vfac, ScanOut *out, TV *__restrict__ vis_out) {
+                       int gridding, double vfac, ScanOut *out, TV *__restrict__ vis_out,
+                       ImgW iw) {
   const DevGeom g{};
   scan_rows<TV, TW, false>(nrows, nchan, uvw, fovc, vis, wgt, mask, gridding, vfac, out, vis_out,
-                           g, (uint32_t *)nullptr, nullptr);
+                           g, (uint32_t *)nullptr, nullptr, iw);
 }
 
 // The scan with the keys of an expected geometry: when consecutive calls
@@ -271,9 +303,10 @@ __global__ void k_scan_keys(size_t nrows, int nchan, const double *__restrict__ 
                             const double *__restrict__ fovc, const TV *__restrict__ vis,
                             const TW *__restrict__ wgt, const uint8_t *__restrict__ mask,
                             int gridding, double vfac, ScanOut *out, TV *__restrict__ vis_out,
-                            DevGeom g, K *__restrict__ keys, uint32_t *__restrict__ vals) {
+                            DevGeom g, K *__restrict__ keys, uint32_t *__restrict__ vals,
+                            ImgW iw) {
   scan_rows<TV, TW, true, K>(nrows, nchan, uvw, fovc, vis, wgt, mask, gridding, vfac, out,
-                             vis_out, g, keys, vals);
+                             vis_out, g, keys, vals, iw);
 }
 
 // --------------------------------------------------------------- k_keys
@@ -283,7 +316,7 @@ __global__ void k_keys(size_t nrows, int nchan, const double *__restrict__ uvw,
                        const double *__restrict__ fovc, const TV *__restrict__ vis,
                        const TW *__restrict__ wgt, const uint8_t *__restrict__ mask,
                        int gridding, DevGeom g, K *__restrict__ keys,
-                       uint32_t *__restrict__ vals) {
+                       uint32_t *__restrict__ vals, ImgW iw) {
   for (size_t r = blockIdx.x * size_t(blockDim.x) + threadIdx.x; r < nrows;
        r += size_t(gridDim.x) * blockDim.x) {
     double u = uvw[3 * r], v = g.vfac * uvw[3 * r + 1], w = uvw[3 * r + 2];
@@ -293,7 +326,10 @@ __global__ void k_keys(size_t nrows, int nchan, const double *__restrict__ uvw,
       if (gridding) {
         TV x = vis[k];
         auto n = x.x * x.x + x.y * x.y;
-        if (wgt) n *= wgt[k];
+        if (iw.grid)
+          n *= decltype(n)(weighted<TW>(iw, uvw, r, c, wgt ? double(wgt[k]) : 1.0));
+        else if (wgt)
+          n *= wgt[k];
         if (mask) n *= mask[k];
         act = (n != 0);
       } else {
@@ -314,46 +350,72 @@ __global__ void k_keys(size_t nrows, int nchan, const double *__restrict__ uvw,
 
 // ------------------------------------------------------------ k_records
 
+// The record of visibility k (row k / nchan, channel k % nchan).
 template <typename R, typename TV, typename TW>
-__global__ void k_records(size_t nvis, int nchan, const uint32_t *__restrict__ sidx,
+__device__ __forceinline__ typename RecOf<R>::type make_record(
+    uint32_t k, int nchan, const double *__restrict__ uvw, const double *__restrict__ fovc,
+    const TV *__restrict__ vis, const TW *__restrict__ wgt, int gridding, const DevGeom &g,
+    const ImgW &iw) {
+  using Rec = typename RecOf<R>::type;
+  size_t r = k / uint32_t(nchan);
+  int c = int(k - r * uint32_t(nchan));
+  double f = fovc[c];
+  double u = uvw[3 * r], v = g.vfac * uvw[3 * r + 1], w = uvw[3 * r + 2];
+  VisPix p;
+  vis_pixel(g, u * f, v * f, w * f, p);
+  double wk = wgt ? double(wgt[k]) : 1.0;
+  if (gridding) wk = weighted<TW>(iw, uvw, r, c, wk);
+  double2 ph = make_double2(1.0, 0.0);
+  if (g.shifting) ph = cexp_turns((u * g.lshift + v * g.mshift + w * g.nshift) * f);
+  Rec o;
+  o.xu = R(p.xu);
+  o.xv = R(p.xv);
+  o.xw = R(p.xw);
+  o.iuv = (uint32_t(p.iu0 + g.nsafe) << 16) | uint32_t(p.iv0 + g.nsafe);
+  o.mp = uint32_t(p.iw);
+  if (gridding) {
+    TV x = vis[k];
+    double xr = double(x.x), xi = double(x.y);
+    double vr = (xr * ph.x - xi * ph.y) * wk;
+    double vi = (xr * ph.y + xi * ph.x) * wk;
+    if (p.flip) vi = -vi;
+    o.vr = R(vr);
+    o.vi = R(vi);
+    o.idx = k;
+  } else {
+    // output = wgt * exp(-2 pi i phase) * (flip ? conj(S) : S)
+    o.vr = R(wk * ph.x);
+    o.vi = R(-wk * ph.y);
+    o.idx = k | (p.flip ? 0x80000000u : 0u);
+  }
+  return o;
+}
+
+// Sorted position of every visibility: pos[sidx[s]] = s (the inactive
+// ones sort last, at positions >= the active count, and have no record).
+__global__ void k_rank(size_t n, const uint32_t *__restrict__ sidx, uint32_t *__restrict__ pos) {
+  for (size_t s = blockIdx.x * size_t(blockDim.x) + threadIdx.x; s < n;
+       s += size_t(gridDim.x) * blockDim.x)
+    pos[sidx[s]] = uint32_t(s);
+}
+
+// Records in visibility order: thread k reads visibility k's coordinates,
+// value and weight (coalesced; a row's uvw is shared by its channels) and
+// writes its record to the sorted slot pos[k] -- one aligned 32-byte (64 in
+// FP64) record per write, so the scatter moves whole sectors, where a
+// gather in sorted order would fetch a sector for every 8-byte visibility
+// and every 24-byte uvw row.
+template <typename R, typename TV, typename TW>
+__global__ void k_records(size_t nvis_tot, size_t nvis, int nchan, const uint32_t *__restrict__ pos,
                           const double *__restrict__ uvw, const double *__restrict__ fovc,
                           const TV *__restrict__ vis, const TW *__restrict__ wgt,
-                          int gridding, DevGeom g, typename RecOf<R>::type *__restrict__ rec) {
-  using Rec = typename RecOf<R>::type;
-  for (size_t s = blockIdx.x * size_t(blockDim.x) + threadIdx.x; s < nvis;
-       s += size_t(gridDim.x) * blockDim.x) {
-    uint32_t k = sidx[s];
-    size_t r = k / uint32_t(nchan);
-    int c = int(k - r * uint32_t(nchan));
-    double f = fovc[c];
-    double u = uvw[3 * r], v = g.vfac * uvw[3 * r + 1], w = uvw[3 * r + 2];
-    VisPix p;
-    vis_pixel(g, u * f, v * f, w * f, p);
-    double wk = wgt ? double(wgt[k]) : 1.0;
-    double2 ph = make_double2(1.0, 0.0);
-    if (g.shifting) ph = cexp_turns((u * g.lshift + v * g.mshift + w * g.nshift) * f);
-    Rec o;
-    o.xu = R(p.xu);
-    o.xv = R(p.xv);
-    o.xw = R(p.xw);
-    o.iuv = (uint32_t(p.iu0 + g.nsafe) << 16) | uint32_t(p.iv0 + g.nsafe);
-    o.mp = uint32_t(p.iw);
-    if (gridding) {
-      TV x = vis[k];
-      double xr = double(x.x), xi = double(x.y);
-      double vr = (xr * ph.x - xi * ph.y) * wk;
-      double vi = (xr * ph.y + xi * ph.x) * wk;
-      if (p.flip) vi = -vi;
-      o.vr = R(vr);
-      o.vi = R(vi);
-      o.idx = k;
-    } else {
-      // output = wgt * exp(-2 pi i phase) * (flip ? conj(S) : S)
-      o.vr = R(wk * ph.x);
-      o.vi = R(-wk * ph.y);
-      o.idx = k | (p.flip ? 0x80000000u : 0u);
-    }
-    rec[s] = o;
+                          int gridding, DevGeom g, typename RecOf<R>::type *__restrict__ rec,
+                          ImgW iw) {
+  for (size_t k = blockIdx.x * size_t(blockDim.x) + threadIdx.x; k < nvis_tot;
+       k += size_t(gridDim.x) * blockDim.x) {
+    const uint32_t p = pos[k];
+    if (p >= nvis) continue;
+    rec[p] = make_record<R, TV, TW>(uint32_t(k), nchan, uvw, fovc, vis, wgt, gridding, g, iw);
   }
 }
 
@@ -1404,6 +1466,52 @@ __device__ __forceinline__ void col_tail(C *cur, C *oth, const C *tw, int t, C (
   }
 }
 
+// In-place col_tail: the data in buf, each middle stage reading all its
+// inputs before a barrier and writing back in place; the last stage leaves
+// its outputs in o[q] = X[t + TPF q].
+template <typename C, int M, int NS, int TPF, int SIGN>
+__device__ __forceinline__ void col_tail_inplace(C *buf, const C *tw, int t, C (&o)[16]) {
+  if constexpr (M / NS > 16) {
+    C v[16];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r] = buf[fpad(t + r * TPF)];
+    const int k = t & (NS - 1);
+    constexpr int off = TwOffset<NS>::value;
+#pragma unroll
+    for (int r = 1; r < 16; ++r) {
+      C w = tw[off + (r - 1) * NS + k];
+      if (SIGN < 0) w.y = -w.y;
+      v[r] = cmul(v[r], w);
+    }
+    dft_reg<16>(v, SIGN);
+    const int d = (t / NS) * NS * 16 + k;
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 16; ++r) buf[fpad(d + r * NS)] = v[r];
+    __syncthreads();
+    col_tail_inplace<C, M, NS * 16, TPF, SIGN>(buf, tw, t, o);
+  } else {
+    constexpr int RL = M / NS, IT = 16 / RL;
+    constexpr int off = TwOffset<NS>::value;
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+      const int j = t + TPF * it;
+      C v[RL];
+#pragma unroll
+      for (int r = 0; r < RL; ++r) v[r] = buf[fpad(j + r * NS)];
+#pragma unroll
+      for (int r = 1; r < RL; ++r) {
+        C w = tw[off + (r - 1) * NS + j];
+        if (SIGN < 0) w.y = -w.y;
+        v[r] = cmul(v[r], w);
+      }
+      dft_reg<RL>(v, SIGN);
+#pragma unroll
+      for (int r = 0; r < RL; ++r) o[it + r * IT] = v[r];
+    }
+  }
+}
+
 // Number of middle (radix-16, not last) stages of an M-point transform.
 template <int M>
 struct ColMid {
@@ -1544,6 +1652,191 @@ k_ucol_bwd(ColArgs a) {
   }
 }
 
+// ---- the band columns staged by the tensor memory accelerator ----
+//
+// k_ucol_bwd_tma is k_ucol_bwd made persistent: each CTA loops over (plane,
+// column group) items, and while it transforms one, the tensor memory
+// accelerator (cp.async.bulk.tensor, 2-D boxes of NB adjacent columns by up
+// to 256 band rows, no multicast) copies the next item's band columns into a
+// shared staging buffer, completing on an mbarrier.  The band loads then
+// overlap the FFTs instead of stalling each CTA at its start, and the stage
+// twiddles are loaded once per CTA instead of once per column group.  The
+// transforms run in place in one buffer per column (the staging buffer
+// takes the place of the second one).
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return uint32_t(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+// One bounded attempt; true once the phase of the given parity completed.
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// Waits for the phase with an iteration limit; false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+  for (int i = 0; i < (1 << 22); ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y,
+                                            uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Staging of one item: NB adjacent columns of the band rows, in two regions
+// that start on box boundaries (every box lands 4 KB-aligned): rows [0, L]
+// (u >= 0) in region 1, rows (L, 2L] (u = -L..-1) in region 2 after it; the
+// last box of a region may run past its rows (the copy engine fills rows
+// past the band with zeros) into the region's pad.  With the full band,
+// region 1 holds all M rows.
+template <typename R, int M>
+struct TmaCfg {
+  static constexpr int NB = ColCfg<R, M>::NB;
+  static constexpr int BR = 256;                 // rows per box (M >= 256)
+  static constexpr int ROWS = M + 2 * BR;        // staging rows
+  static constexpr int BOX_BYTES = BR * NB * 2 * int(sizeof(R));
+  static constexpr size_t stage_bytes() { return size_t(ROWS) * NB * 2 * sizeof(R); }
+};
+
+// Boxes of region 1 (rows [0, L] or all rows with the full band).
+__device__ __forceinline__ int tma_boxes1(const ColArgs &a, int M, int BR) {
+  return a.band_full ? M / BR : (a.L + 1 + BR - 1) / BR;
+}
+
+// Issues the boxes of one item (plane lp, first column j0) into the staging
+// buffer and arms the barrier with their bytes (one thread).
+template <typename R, int M>
+__device__ __forceinline__ void tma_issue_item(const ColArgs &a, const CUtensorMap *map,
+                                               typename Cplx<R>::type *stage, uint64_t *bar,
+                                               int lp, int j0) {
+  using Cfg = TmaCfg<R, M>;
+  int jx = j0 + a.nv - a.ny / 2;
+  jx -= (jx >= a.nv) ? a.nv : 0;
+  const int x = 2 * (lp * a.nv + jx);
+  const int n1 = tma_boxes1(a, M, Cfg::BR);
+  const int n2 = a.band_full ? 0 : (a.L + Cfg::BR - 1) / Cfg::BR;
+  mbar_expect_tx(bar, uint32_t((n1 + n2) * Cfg::BOX_BYTES));
+  for (int k = 0; k < n1; ++k)
+    tma_load_2d(stage + size_t(k * Cfg::BR) * Cfg::NB, map, x, k * Cfg::BR, bar);
+  for (int k = 0; k < n2; ++k)
+    tma_load_2d(stage + size_t((n1 + k) * Cfg::BR) * Cfg::NB, map, x, a.L + 1 + k * Cfg::BR, bar);
+}
+
+// In-place variant of col_fft: v[q] = x[t + TPF q] -> o[q] = X[t + TPF q],
+// every exchange through the one buffer buf, with a barrier between the
+// reads and the writes of each stage.
+template <typename C, int M, int TPF, int SIGN>
+__device__ __forceinline__ void col_fft_inplace(C (&v)[16], C *buf, const C *tw, int t,
+                                                C (&o)[16]) {
+  dft_reg<16>(v, SIGN);
+  __syncthreads();  // earlier readers of buf are done
+#pragma unroll
+  for (int r = 0; r < 16; ++r) buf[fpad(16 * t + r)] = v[r];
+  __syncthreads();
+  col_tail_inplace<C, M, 16, TPF, SIGN>(buf, tw, t, o);
+}
+
+template <typename R, int LOGM>
+__global__ void __launch_bounds__(ColCfg<R, (1 << LOGM)>::THREADS, ColCfg<R, (1 << LOGM)>::MINB)
+k_ucol_bwd_tma(ColArgs a, const __grid_constant__ CUtensorMap tmap, int npl, int *err) {
+  using C = typename Cplx<R>::type;
+  constexpr int M = 1 << LOGM, TPF = ColCfg<R, M>::TPF;
+  using Cfg = TmaCfg<R, M>;
+  constexpr int NB = Cfg::NB;
+  constexpr int BL = FftBuf<M>::value;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  // the staging buffer starts on a 128-byte boundary (the host adds 128 bytes)
+  const uint32_t mis = smem_u32(smem_raw) & 127u;
+  C *stage = reinterpret_cast<C *>(smem_raw + (mis ? 128u - mis : 0u));   // [ROWS][NB]
+  C *bufall = stage + size_t(Cfg::ROWS) * NB;                               // [NB][BL]
+  C *tws = bufall + size_t(NB) * BL;                                        // [M]
+  __shared__ __align__(8) uint64_t bar;
+  const int grp = threadIdx.x / TPF, t = threadIdx.x - grp * TPF;
+  C *A = bufall + size_t(grp) * BL;
+  const int npairs = (a.ny + NB - 1) / NB;
+  const int nitems = npairs * npl;
+  const C *twB = reinterpret_cast<const C *>(a.twB);
+  const C *twQ = reinterpret_cast<const C *>(a.twQ);
+  const int reg2 = tma_boxes1(a, M, Cfg::BR) * Cfg::BR;  // first staging row of region 2
+  fill_table<C, M, ColCfg<R, M>::THREADS>(tws, reinterpret_cast<const C *>(a.twM));
+  int item = blockIdx.x;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (item < nitems)
+      tma_issue_item<R, M>(a, &tmap, stage, &bar, item / npairs, (item % npairs) * NB);
+  }
+  __syncthreads();  // the barrier is initialised before anyone waits on it
+  const int half_nu = a.nu / 2, half_nx = a.nx / 2;
+  for (uint32_t parity = 0; item < nitems; item += gridDim.x, parity ^= 1u) {
+    const int lp = item / npairs, j = (item % npairs) * NB + grp;
+    if (!mbar_wait(&bar, parity)) {  // the copy did not complete: report and stop
+      if (threadIdx.x == 0) atomicOr(err, 2);
+      mbar_wait(&bar, parity);
+      return;
+    }
+    // the untwisted band values at slots t + TPF q (zero between the halves)
+    C g[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const int b = t + TPF * q;
+      g[q].x = R(0);
+      g[q].y = R(0);
+      if (a.band_full || b <= a.L)
+        g[q] = stage[size_t(b) * NB + grp];
+      else if (b >= M - a.L)
+        g[q] = stage[size_t(reg2 + b - (M - a.L)) * NB + grp];
+    }
+    __syncthreads();  // the staging buffer is free for the next item's boxes
+    const int next = item + gridDim.x;
+    if (threadIdx.x == 0 && next < nitems)
+      tma_issue_item<R, M>(a, &tmap, stage, &bar, next / npairs, (next % npairs) * NB);
+    const bool jv = j < a.ny;
+    C *rowp = reinterpret_cast<C *>(a.H) + (size_t(lp) * a.ny + (jv ? j : 0)) * a.nx;
+    for (int k2 = 0; k2 < a.K; ++k2) {
+      C v[16];
+      if (k2 == 0) {
+#pragma unroll
+        for (int q = 0; q < 16; ++q) v[q] = g[q];
+      } else {
+        const C base = __ldg(&twB[k2 * TPF + t]);
+#pragma unroll
+        for (int q = 0; q < 16; ++q)
+          v[q] = cmul(g[q], col_twist<C, TPF>(a, twB, twQ, k2, t, q, M, base));
+      }
+      C o[16];
+      col_fft_inplace<C, M, TPF, +1>(v, A, tws, t, o);
+      if (jv) {
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          const int k = a.K * (t + TPF * q) + k2;
+          const int i = (k < half_nu ? k : k - a.nu) + half_nx;
+          if (i >= 0 && i < a.nx) rowp[i] = o[q];
+        }
+      }
+    }
+  }
+}
+
 // dirty2ms direction, the exact transpose: H image rows -> band rows of the
 // image columns, forward (-) transform along u.  Band entries of other
 // columns are left untouched (zeroed by the caller).  TWS: the twist tables
@@ -1676,22 +1969,6 @@ k_row_fft(void *data, long long rows, const void *twv, int sign) {
 // of summed visibility weights over the v >= 0 half plane, finished into
 // natural, uniform or Briggs imaging weights, then looked up per visibility.
 // (u, v) are in wavelengths, u / lambda with lambda = c / f per channel.
-
-struct WeightGrid {
-  int W, H;        // grid is W x H/2
-  double psx, psy; // pixel scales (radians)
-};
-
-__device__ __forceinline__ bool weight_cell(const WeightGrid &g, double u, double v, int &x,
-                                            int &y) {
-  if (v < 0.0) {
-    u = -u;
-    v = -v;
-  }
-  x = int(floor(u * double(g.W) * g.psx + double(g.W / 2)));
-  y = int(floor(v * double(g.H) * g.psy));
-  return x >= 0 && x < g.W && y < g.H / 2;
-}
 
 __global__ void k_weights_grid(size_t nrows, int nchan, int npol, const double *__restrict__ uvw,
                                const double *__restrict__ lambda, const float *__restrict__ wgt,

@@ -190,6 +190,24 @@ struct Facet {
 Facet tuning_facet(size_t npix_x, size_t npix_y, int nfx, int nfy, int ifx, int ify,
                    double pixsize_x, double pixsize_y, double center_x, double center_y);
 
+// Geometry of an ImageWeights grid (structures/imageweights.h:73-102): the
+// grid is W x H/2 cells over the v >= 0 half plane.
+struct WeightGrid {
+  int W, H;
+  double psx, psy;  // pixel scales (radians)
+};
+
+// Imaging weights looked up per visibility (device pointers; grid ==
+// nullptr: none) while the visibilities are scanned and their records are
+// built: the finished ImageWeights grid and each channel's wavelength.  The
+// visibility weight becomes weight x imaging weight, rounded to float when
+// the weights are float (as wsg_weights_apply would have stored it).
+struct ImgW {
+  const double *grid = nullptr;
+  const double *lambda = nullptr;
+  WeightGrid g{};
+};
+
 // Nominal device bytes for one pass with `planes` planes resident.
 size_t plan_bytes(const GridPlan &g, size_t planes, bool gridding);
 

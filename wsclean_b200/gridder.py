@@ -636,6 +636,13 @@ class Stream:
         L.check(L.lib().wsg_stream_get_stats(self._h, ctypes.byref(s)))
         return s.as_dict()
 
+    def set_imaging_weights(self, weights):
+        """Fold a finished ``ImageWeights`` into every later ``add``: each
+        visibility is gridded with weight x the imaging weight of its uv cell,
+        looked up on the device (None turns it off)."""
+        L.check(L.lib().wsg_stream_set_imaging_weights(self._h, weights._h if weights else None))
+        self._imaging_weights = weights
+
 
 class ImageWeights:
     """WSClean's ImageWeights on the GPU (``wsg_weights_*``): ``grid`` the
