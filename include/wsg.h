@@ -344,7 +344,11 @@ int wsg_stream_create(wsg_ctx *ctx, const wsg_args *a, double wmin, double wmax,
 int wsg_stream_destroy(wsg_stream *s);
 /* Adds nrows rows (uvw nrows x 3, vis nrows x nchan, wgt/mask or NULL).
  * After a prediction (wsg_stream_predict_begin) the first add starts a new
- * gridding on a cleared grid, as a major cycle's Invert follows its Predict. */
+ * gridding on a cleared grid, as a major cycle's Invert follows its Predict.
+ * Rows are checked against the declared extent when their batch is sorted:
+ * a chunk with an active visibility outside it makes the wsg_stream_add
+ * that spreads its batch, or wsg_stream_finish, fail with WSG_ERR_INVALID,
+ * and that batch is dropped. */
 int wsg_stream_add(wsg_stream *s, size_t nrows, const double *uvw, const void *vis,
                    const void *wgt, const uint8_t *mask);
 /* Transforms the accumulated grid into dirty (or adds it when accumulate);

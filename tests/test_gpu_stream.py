@@ -112,8 +112,10 @@ def test_stream_rejects_chunk_outside_extent():
     wide[:, 2] *= 3.0
     with G.Stream(freq, 64, 64, px, px, 1e-5, ext, **KW) as s:
         s.add(uvw[:500], vis[:500])
+        # the rows are checked when their batch is sorted: at the latest by finish()
         with pytest.raises(L.InvalidArgument):
             s.add(wide, vis[500:])
+            s.finish()
 
 
 def test_stream_predict_then_grid(cfg5):

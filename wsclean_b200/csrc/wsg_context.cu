@@ -2464,9 +2464,7 @@ StreamGridder::~StreamGridder() {
     for (DevBuf *d : {&b.uvw, &b.vis, &b.wgt, &b.mask}) d->release();
   }
   if (fft_) cufftDestroy(fft_);
-  for (DevBuf *b : {&band_, &H_, &img_, &cf_, &tw_, &fftwork_, &vout_, &fovc_, &scan_d_, &lambda_})
-    b->release();
-  scan_h_.release();
+  for (DevBuf *b : {&band_, &H_, &img_, &cf_, &tw_, &fftwork_, &vout_, &lambda_}) b->release();
 }
 
 // Planes per pass of the final transforms (the u-transformed rows of a pass
@@ -2570,55 +2568,6 @@ void StreamGridder::copy_into(void *dst, const void *src, size_t bytes, PinnedBu
   CK(cudaMemcpyAsync(dst, pin.p, bytes, cudaMemcpyHostToDevice, copy_));
 }
 
-// Rejects a chunk (device copies on the copy stream) with an active
-// visibility outside the declared extent, as prepare() does for the fixed
-// grid: the chunk's visibility scan runs on the copy stream right after its
-// copies, so the check does not wait for the spread of an earlier batch.
-void StreamGridder::check_extent(const Staged &s, size_t nrows) {
-  const size_t nchan = a_.nchan;
-  if (fovc_.n == 0) {
-    std::vector<double> f(nchan);
-    for (size_t c = 0; c < nchan; ++c) f[c] = freq_[c] / kSpeedOfLight;
-    CK(cudaMemcpy(fovc_.ensure(nchan * sizeof(double)), f.data(), nchan * sizeof(double),
-                  cudaMemcpyHostToDevice));
-  }
-  ScanOut *d = reinterpret_cast<ScanOut *>(scan_d_.ensure(sizeof(ScanOut)));
-  ScanOut *h = reinterpret_cast<ScanOut *>(scan_h_.ensure(sizeof(ScanOut)));
-  *h = ScanOut{};
-  h->wmin_bits = 0x7ff0000000000000ull;
-  CK(cudaMemcpyAsync(d, h, sizeof(ScanOut), cudaMemcpyHostToDevice, copy_));
-  wsg_args ac = a_;
-  ac.nrows = nrows;
-  ac.wgt = s.wgt;
-  with_types(ac, [&](auto *tw, auto *tv) {
-    using TW = std::remove_pointer_t<decltype(tw)>;
-    using TV = std::remove_pointer_t<decltype(tv)>;
-    const int nb = std::min(launch_blocks(nrows, 256), cx_.num_sms * 8);
-    k_scan<TV, TW><<<nb, 256, 0, copy_>>>(nrows, int(nchan), s.uvw,
-                                          reinterpret_cast<const double *>(fovc_.p),
-                                          reinterpret_cast<const TV *>(s.vis),
-                                          reinterpret_cast<const TW *>(s.wgt), s.mask, 1,
-                                          a_.negate_v ? -1.0 : 1.0, d, (TV *)nullptr, s.iw);
-  });
-  cuda_check(cudaGetLastError(), "k_scan launch");
-  g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
-  CK(cudaMemcpyAsync(h, d, sizeof(ScanOut), cudaMemcpyDeviceToHost, copy_));
-  CK(cudaStreamSynchronize(copy_));
-  if (h->nvis == 0) return;
-  auto bits2d = [](unsigned long long b) {
-    double x;
-    std::memcpy(&x, &b, 8);
-    return x;
-  };
-  const GridPlan &g = gp_;
-  auto within = [](double x, double lim) { return x <= lim * (1.0 + 1e-12) + 1e-9; };
-  require(bits2d(h->wmin_bits) >= g.wmin_d * (1.0 - 1e-12) - 1e-9 &&
-              within(bits2d(h->wmax_bits), g.wmax_d),
-          "a chunk's |w| range lies outside the extent declared for the stream");
-  require(within(bits2d(h->umax_bits), g.umax) && within(bits2d(h->vmax_bits), g.vmax),
-          "a chunk's |u| or |v| exceeds the extent declared for the stream");
-}
-
 // WSClean multiplies each visibility's weight by the imaging weight of its
 // uv cell before gridding (MSGridderBase::readAndWeightVisibilities,
 // gridding/msgridderbase.cpp:583-590,640-659).  Here the lookup happens in
@@ -2642,10 +2591,14 @@ void StreamGridder::set_imaging_weights(const ImageWeightsGpu *w) {
 }
 
 // Sorts and spreads the current batch (after its copies) and switches to
-// the other one.
+// the other one.  The batch's scan checks its rows against the declared
+// extent (prepare() with the fixed grid); a batch that fails is dropped.
 void StreamGridder::flush_batch() {
   Batch &b = batch_[bcur_];
   if (b.rows == 0) return;
+  const size_t rows = b.rows;
+  b.rows = 0;
+  bcur_ ^= 1;
   CK(cudaEventRecord(b.filled, copy_));
   CK(cudaStreamWaitEvent(cx_.stream, b.filled, 0));
   Staged s;
@@ -2655,12 +2608,10 @@ void StreamGridder::flush_batch() {
   s.mask = b.has_mask ? reinterpret_cast<const uint8_t *>(b.mask.p) : nullptr;
   s.iw = iw_;
   if (dbl_)
-    add_t<double>(s, b.rows);
+    add_t<double>(s, rows);
   else
-    add_t<float>(s, b.rows);
+    add_t<float>(s, rows);
   CK(cudaEventRecord(b.spread, cx_.stream));
-  b.rows = 0;
-  bcur_ ^= 1;
 }
 
 void StreamGridder::add(size_t nrows, const double *uvw, const void *vis, const void *wgt,
@@ -2712,13 +2663,7 @@ void StreamGridder::add(size_t nrows, const double *uvw, const void *vis, const 
   if (wgt)
     copy_into(static_cast<char *>(b->wgt.p) + r0 * nchan * wsz, wgt, nrows * nchan * wsz, sl.h_wgt);
   if (mask) copy_into(static_cast<char *>(b->mask.p) + r0 * nchan, mask, nrows * nchan, sl.h_mask);
-  Staged s;
-  s.uvw = reinterpret_cast<const double *>(static_cast<char *>(b->uvw.p) + r0 * 3 * sizeof(double));
-  s.vis = static_cast<char *>(b->vis.p) + r0 * nchan * vsz;
-  s.wgt = wgt ? static_cast<char *>(b->wgt.p) + r0 * nchan * wsz : nullptr;
-  s.mask = mask ? reinterpret_cast<const uint8_t *>(b->mask.p) + r0 * nchan : nullptr;
-  s.iw = iw_;
-  check_extent(s, nrows);  // waits for the copies; a rejected chunk is not kept
+  CK(cudaStreamSynchronize(copy_));
   b->rows += nrows;
 }
 

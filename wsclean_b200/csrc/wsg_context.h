@@ -360,13 +360,9 @@ class StreamGridder {
   Batch batch_[2];
   int bcur_ = 0;
   size_t batch_rows_ = 0;
-  // the extent check of a chunk at add(): f/c on the device, the scan's
-  // statistics and their page-locked read-back
-  DevBuf fovc_, scan_d_, lambda_;
-  PinnedBuf scan_h_;
+  DevBuf lambda_;  // channel wavelengths of the imaging-weight lookup
   ImgW iw_;
   bool err_armed_ = false;  // the device error word was cleared for this gridding
-  void check_extent(const Staged &s, size_t nrows);
   void copy_into(void *dst, const void *src, size_t bytes, PinnedBuf &pin);
   void flush_batch();
 

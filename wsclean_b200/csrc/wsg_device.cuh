@@ -1808,8 +1808,12 @@ k_ucol_bwd_tma(ColArgs a, const __grid_constant__ CUtensorMap tmap, int npl, int
     }
     __syncthreads();  // the staging buffer is free for the next item's boxes
     const int next = item + gridDim.x;
-    if (threadIdx.x == 0 && next < nitems)
+    if (threadIdx.x == 0 && next < nitems) {
+      // order the reads above (generic proxy) before the copy engine's
+      // writes to the same buffer (async proxy)
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       tma_issue_item<R, M>(a, &tmap, stage, &bar, next / npairs, (next % npairs) * NB);
+    }
     const bool jv = j < a.ny;
     C *rowp = reinterpret_cast<C *>(a.H) + (size_t(lp) * a.ny + (jv ? j : 0)) * a.nx;
     for (int k2 = 0; k2 < a.K; ++k2) {
