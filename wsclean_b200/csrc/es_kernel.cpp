@@ -626,7 +626,7 @@ size_t plan_bytes(const GridPlan &g, size_t planes, bool gridding) {
   const size_t cs = g.fp32 ? 8 : 16;
   // both directions keep the grid and its v transform apart
   (void)gridding;
-  return planes * cs * (2 * g.band_rows * g.nv + g.ny * g.nx);
+  return planes * cs * (2 * g.band_rows * g.nv + g.ny * g.hrow());
 }
 
 }  // namespace wsg

@@ -208,6 +208,14 @@ void Context::synchronize() {
     err_pending = false;
     check_device_error(reinterpret_cast<const int *>(reinterpret_cast<char *>(b_small.p) + 3072));
   }
+  for (int *w : plan_err) {
+    int h = 0;
+    CK(cudaMemcpy(&h, w, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h == 0) continue;
+    CK(cudaMemset(w, 0, sizeof(int)));
+    if (h & 2) throw std::runtime_error("internal error: a staged copy into shared memory did not complete");
+    throw std::runtime_error("internal error: a visibility record fell outside its tile");
+  }
 }
 
 void Context::release_buffers() {
@@ -543,25 +551,73 @@ struct ColKernels {
             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
       return false;
-    const size_t smem = Cfg::stage_bytes() +
+    const size_t base = Cfg::stage_bytes() +
                         (size_t(NB) * FftBuf<M>::value + M) * 2 * sizeof(R) + 128;
-    auto *kern = k_ucol_bwd_tma<R, LOGM>;
+    // the twist tables go to shared memory too when that costs no resident CTA
+    const size_t extra = size_t(a.K) * (M / 16 + 32) * 2 * sizeof(R);
+    const bool tws = twist_tables_fit(base, extra);
+    const size_t smem = tws ? base + extra : base;
+    auto *kern = tws ? k_ucol_bwd_tma<R, LOGM, true> : k_ucol_bwd_tma<R, LOGM, false>;
     smem_attr(kern, smem);
-    static int per_sm = -1;  // resident CTAs per SM (one instantiation, one answer)
-    if (per_sm < 0) {
+    static int per_sm[2] = {-1, -1};  // resident CTAs per SM of each instantiation
+    if (per_sm[tws] < 0) {
       int n = 0;
       cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, ColCfg<R, M>::THREADS,
                                                                smem),
                  "occupancy");
-      per_sm = std::max(n, 1);
+      per_sm[tws] = std::max(n, 1);
     }
     int dev = 0, nsm = 148;
     cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
     cuda_check(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev), "attribute");
     const long long nitems = (long long)((a.ny + NB - 1) / NB) * npl;
-    const int grid = int(std::min<long long>(nitems, (long long)nsm * per_sm));
+    const int grid = int(std::min<long long>(nitems, (long long)nsm * per_sm[tws]));
     kern<<<grid, ColCfg<R, M>::THREADS, smem, st>>>(a, map, npl, err);
     cuda_check(cudaGetLastError(), "k_ucol_bwd_tma launch");
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+    return true;
+  }
+  // The image-to-band transform with each pass's H-row segments staged by
+  // bulk copies (k_ucol_fwd_bulk), when its shared memory fits a CTA.
+  // Returns false when not used.
+  template <int LOGM>
+  static bool run_bulk(const ColArgs &a, int npl, cudaStream_t st, int *err) {
+    constexpr int M = 1 << LOGM;
+    using Cfg = ColCfg<R, M>;
+    constexpr int NB = Cfg::NB;
+    if (!err || env_int("WSG_UCOL_TMA", 1) == 0) return false;
+    const size_t cs = 2 * sizeof(R);
+    if ((size_t(a.hseg) * cs) % 16 != 0 || (reinterpret_cast<uintptr_t>(a.H) & 15) != 0)
+      return false;
+    const size_t base = 128 + (size_t(NB) * a.hseg + size_t(NB) * FftBuf<M>::value + M) * cs;
+    if (base > 227 * 1024) return false;
+    // the twist tables go to shared memory too when that costs no resident
+    // CTA (registers or shared memory, whichever binds)
+    const size_t extra = size_t(a.K) * (M / 16 + 32) * cs;
+    auto *k0 = k_ucol_fwd_bulk<R, LOGM, false>;
+    auto *k1 = k_ucol_fwd_bulk<R, LOGM, true>;
+    int n0 = 0, n1 = 0;
+    smem_attr(k0, base);
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n0, k0, Cfg::THREADS, base),
+               "occupancy");
+    if (n0 < 1) return false;
+    if (base + extra <= 227 * 1024) {
+      smem_attr(k1, base + extra);
+      cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n1, k1, Cfg::THREADS,
+                                                               base + extra),
+                 "occupancy");
+    }
+    const bool tws = n1 >= n0;
+    const size_t smem = tws ? base + extra : base;
+    auto *kern = tws ? k1 : k0;
+    const int per_sm = tws ? n1 : n0;
+    int dev = 0, nsm = 148;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    cuda_check(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev), "attribute");
+    const long long nitems = (long long)((a.ny + NB - 1) / NB) * npl;
+    const int grid = int(std::min<long long>(nitems, (long long)nsm * per_sm));
+    kern<<<grid, Cfg::THREADS, smem, st>>>(a, npl, err);
+    cuda_check(cudaGetLastError(), "k_ucol_fwd_bulk launch");
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     return true;
   }
@@ -570,6 +626,7 @@ struct ColKernels {
     constexpr int M = 1 << LOGM;
     using Cfg = ColCfg<R, M>;
     if (bwd && run_tma<LOGM>(a, npl, st, err)) return;
+    if (!bwd && run_bulk<LOGM>(a, npl, st, err)) return;
     const size_t smem = ColSmem2<R, M>::bytes();
     dim3 grid((a.ny + Cfg::NB - 1) / Cfg::NB, npl);
     if (bwd) {
@@ -591,7 +648,7 @@ struct ColKernels {
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
   }
   // err: the device error word (bit 2: a staged copy did not complete), or
-  // nullptr to stay with the plain loads
+  // nullptr to stay with the plain loads (either direction)
   static void run(int logM, bool bwd, const ColArgs &a, int npl, cudaStream_t st,
                   int *err = nullptr) {
     switch (logM) {
@@ -915,6 +972,10 @@ ScreenArgs make_screen(const GridPlan &g, const double *d_cf, const ChebCorr &cc
   s.do_w = g.do_w;
   s.divide_by_n = g.do_w && g.divide_by_n;
   s.P = int(P);
+  s.K = g.K;
+  s.hseg = int(g.hseg());
+  s.hm0 = g.hm0();
+  s.nbs = int((g.hseg() + 31) / 32);
   s.cfu = d_cf;
   s.cfv = d_cf + g.nx / 2 + 1;
   s.ncheb = cc.n;
@@ -941,7 +1002,15 @@ ColArgs make_col(const GridPlan &g, size_t P, const void *tw, void *band, void *
   c.twQ = reinterpret_cast<const char *>(tw) + (M + size_t(g.K) * (M / 16)) * cs;
   c.band = band;
   c.H = H;
+  c.hseg = int(g.hseg());
+  c.hm0 = g.hm0();
   return c;
+}
+
+// Screen kernel grid: 32-entry blocks of every H-row segment by 32 image
+// columns.
+dim3 screen_grid(const GridPlan &g) {
+  return dim3(unsigned(size_t(g.K) * ((g.hseg() + 31) / 32)), unsigned((g.ny + 31) / 32));
 }
 
 }  // namespace
@@ -1147,7 +1216,7 @@ bool Context::grid_core(const wsg_args &a, const Staged &s, double *img, bool ac
   const size_t rowsP = gp.band_rows * P;
   char *band = reinterpret_cast<char *>(b_band.ensure(rowsP * nv * cs));
   char *bandf = reinterpret_cast<char *>(b_bandf.ensure(rowsP * nv * cs));
-  char *H = reinterpret_cast<char *>(b_H.ensure(P * gp.ny * gp.nx * cs));
+  char *H = reinterpret_cast<char *>(b_H.ensure(P * gp.ny * gp.hrow() * cs));
   const void *tw = upload_twiddles(gp, dbl);
   ColArgs ca = make_col(gp, P, tw, bandf, H);
   const long Lv = band_v_halfwidth(gp);
@@ -1193,7 +1262,7 @@ bool Context::grid_core(const wsg_args &a, const Staged &s, double *img, bool ac
     sa.pb0 = int(pb0);
     sa.npl = int(npl);
     sa.ld = ld;
-    dim3 sg((gp.nx + 31) / 32, (gp.ny + 31) / 32);
+    const dim3 sg = screen_grid(gp);
     k_screen_add<R><<<sg, 256, 0, stream>>>(sa, H, img, direct_out, out_mode);
     cuda_check(cudaGetLastError(), "k_screen_add launch");
   g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
@@ -1267,7 +1336,7 @@ void Context::degrid_core(const wsg_args &a, const Staged &s, const double *img,
   const size_t rowsP = gp.band_rows * P;
   char *bandi = reinterpret_cast<char *>(b_bandd.ensure(rowsP * nv * cs));
   char *band = reinterpret_cast<char *>(b_bandf.ensure(rowsP * nv * cs));
-  char *H = reinterpret_cast<char *>(b_H.ensure(P * gp.ny * gp.nx * cs));
+  char *H = reinterpret_cast<char *>(b_H.ensure(P * gp.ny * gp.hrow() * cs));
   const void *tw = upload_twiddles(gp, dbl);
   ColArgs ca = make_col(gp, P, tw, bandi, H);
   const TileLayout tl = make_layout(gp.T, gp.kernel.W);
@@ -1304,7 +1373,7 @@ void Context::degrid_core(const wsg_args &a, const Staged &s, const double *img,
     sa.pb0 = int(pb0);
     sa.npl = int(npl);
     sa.ld = ld;
-    dim3 sg((gp.nx + 31) / 32, (gp.ny + 31) / 32);
+    const dim3 sg = screen_grid(gp);
     // the caller's image itself (FP32 or FP64) when given, else the FP64 copy
     const void *src = direct_in ? direct_in : static_cast<const void *>(img);
     const int src_f32 = (direct_in && a.dirty_type == WSG_F32) ? 1 : 0;
@@ -1321,7 +1390,7 @@ void Context::degrid_core(const wsg_args &a, const Staged &s, const double *img,
       clear_outside_columns(bandi, rowsP, nv, gp.ny, cs, stream);
       bandd_zero = zl;
     }
-    ColKernels<R>::run(gp.logM, false, ca, int(npl), stream);
+    ColKernels<R>::run(gp.logM, false, ca, int(npl), stream, d_err);
     // transform along v
     {
       cufftHandle h = fft_plan(int(nv), 1, int(nv), 1, int(nv), int(rowsP), dbl);
@@ -1865,11 +1934,15 @@ Plan::Plan(Context &cx, const wsg_args &a, const wsg_job *jobs, size_t njobs) : 
     build<double>(js);
   else
     build<float>(js);
+  // registered once built: a plan whose construction failed is never checked
+  cx_.plan_err.push_back(reinterpret_cast<int *>(small_.p) + 2);
 }
 
 Plan::~Plan() {
   cudaSetDevice(cx_.device);
   cudaStreamSynchronize(cx_.stream);
+  auto &pe = cx_.plan_err;
+  pe.erase(std::remove(pe.begin(), pe.end(), reinterpret_cast<int *>(small_.p) + 2), pe.end());
   for (auto &g : graphs_)
     if (g.exec) cudaGraphExecDestroy(g.exec);
   for (auto &j : jobs_)
@@ -1918,6 +1991,7 @@ void Plan::build(const std::vector<wsg_job> &js) {
   chunks_.ensure((std::max<size_t>(cap, 1) + 1) * sizeof(int));
   chunk_job_.ensure((std::max<size_t>(cap, 1) + 1) * sizeof(int));
   small_.ensure(4096);
+  CK(cudaMemsetAsync(small_.p, 0, 4096, cx_.stream));
   DevBuf wsub, msub;
   jobs_.assign(js.size(), PlanJob{});
   int forceW = 0;
@@ -2034,7 +2108,7 @@ void Plan::build(const std::vector<wsg_job> &js) {
     PlanJob &pj = jobs_[j];
     if (pj.nrec == 0) continue;
     const GridPlan &gp = pj.gp;
-    hmax = std::max(hmax, gp.nplanes * gp.ny * gp.nx * cs);
+    hmax = std::max(hmax, gp.nplanes * gp.ny * gp.hrow() * cs);
     JobGeom &g = jg[j];
     g.nu = int(gp.nu);
     g.nv = int(gp.nv);
@@ -2075,7 +2149,7 @@ void Plan::enqueue_grid(const void *vis, void *const *dirty, int accumulate) {
   int *counter = d_nch + 1;
   int *d_err = d_nch + 2;
   CK(cudaMemsetAsync(band_.p, 0, band_total_, st));
-  CK(cudaMemsetAsync(counter, 0, 2 * sizeof(int), st));
+  CK(cudaMemsetAsync(counter, 0, sizeof(int), st));  // (the error word stays until read)
   const TileLayout tl = make_layout(T_, W_);
   const size_t smem = GridKernels<R>::smem_bytes(tl, W_, true);
   GridArgs ga{};
@@ -2131,7 +2205,7 @@ void Plan::enqueue_grid(const void *vis, void *const *dirty, int accumulate) {
                                 gp.nplanes);
     sa.pb0 = 0;
     sa.npl = int(gp.nplanes);
-    dim3 sg((gp.nx + 31) / 32, (gp.ny + 31) / 32);
+    const dim3 sg = screen_grid(gp);
     k_screen_add<R><<<sg, 256, 0, st>>>(sa, H_.p, img, nullptr, 0);
     cuda_check(cudaGetLastError(), "k_screen_add launch");
     if (a_.dirty_type == WSG_F64)
@@ -2170,13 +2244,13 @@ void Plan::enqueue_degrid(const void *const *dirty, void *vis) {
                                 gp.nplanes);
     sa.pb0 = 0;
     sa.npl = int(gp.nplanes);
-    dim3 sg((gp.nx + 31) / 32, (gp.ny + 31) / 32);
+    const dim3 sg = screen_grid(gp);
     k_screen_put<R><<<sg, 256, 0, st>>>(sa, img, 0, H_.p);
     cuda_check(cudaGetLastError(), "k_screen_put launch");
     char *band = static_cast<char *>(band_.p) + pj.band_off;
     clear_outside_columns(band, gp.band_rows * gp.nplanes, gp.nv, gp.ny, cs, st);
     ColArgs ca = make_col(gp, gp.nplanes, static_cast<char *>(tw_.p) + pj.tw_off, band, H_.p);
-    ColKernels<R>::run(gp.logM, false, ca, int(gp.nplanes), st);
+    ColKernels<R>::run(gp.logM, false, ca, int(gp.nplanes), st, d_err);
     CF(cufftSetStream(pj.fft, st));
     CF(cufftSetWorkArea(pj.fft, fftwork_.p));
     if (sizeof(R) == 8)
@@ -2187,7 +2261,7 @@ void Plan::enqueue_degrid(const void *const *dirty, void *vis) {
                       reinterpret_cast<cufftComplex *>(band), CUFFT_FORWARD));
     g_kernel_launches.fetch_add(2, std::memory_order_relaxed);
   }
-  CK(cudaMemsetAsync(counter, 0, 2 * sizeof(int), st));
+  CK(cudaMemsetAsync(counter, 0, sizeof(int), st));  // (the error word stays until read)
   const TileLayout tl = make_layout(T_, W_);
   const size_t smem = GridKernels<R>::smem_bytes(tl, W_, false);
   GridArgs ga{};
@@ -2417,7 +2491,7 @@ StreamGridder::StreamGridder(Context &cx, const wsg_args &a, double wmin, double
   CF(cufftMakePlanMany(fft_, 1, &n, &inembed, 1, n, &onembed, 1, n, dbl_ ? CUFFT_Z2Z : CUFFT_C2C,
                        int(g.band_rows * g.nplanes), &work));
   fftwork_.ensure(std::max<size_t>(work, 256));
-  H_.ensure(plane_batch() * g.nx * g.ny * cs);
+  H_.ensure(plane_batch() * g.hrow() * g.ny * cs);
   CK(cudaStreamCreateWithFlags(&copy_, cudaStreamNonBlocking));
   for (auto &sl : slots_) {
     CK(cudaEventCreateWithFlags(&sl.copied, cudaEventDisableTiming));
@@ -2472,7 +2546,7 @@ StreamGridder::~StreamGridder() {
 size_t StreamGridder::plane_batch() const {
   size_t freeb = 0, total = 0;
   CK(cudaMemGetInfo(&freeb, &total));
-  const size_t per = gp_.nx * gp_.ny * (dbl_ ? 16 : 8);
+  const size_t per = gp_.hrow() * gp_.ny * (dbl_ ? 16 : 8);
   return std::max<size_t>(1, std::min<size_t>(gp_.nplanes, (freeb / 4) / std::max<size_t>(per, 1)));
 }
 
@@ -2708,7 +2782,7 @@ void StreamGridder::finish_t(void *dirty, int accumulate) {
     ScreenArgs sa = make_screen(g, reinterpret_cast<const double *>(cf_.p), cc_, np);
     sa.pb0 = int(p0);
     sa.npl = int(np);
-    dim3 sg((g.nx + 31) / 32, (g.ny + 31) / 32);
+    const dim3 sg = screen_grid(g);
     k_screen_add<R><<<sg, 256, 0, st>>>(sa, H_.p, img, nullptr, 0);
     cuda_check(cudaGetLastError(), "k_screen_add launch");
   }
@@ -2747,7 +2821,7 @@ void StreamGridder::predict_begin_t(const double *img) {
     ScreenArgs sa = make_screen(g, reinterpret_cast<const double *>(cf_.p), cc_, np);
     sa.pb0 = int(p0);
     sa.npl = int(np);
-    dim3 sg((g.nx + 31) / 32, (g.ny + 31) / 32);
+    const dim3 sg = screen_grid(g);
     k_screen_put<R><<<sg, 256, 0, st>>>(sa, img, 0, H_.p);
     cuda_check(cudaGetLastError(), "k_screen_put launch");
     ColArgs ca = make_col(g, g.nplanes, tw_.p, static_cast<char *>(band_.p) + p0 * g.nv * cs, H_.p);
@@ -3545,11 +3619,11 @@ void ms2dirty_noalloc(const wsg_args &a, const void *vis, void *dirty, cudaStrea
                                cudaMemcpyHostToDevice, stream), "twv H2D");
 
     // grids: as many w planes per pass as fit in what is left
-    const size_t per_plane = (gp.band_rows * gp.nv + gp.ny * gp.nx) * 8 + 1024;
+    const size_t per_plane = (gp.band_rows * gp.nv + gp.ny * gp.hrow()) * 8 + 1024;
     const size_t P = std::min(gp.nplanes, ar.left() / per_plane);
     require(P >= 1, "problem too large for the allocation-free entry point (no room for one w plane)");
     char *band = reinterpret_cast<char *>(ar.take(gp.band_rows * P * gp.nv * 8));
-    char *H = reinterpret_cast<char *>(ar.take(P * gp.ny * gp.nx * 8));
+    char *H = reinterpret_cast<char *>(ar.take(P * gp.ny * gp.hrow() * 8));
     const DevKernel<float> kc = make_kernel<float>(gp.poly);
     const TileLayout tl = make_layout(gp.T, gp.kernel.W);
     const size_t smem = GridKernels<float>::smem_bytes(tl, gp.kernel.W, true);
@@ -3577,7 +3651,7 @@ void ms2dirty_noalloc(const wsg_args &a, const void *vis, void *dirty, cudaStrea
       ScreenArgs sa = make_screen(gp, d_cf, cc, P);
       sa.pb0 = int(pb0);
       sa.npl = int(npl);
-      dim3 sg((gp.nx + 31) / 32, (gp.ny + 31) / 32);
+      const dim3 sg = screen_grid(gp);
       k_screen_add<float><<<sg, 256, 0, stream>>>(sa, H, img, nullptr, 0);
       cuda_check(cudaGetLastError(), "k_screen_add launch");
       g_kernel_launches.fetch_add(1, std::memory_order_relaxed);

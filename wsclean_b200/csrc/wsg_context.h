@@ -138,6 +138,9 @@ class Context {
   cudaStream_t scan_st = nullptr;
   DevBuf *fovc_buf = nullptr;
   bool err_pending = false;  // a device-side consistency check not yet read
+  // error words of the plans on this context, read (and cleared) by
+  // synchronize(): plan executions are asynchronous and may be graph-recorded
+  std::vector<int *> plan_err;
   // the scan's statistics come back through mapped pinned memory written by
   // a kernel: a copy-engine read-back would queue behind the previous call's
   // device-to-host copy of its output

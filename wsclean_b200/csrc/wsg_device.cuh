@@ -567,6 +567,35 @@ template <typename R, int W> struct WarpStage {
   static constexpr size_t bytes = sizeof(R) * (32 * KST + 64) + 128;  // kv, (vr,vi), luv
 };
 
+// W consecutive values of a staged row, by 16- or 8-byte vector loads where
+// the layout allows: with W even every staged row, and its v block at W,
+// starts on a 16-byte boundary (the tile before the staging areas holds
+// 2 W planes, and the row stride is a multiple of 16 bytes).
+template <int W, typename R>
+__device__ __forceinline__ void lds_row(const R *p, R (&out)[W]) {
+  if constexpr (sizeof(R) == 4 && W % 4 == 0) {
+#pragma unroll
+    for (int i = 0; i < W / 4; ++i) {
+      const float4 v = reinterpret_cast<const float4 *>(p)[i];
+      out[4 * i] = v.x;
+      out[4 * i + 1] = v.y;
+      out[4 * i + 2] = v.z;
+      out[4 * i + 3] = v.w;
+    }
+  } else if constexpr (W % 2 == 0) {
+    using V2 = typename Cplx<R>::type;
+#pragma unroll
+    for (int i = 0; i < W / 2; ++i) {
+      const V2 v = reinterpret_cast<const V2 *>(p)[i];
+      out[2 * i] = v.x;
+      out[2 * i + 1] = v.y;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < W; ++i) out[i] = p[i];
+  }
+}
+
 template <int W, typename R>
 __device__ __forceinline__ void eval_const(const DevKernel<R> &k, R x, R *out) {
   constexpr int DEG = KDeg<W>::value;
@@ -883,9 +912,9 @@ k_spread(GridArgs a, DevGeom g, DevKernel<R> kc) {
           }
           const R *kb = kv + jj * KST;
           R kvv[W];
-#pragma unroll
-          for (int c = 0; c < W; ++c) kvv[c] = kb[W + c];
-          const R vr = vv[2 * jj], vi = vv[2 * jj + 1];
+          lds_row<W>(kb + W, kvv);
+          const C vx = reinterpret_cast<const C *>(vv)[jj];
+          const R vr = vx.x, vi = vx.y;
 #pragma unroll
           for (int k = 0; k < PPL; ++k) {
             const R f = kb[2 * W + (ok[k] ? pp[k] : 0)] * kb[ok[k] ? cu[k] : 0];
@@ -919,6 +948,10 @@ k_spread(GridArgs a, DevGeom g, DevKernel<R> kc) {
     const int nline = by_list ? norig * W * W : W * nbu;
     const int linelen = by_list ? W : nbv;
     const JobRegs jr(jb);
+    // bounding-box lines: (plane, row) of line = p nbu + r, stepped without
+    // a division
+    int bp = 0, br = warp;
+    while (!by_list && nbu > 0 && br >= nbu) { br -= nbu; ++bp; }
     for (int line = warp; line < nline; line += NWARP) {
       int p, ia, ib0;
       if (by_list) {
@@ -928,9 +961,11 @@ k_spread(GridArgs a, DevGeom g, DevKernel<R> kc) {
         ia = int(luv >> 16) + (pr - p * W);
         ib0 = int(luv & 0xffffu);
       } else {
-        p = line / nbu;
-        ia = lu0 + (line - p * nbu);
+        p = bp;
+        ia = lu0 + br;
         ib0 = lv0;
+        br += NWARP;
+        while (br >= nbu) { br -= nbu; ++bp; }
       }
       const int plane = mp + p;
       const int bi = jr.band_row(jr.wrap_u(ucorner + ia));
@@ -1080,12 +1115,21 @@ k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
       const int nline = by_list ? norig * W * W : W * nbu;
       const int linelen = by_list ? W : nbv;
       const JobRegs jr(jb);
+      // bounding-box lines: (plane, row) of line = p nbu + r, stepped by
+      // NWARP lines without a division
+      int bp = 0, br = warp;
+      while (!by_list && nbu > 0 && br >= nbu) { br -= nbu; ++bp; }
       for (int l0 = warp; l0 < nline; l0 += 4 * NWARP) {
         C val[4];
         int sidx[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
           const int line = l0 + q * NWARP;
+          const int lp = bp, lr = br;
+          if (!by_list) {
+            br += NWARP;
+            while (br >= nbu) { br -= nbu; ++bp; }
+          }
           val[q].x = R(0);
           val[q].y = R(0);
           sidx[q] = -1;
@@ -1098,8 +1142,8 @@ k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
               ia = int(luv >> 16) + (pr - p * W);
               ib = int(luv & 0xffffu) + lane;
             } else {
-              p = line / nbu;
-              ia = lu0 + (line - p * nbu);
+              p = lp;
+              ia = lu0 + lr;
               ib = lv0 + lane;
             }
             sidx[q] = p * tl.PS + ia * tl.RS + ib;
@@ -1171,8 +1215,7 @@ k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
             }
             const R *kb = kv + jj * KST;
             R kvv[W];
-#pragma unroll
-            for (int c = 0; c < W; ++c) kvv[c] = kb[W + c];
+            lds_row<W>(kb + W, kvv);
 #pragma unroll
             for (int k = 0; k < PPL; ++k) {
               C t;
@@ -1376,8 +1419,20 @@ struct ColArgs {
   const void *twB;      // exp(+2 pi i t k2 / nu), [k2][t], K x M/16 entries
   const void *twQ;      // exp(+2 pi i (M/16 q - neg M) k2 / nu), [k2][q][neg], K x 32
   void *band;           // [band_rows][P][nv] complex
-  void *H;              // [P][ny][nx] complex: u-transformed image columns
+  void *H;              // [P][ny][K * hseg] complex: u-transformed image columns
+  int hseg, hm0;        // row layout of H (GridPlan::hseg / hm0)
 };
+
+// Offset in an H row of output q of thread t in pass k2 (m = t + TPF q, the
+// upper half of the outputs being the negative frequencies m - M), and
+// whether that output is one of the nx image rows kept.
+template <int TPF>
+__device__ __forceinline__ int h_pos(const ColArgs &a, int k2, int t, int q, bool &keep) {
+  const int mq = t + TPF * (q < 8 ? q : q - 16);
+  const int i = a.K * mq + k2 + a.nx / 2;
+  keep = unsigned(i) < unsigned(a.nx);
+  return k2 * a.hseg + (mq - a.hm0);
+}
 
 // u of buffer slot b (b in [0, M)), or a value > nu if the slot is empty.
 __device__ __forceinline__ int slot_u(const ColArgs &a, int b, int M) {
@@ -1625,8 +1680,7 @@ k_ucol_bwd(ColArgs a) {
 #pragma unroll
   for (int q = 0; q < 16; ++q) g[q] = A[fpad(t + TPF * q)];
   __syncthreads();
-  C *rowp = H + (size_t(lp) * a.ny + j) * a.nx;
-  const int half_nu = a.nu / 2, half_nx = a.nx / 2;
+  C *rowp = H + (size_t(lp) * a.ny + j) * (size_t(a.K) * a.hseg);
   for (int k2 = 0; k2 < a.K; ++k2) {
     C v[16];
     if (k2 == 0) {
@@ -1644,9 +1698,9 @@ k_ucol_bwd(ColArgs a) {
     if (jv) {
 #pragma unroll
       for (int q = 0; q < 16; ++q) {
-        const int k = a.K * (t + TPF * q) + k2;
-        const int i = (k < half_nu ? k : k - a.nu) + half_nx;
-        if (i >= 0 && i < a.nx) rowp[i] = o[q];
+        bool keep;
+        const int pos = h_pos<TPF>(a, k2, t, q, keep);
+        if (keep) rowp[pos] = o[q];
       }
     }
   }
@@ -1755,7 +1809,7 @@ __device__ __forceinline__ void col_fft_inplace(C (&v)[16], C *buf, const C *tw,
   col_tail_inplace<C, M, 16, TPF, SIGN>(buf, tw, t, o);
 }
 
-template <typename R, int LOGM>
+template <typename R, int LOGM, bool TWS>
 __global__ void __launch_bounds__(ColCfg<R, (1 << LOGM)>::THREADS, ColCfg<R, (1 << LOGM)>::MINB)
 k_ucol_bwd_tma(ColArgs a, const __grid_constant__ CUtensorMap tmap, int npl, int *err) {
   using C = typename Cplx<R>::type;
@@ -1778,6 +1832,13 @@ k_ucol_bwd_tma(ColArgs a, const __grid_constant__ CUtensorMap tmap, int npl, int
   const C *twQ = reinterpret_cast<const C *>(a.twQ);
   const int reg2 = tma_boxes1(a, M, Cfg::BR) * Cfg::BR;  // first staging row of region 2
   fill_table<C, M, ColCfg<R, M>::THREADS>(tws, reinterpret_cast<const C *>(a.twM));
+  if constexpr (TWS) {  // the twist tables after the stage table (barrier below)
+    C *twBs = tws + M, *twQs = twBs + a.K * TPF;
+    for (int i = threadIdx.x; i < a.K * TPF; i += blockDim.x) twBs[i] = twB[i];
+    for (int i = threadIdx.x; i < a.K * 32; i += blockDim.x) twQs[i] = twQ[i];
+    twB = twBs;
+    twQ = twQs;
+  }
   int item = blockIdx.x;
   if (threadIdx.x == 0) {
     mbar_init(&bar, 1);
@@ -1786,7 +1847,6 @@ k_ucol_bwd_tma(ColArgs a, const __grid_constant__ CUtensorMap tmap, int npl, int
       tma_issue_item<R, M>(a, &tmap, stage, &bar, item / npairs, (item % npairs) * NB);
   }
   __syncthreads();  // the barrier is initialised before anyone waits on it
-  const int half_nu = a.nu / 2, half_nx = a.nx / 2;
   for (uint32_t parity = 0; item < nitems; item += gridDim.x, parity ^= 1u) {
     const int lp = item / npairs, j = (item % npairs) * NB + grp;
     if (!mbar_wait(&bar, parity)) {  // the copy did not complete: report and stop
@@ -1815,12 +1875,20 @@ k_ucol_bwd_tma(ColArgs a, const __grid_constant__ CUtensorMap tmap, int npl, int
       tma_issue_item<R, M>(a, &tmap, stage, &bar, next / npairs, (next % npairs) * NB);
     }
     const bool jv = j < a.ny;
-    C *rowp = reinterpret_cast<C *>(a.H) + (size_t(lp) * a.ny + (jv ? j : 0)) * a.nx;
+    C *rowp = reinterpret_cast<C *>(a.H) + (size_t(lp) * a.ny + (jv ? j : 0)) * (size_t(a.K) * a.hseg);
     for (int k2 = 0; k2 < a.K; ++k2) {
       C v[16];
       if (k2 == 0) {
 #pragma unroll
         for (int q = 0; q < 16; ++q) v[q] = g[q];
+      } else if constexpr (TWS) {
+        const C base = twB[k2 * TPF + t];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          const int b = t + TPF * q;
+          const int neg = (!a.band_full && b >= M - a.L) ? 1 : 0;
+          v[q] = cmul(g[q], cmul(twQ[(k2 * 16 + q) * 2 + neg], base));
+        }
       } else {
         const C base = __ldg(&twB[k2 * TPF + t]);
 #pragma unroll
@@ -1832,9 +1900,9 @@ k_ucol_bwd_tma(ColArgs a, const __grid_constant__ CUtensorMap tmap, int npl, int
       if (jv) {
 #pragma unroll
         for (int q = 0; q < 16; ++q) {
-          const int k = a.K * (t + TPF * q) + k2;
-          const int i = (k < half_nu ? k : k - a.nu) + half_nx;
-          if (i >= 0 && i < a.nx) rowp[i] = o[q];
+          bool keep;
+          const int pos = h_pos<TPF>(a, k2, t, q, keep);
+          if (keep) rowp[pos] = o[q];
         }
       }
     }
@@ -1871,23 +1939,23 @@ k_ucol_fwd(ColArgs a) {
     twB = twBs;
     twQ = twQs;
   }
-  const C *rowp = reinterpret_cast<const C *>(a.H) + (size_t(lp) * a.ny + (jv ? j : 0)) * a.nx;
+  const C *rowp = reinterpret_cast<const C *>(a.H) +
+                  (size_t(lp) * a.ny + (jv ? j : 0)) * (size_t(a.K) * a.hseg);
   fill_table<C, M, ColCfg<R, M>::THREADS>(tws, reinterpret_cast<const C *>(a.twM));
-  const int half_nx = a.nx / 2;
   C acc[16];
 #pragma unroll
   for (int q = 0; q < 16; ++q) acc[q].x = acc[q].y = R(0);
   for (int k2 = 0; k2 < a.K; ++k2) {
     C v[16];
-    // output row k = K (t + TPF q) + k2 is image row k + nx/2 for q < 8 and
-    // k - nu + nx/2 for q >= 8 (nu = 16 K TPF: the wrap at nu/2 falls at q = 8)
-    const int ib = a.K * t + k2 + half_nx, istep = a.K * TPF;
+    // input q is image row K m + k2 + nx/2, m = t + TPF q for q < 8 and
+    // t + TPF q - M for q >= 8 (nu = 16 K TPF: the wrap at nu/2 falls at q = 8)
 #pragma unroll
     for (int q = 0; q < 16; ++q) {
-      const int i = ib + istep * (q < 8 ? q : q - 16);
+      bool keep;
+      const int pos = h_pos<TPF>(a, k2, t, q, keep);
       v[q].x = R(0);
       v[q].y = R(0);
-      if (jv && unsigned(i) < unsigned(a.nx)) v[q] = rowp[i];
+      if (jv && keep) v[q] = rowp[pos];
     }
     C *S = (kFlip && (k2 & 1)) ? B : A;
     C *O = (kFlip && (k2 & 1)) ? A : B;
@@ -1932,6 +2000,155 @@ k_ucol_fwd(ColArgs a) {
       jx -= (jx >= a.nv) ? a.nv : 0;
       band[(size_t(slot_bi(a, u)) * a.P + lp) * a.nv + jx] = bufall[c * 2 * BL + fpad(b)];
     }
+  }
+}
+
+// ---- the image rows staged by bulk copies ----
+//
+// k_ucol_fwd_bulk is k_ucol_fwd made persistent over (plane, column group)
+// items.  The input of each pass -- one contiguous segment of hseg entries
+// per column of the segmented H row -- is brought into shared memory by 1-D
+// bulk copies (cp.async.bulk, completing on an mbarrier, no multicast).  The
+// next segment (the next pass, or the first pass of the CTA's next item) is
+// requested as soon as the current one has been read into registers, so it
+// lands while the current pass transforms.  The transforms run in place in
+// one buffer per column.
+
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes,
+                                          uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+      ::"r"(smem_u32(dst)), "l"(__cvta_generic_to_global(src)), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Requests segment k2 of the H rows of columns [j0, j0 + NB) of plane lp
+// into the staging buffer and arms the barrier with their bytes (one thread).
+template <typename C, int NB>
+__device__ __forceinline__ void fwd_issue(const ColArgs &a, C *stage, uint64_t *bar, int lp,
+                                          int j0, int k2) {
+  const size_t hrow = size_t(a.K) * a.hseg;
+  const uint32_t bytes = uint32_t(a.hseg) * uint32_t(sizeof(C));
+  const int nc = min(NB, a.ny - j0);
+  mbar_expect_tx(bar, uint32_t(nc) * bytes);
+  const C *src = reinterpret_cast<const C *>(a.H) + (size_t(lp) * a.ny + j0) * hrow +
+                 size_t(k2) * a.hseg;
+  for (int c = 0; c < nc; ++c) bulk_load(stage + size_t(c) * a.hseg, src + c * hrow, bytes, bar);
+}
+
+template <typename R, int LOGM, bool TWS>
+__global__ void __launch_bounds__(ColCfg<R, (1 << LOGM)>::THREADS, ColCfg<R, (1 << LOGM)>::MINB)
+k_ucol_fwd_bulk(ColArgs a, int npl, int *err) {
+  using C = typename Cplx<R>::type;
+  constexpr int M = 1 << LOGM, TPF = ColCfg<R, M>::TPF, NB = ColCfg<R, M>::NB;
+  constexpr int BL = FftBuf<M>::value;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  // the staging buffer starts on a 128-byte boundary (the host adds 128 bytes)
+  const uint32_t mis = smem_u32(smem_raw) & 127u;
+  C *stage = reinterpret_cast<C *>(smem_raw + (mis ? 128u - mis : 0u));  // [NB][hseg]
+  C *bufall = stage + size_t(NB) * a.hseg;                                 // [NB][BL]
+  C *tws = bufall + size_t(NB) * BL;                                       // [M]
+  __shared__ __align__(8) uint64_t bar;
+  const int grp = threadIdx.x / TPF, t = threadIdx.x - grp * TPF;
+  C *A = bufall + size_t(grp) * BL;
+  C *band = reinterpret_cast<C *>(a.band);
+  const C *twB = reinterpret_cast<const C *>(a.twB);
+  const C *twQ = reinterpret_cast<const C *>(a.twQ);
+  const int npairs = (a.ny + NB - 1) / NB;
+  const int nitems = npairs * npl;
+  fill_table<C, M, ColCfg<R, M>::THREADS>(tws, reinterpret_cast<const C *>(a.twM));
+  if constexpr (TWS) {  // the twist tables after the stage table (barrier below)
+    C *twBs = tws + M, *twQs = twBs + a.K * TPF;
+    for (int i = threadIdx.x; i < a.K * TPF; i += blockDim.x) twBs[i] = twB[i];
+    for (int i = threadIdx.x; i < a.K * 32; i += blockDim.x) twQs[i] = twQ[i];
+    twB = twBs;
+    twQ = twQs;
+  }
+  int item = blockIdx.x;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (item < nitems) fwd_issue<C, NB>(a, stage, &bar, item / npairs, (item % npairs) * NB, 0);
+  }
+  __syncthreads();  // the barrier and the tables are in place
+  uint32_t parity = 0;
+  for (; item < nitems; item += gridDim.x) {
+    const int lp = item / npairs, jb = (item % npairs) * NB;
+    const bool jv = jb + grp < a.ny;
+    C acc[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) acc[q].x = acc[q].y = R(0);
+    for (int k2 = 0; k2 < a.K; ++k2, parity ^= 1u) {
+      if (!mbar_wait(&bar, parity)) {  // the copy did not complete: report and stop
+        if (threadIdx.x == 0) atomicOr(err, 2);
+        mbar_wait(&bar, parity);
+        return;
+      }
+      C v[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        bool keep;
+        const int pos = h_pos<TPF>(a, k2, t, q, keep) - k2 * a.hseg;
+        v[q].x = R(0);
+        v[q].y = R(0);
+        if (jv && keep) v[q] = stage[size_t(grp) * a.hseg + pos];
+      }
+      __syncthreads();  // the staging buffer is free for the next segment
+      if (threadIdx.x == 0) {
+        int ni = item, nk = k2 + 1;
+        if (nk == a.K) {
+          ni = item + gridDim.x;
+          nk = 0;
+        }
+        if (ni < nitems) {
+          // order the reads above (generic proxy) before the copy engine's
+          // writes to the same buffer (async proxy)
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          fwd_issue<C, NB>(a, stage, &bar, ni / npairs, (ni % npairs) * NB, nk);
+        }
+      }
+      C o[16];
+      col_fft_inplace<C, M, TPF, -1>(v, A, tws, t, o);
+      if (k2 == 0) {
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          acc[q].x += o[q].x;
+          acc[q].y += o[q].y;
+        }
+      } else {
+        const C base = TWS ? twB[k2 * TPF + t] : __ldg(&twB[k2 * TPF + t]);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          C w;
+          if constexpr (TWS) {
+            const int b = t + TPF * q;
+            const int neg = (!a.band_full && b >= M - a.L) ? 1 : 0;
+            w = cmul(twQ[(k2 * 16 + q) * 2 + neg], base);
+          } else {
+            w = col_twist<C, TPF>(a, twB, twQ, k2, t, q, M, base);
+          }
+          w.y = -w.y;
+          const C val = cmul(o[q], w);
+          acc[q].x += val.x;
+          acc[q].y += val.y;
+        }
+      }
+    }
+    __syncthreads();  // the last transform's reads of A are done
+#pragma unroll
+    for (int q = 0; q < 16; ++q) A[fpad(t + TPF * q)] = acc[q];
+    __syncthreads();
+    for (int it = threadIdx.x; it < NB * M; it += blockDim.x) {
+      const int c = it % NB, b = it / NB;
+      const int jj = jb + c;
+      const int u = slot_u(a, b, M);
+      if (jj < a.ny && u < (1 << 29)) {
+        int jx = jj + a.nv - a.ny / 2;
+        jx -= (jx >= a.nv) ? a.nv : 0;
+        band[(size_t(slot_bi(a, u)) * a.P + lp) * a.nv + jx] = bufall[c * BL + fpad(b)];
+      }
+    }
+    // (the next item's first transform writes A only after a barrier)
   }
 }
 
@@ -2135,6 +2352,7 @@ struct ScreenArgs {
   double nshift, dw, wmin;
   int do_w, divide_by_n;
   int P, pb0, npl;          // layout planes, first plane, planes in this pass
+  int K, hseg, hm0, nbs;    // H row layout (ColArgs), 32-entry blocks per segment
   const double *cfu, *cfv;  // nx/2+1, ny/2+1 grid-correction factors
   double cheb[kDMaxCheb];   // corfunc(v) as Chebyshev series in y=v^2
   int ncheb;
@@ -2174,7 +2392,16 @@ __device__ __forceinline__ void pixel_terms(const ScreenArgs &s, int i, int j,
   q = nm1 + s.nshift;
 }
 
-// ms2dirty: img(i,j) += corr(i,j) * sum_p Re(H[p][j][i] * exp(-2 pi i w_p q)),
+// Image row of entry mm of H-row segment k2, or -1 for an entry that holds
+// no image row.  A screen CTA covers 32 consecutive entries of one segment
+// (blockIdx.x = k2 * nbs + block) by 32 image columns, so that its H
+// accesses are contiguous; its image rows are every K-th.
+__device__ __forceinline__ int screen_row(const ScreenArgs &s, int k2, int mm) {
+  const int i = s.K * (mm + s.hm0) + k2 + s.nx / 2;
+  return (mm < s.hseg && unsigned(i) < unsigned(s.nx)) ? i : -1;
+}
+
+// ms2dirty: img(i,j) += corr(i,j) * sum_p Re(H[p][j][pos(i)] * exp(-2 pi i w_p q)),
 // FP64 phases (recurrence over planes) and FP64 accumulation.
 template <typename R>
 // out_mode 0: img += the sum (FP64 accumulator); 1 / 2: out = the sum as
@@ -2185,18 +2412,20 @@ __global__ void __launch_bounds__(256) k_screen_add(ScreenArgs s, const void *Hv
   using C = typename Cplx<R>::type;
   const C *H = reinterpret_cast<const C *>(Hv);
   __shared__ double tile[32][33];
-  const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
+  const int k2 = blockIdx.x / s.nbs, mm0 = (blockIdx.x - k2 * s.nbs) * 32;
+  const int j0 = blockIdx.y * 32;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
-  const int i = i0 + tx;
+  const int i = screen_row(s, k2, mm0 + tx);
+  const size_t hrow = size_t(s.K) * s.hseg;
   // planes loaded together; the first batch is in flight while the pixel's
   // FP64 terms are computed
   constexpr int PB = sizeof(R) == 4 ? 16 : 8;
   for (int k = 0; k < 4; ++k) {
     const int j = j0 + ty + 8 * k;
     double val = 0;
-    if (i < s.nx && j < s.ny) {
-      const C *hp = H + size_t(j) * s.nx + i;
-      const size_t pstride = size_t(s.ny) * s.nx;
+    if (i >= 0 && j < s.ny) {
+      const C *hp = H + size_t(j) * hrow + (size_t(k2) * s.hseg + mm0 + tx);
+      const size_t pstride = size_t(s.ny) * hrow;
       C hb[PB];
 #pragma unroll
       for (int u = 0; u < PB; ++u)
@@ -2240,8 +2469,8 @@ __global__ void __launch_bounds__(256) k_screen_add(ScreenArgs s, const void *Hv
   }
   __syncthreads();
   for (int k = 0; k < 4; ++k) {
-    const int ii = i0 + ty + 8 * k, jj = j0 + tx;
-    if (ii < s.nx && jj < s.ny) {
+    const int ii = screen_row(s, k2, mm0 + ty + 8 * k), jj = j0 + tx;
+    if (ii >= 0 && jj < s.ny) {
       const size_t o = size_t(ii) * s.ld + jj;
       const double x = tile[tx][ty + 8 * k];
       if (out_mode == 0)
@@ -2254,7 +2483,7 @@ __global__ void __launch_bounds__(256) k_screen_add(ScreenArgs s, const void *Hv
   }
 }
 
-// dirty2ms: H[p][j][i] = dirty(i,j) * corr(i,j) * exp(+2 pi i w_p q)
+// dirty2ms: H[p][j][pos(i)] = dirty(i,j) * corr(i,j) * exp(+2 pi i w_p q)
 template <typename R>
 // in_f32: img points to the caller's FP32 image instead of the FP64 copy
 __global__ void __launch_bounds__(256) k_screen_put(ScreenArgs s, const void *img, int in_f32,
@@ -2262,12 +2491,13 @@ __global__ void __launch_bounds__(256) k_screen_put(ScreenArgs s, const void *im
   using C = typename Cplx<R>::type;
   C *H = reinterpret_cast<C *>(Hv);
   __shared__ double tile[32][33];
-  const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
+  const int k2 = blockIdx.x / s.nbs, mm0 = (blockIdx.x - k2 * s.nbs) * 32;
+  const int j0 = blockIdx.y * 32;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   for (int k = 0; k < 4; ++k) {  // coalesced read along j
-    const int ii = i0 + ty + 8 * k, jj = j0 + tx;
+    const int ii = screen_row(s, k2, mm0 + ty + 8 * k), jj = j0 + tx;
     double x = 0.0;
-    if (ii < s.nx && jj < s.ny) {
+    if (ii >= 0 && jj < s.ny) {
       const size_t o = size_t(ii) * s.ld + jj;
       x = in_f32 ? double(reinterpret_cast<const float *>(img)[o])
                  : reinterpret_cast<const double *>(img)[o];
@@ -2275,16 +2505,17 @@ __global__ void __launch_bounds__(256) k_screen_put(ScreenArgs s, const void *im
     tile[tx][ty + 8 * k] = x;
   }
   __syncthreads();
-  const int i = i0 + tx;
-  const size_t pstride = size_t(s.ny) * s.nx;
+  const int i = screen_row(s, k2, mm0 + tx);
+  const size_t hrow = size_t(s.K) * s.hseg;
+  const size_t pstride = size_t(s.ny) * hrow;
   for (int k = 0; k < 4; ++k) {
     const int j = j0 + ty + 8 * k;
-    if (i >= s.nx || j >= s.ny) continue;
+    if (i < 0 || j >= s.ny) continue;
     double corr, q;
     bool inside;
     pixel_terms(s, i, j, corr, q, inside);
     const double val = tile[ty + 8 * k][tx] * corr;
-    C *hp = H + size_t(j) * s.nx + i;
+    C *hp = H + size_t(j) * hrow + (size_t(k2) * s.hseg + mm0 + tx);
     if (s.do_w && inside) {
       const double w0 = s.wmin + s.pb0 * s.dw;
       double2 sc = cexp_turns(w0 * q);

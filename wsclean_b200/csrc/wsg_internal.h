@@ -121,6 +121,19 @@ struct GridPlan {
   // nu = K * 2^logM with 2^logM >= band_rows: the u transform of an image
   // column is K pruned FFTs of length 2^logM
   int logM = 0, K = 1;
+  // Layout of one u-transformed image row (the array between the u
+  // transform and the w-screen): pixel row i, at s = i - nx/2 = K m + k2
+  // (0 <= k2 < K), is written by the k2-th pruned FFT as its output m.  The
+  // row holds K segments of hseg() entries, one per k2, each ordered by m
+  // from hm0(), so that every FFT reads or writes one contiguous run.  With
+  // K == 1 this is the natural order, entry i for pixel i.
+  int hm0() const { return -int((nx / 2 + K - 1) / K); }
+  size_t hseg() const {
+    if (K == 1) return nx;
+    const size_t nm = size_t(int((nx - 1 - nx / 2) / K) - hm0() + 1);
+    return (nm + 31) & ~size_t(31);
+  }
+  size_t hrow() const { return size_t(K) * hseg(); }
   // bins and sort keys
   int T = 16;
   int ntu = 0, ntv = 0, nwmin = 1;
