@@ -1,4 +1,5 @@
-// Device kernels of libwsg (sm_100a).  Host orchestration is in wsg_context.cu.
+// Device kernels of libwsg (sm_100a).  Host orchestration: the wsg_*.cu units
+// listed in wsg_host.cuh; the heavy kernel templates are launched from wsg_launch.cu.
 //
 // Data flow of one ms2dirty call (dirty2ms runs the transpose in reverse):
 //   k_scan      active mask, |w| and |u| ranges, nvis        (ducc0 scanData, wgridder.h:1578-1618)
@@ -59,7 +60,7 @@ struct ScanOut {
 };
 
 // Copies the scan's statistics into mapped pinned host memory (one warp).
-__global__ void k_scan_readback(const ScanOut *src, ScanOut *dst_host) {
+static __global__ void k_scan_readback(const ScanOut *src, ScanOut *dst_host) {
   constexpr int N = sizeof(ScanOut) / sizeof(unsigned long long);
   const auto *s = reinterpret_cast<const unsigned long long *>(src);
   auto *d = reinterpret_cast<volatile unsigned long long *>(dst_host);
@@ -393,7 +394,7 @@ __device__ __forceinline__ typename RecOf<R>::type make_record(
 
 // Sorted position of every visibility: pos[sidx[s]] = s (the inactive
 // ones sort last, at positions >= the active count, and have no record).
-__global__ void k_rank(size_t n, const uint32_t *__restrict__ sidx, uint32_t *__restrict__ pos) {
+static __global__ void k_rank(size_t n, const uint32_t *__restrict__ sidx, uint32_t *__restrict__ pos) {
   for (size_t s = blockIdx.x * size_t(blockDim.x) + threadIdx.x; s < n;
        s += size_t(gridDim.x) * blockDim.x)
     pos[sidx[s]] = uint32_t(s);
@@ -434,7 +435,7 @@ __global__ void k_plan_remap(size_t n, Rec *__restrict__ rec, uint32_t nch, uint
 
 // Batch plans: append a job's chunk starts (shifted by its record offset)
 // and tag the chunks with the job.
-__global__ void k_plan_chunks(int n, const int *__restrict__ in, int *__restrict__ out,
+static __global__ void k_plan_chunks(int n, const int *__restrict__ in, int *__restrict__ out,
                               int *__restrict__ job_of, int rec_off, int job) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     out[i] = in[i] + rec_off;
@@ -2191,7 +2192,7 @@ k_row_fft(void *data, long long rows, const void *twv, int sign) {
 // natural, uniform or Briggs imaging weights, then looked up per visibility.
 // (u, v) are in wavelengths, u / lambda with lambda = c / f per channel.
 
-__global__ void k_weights_grid(size_t nrows, int nchan, int npol, const double *__restrict__ uvw,
+static __global__ void k_weights_grid(size_t nrows, int nchan, int npol, const double *__restrict__ uvw,
                                const double *__restrict__ lambda, const float *__restrict__ wgt,
                                int as_taper, WeightGrid g, double *__restrict__ grid,
                                double *__restrict__ total) {
@@ -2216,7 +2217,7 @@ __global__ void k_weights_grid(size_t nrows, int nchan, int npol, const double *
   if ((threadIdx.x & 31) == 0 && sum != 0.0) atomicAdd(total, sum);
 }
 
-__global__ void k_weights_sumsq(size_t n, const double *__restrict__ grid, double *__restrict__ out) {
+static __global__ void k_weights_sumsq(size_t n, const double *__restrict__ grid, double *__restrict__ out) {
   double s = 0.0;
   for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n;
        i += size_t(gridDim.x) * blockDim.x)
@@ -2226,7 +2227,7 @@ __global__ void k_weights_sumsq(size_t n, const double *__restrict__ grid, doubl
 }
 
 // mode 0 natural, 1 uniform, 2 Briggs (s2 = (5 * 10^-robust)^2 / (sum W^2 / sum W))
-__global__ void k_weights_finish(size_t n, double *__restrict__ grid, int mode,
+static __global__ void k_weights_finish(size_t n, double *__restrict__ grid, int mode,
                                  const double *__restrict__ sums, double num_sq) {
   const double s2 = mode == 2 ? num_sq / (sums[1] / sums[0]) : 0.0;
   for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n;
@@ -2242,7 +2243,7 @@ __global__ void k_weights_finish(size_t n, double *__restrict__ grid, int mode,
 }
 
 // out = in * imaging weight of the visibility's cell (0 outside the grid)
-__global__ void k_weights_apply(size_t nrows, int nchan, int npol, const double *__restrict__ uvw,
+static __global__ void k_weights_apply(size_t nrows, int nchan, int npol, const double *__restrict__ uvw,
                                 const double *__restrict__ lambda, WeightGrid g,
                                 const double *__restrict__ grid, const float *__restrict__ in,
                                 float *__restrict__ out) {
@@ -2269,7 +2270,7 @@ __global__ void k_weights_apply(size_t nrows, int nchan, int npol, const double 
 // cut bin.  A visibility's bin is min(floor((|w f/c| - wmin) * xdw), NBIN-1)
 // with xdw = NBIN / (wmax - wmin), as the reference computes it.
 
-__global__ void k_wrange(size_t nrows, int nchan, const double *__restrict__ uvw,
+static __global__ void k_wrange(size_t nrows, int nchan, const double *__restrict__ uvw,
                          const double *__restrict__ fovc, const uint8_t *__restrict__ mask,
                          unsigned long long *out /* [0] min bits, [1] max bits, [2] count */) {
   double lo = 1e300, hi = 0;
@@ -2305,7 +2306,7 @@ __device__ __forceinline__ int w_bin(double aw, double wmin, double xdw) {
   return int(b < (unsigned long long)(kTuneBins - 1) ? b : (unsigned long long)(kTuneBins - 1));
 }
 
-__global__ void k_whist(size_t nrows, int nchan, const double *__restrict__ uvw,
+static __global__ void k_whist(size_t nrows, int nchan, const double *__restrict__ uvw,
                         const double *__restrict__ fovc, const uint8_t *__restrict__ mask,
                         double wmin, double xdw, unsigned long long *hist) {
   __shared__ unsigned int h[kTuneBins];
@@ -2325,7 +2326,7 @@ __global__ void k_whist(size_t nrows, int nchan, const double *__restrict__ uvw,
 }
 
 // hi[k] = mask_k and bin >= icut; lo[k] = mask_k and bin < icut
-__global__ void k_wsplit(size_t nrows, int nchan, const double *__restrict__ uvw,
+static __global__ void k_wsplit(size_t nrows, int nchan, const double *__restrict__ uvw,
                          const double *__restrict__ fovc, const uint8_t *__restrict__ mask,
                          double wmin, double xdw, int icut, uint8_t *__restrict__ hi,
                          uint8_t *__restrict__ lo) {
@@ -2557,14 +2558,14 @@ __global__ void k_store_image(size_t n, const double *__restrict__ in, TO *__res
     out[i] = TO(in[i]);
 }
 
-__global__ void k_scale(size_t n, double *__restrict__ x, double f) {
+static __global__ void k_scale(size_t n, double *__restrict__ x, double f) {
   for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n;
        i += size_t(gridDim.x) * blockDim.x)
     x[i] *= f;
 }
 
 // trimmed x-major FP64 image <- untrimmed float image (index x + y*width)
-__global__ void k_untrim(int wt, int ht, int width, int dx, int dy, const float *__restrict__ in,
+static __global__ void k_untrim(int wt, int ht, int width, int dx, int dy, const float *__restrict__ in,
                          double *__restrict__ out) {
   for (size_t t = blockIdx.x * size_t(blockDim.x) + threadIdx.x; t < size_t(wt) * ht;
        t += size_t(gridDim.x) * blockDim.x) {
@@ -2574,7 +2575,7 @@ __global__ void k_untrim(int wt, int ht, int width, int dx, int dy, const float 
 }
 
 // untrimmed float image (NaN outside) <- trimmed x-major FP64 image
-__global__ void k_retrim(int wt, int ht, int width, int height, int dx, int dy,
+static __global__ void k_retrim(int wt, int ht, int width, int height, int dx, int dy,
                          const double *__restrict__ in, float *__restrict__ out) {
   for (size_t t = blockIdx.x * size_t(blockDim.x) + threadIdx.x; t < size_t(width) * height;
        t += size_t(gridDim.x) * blockDim.x) {
