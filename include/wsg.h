@@ -357,7 +357,11 @@ int wsg_stream_finish(wsg_stream *s, void *dirty, int accumulate);
 /* Loads a model image for prediction (rows added since the last
  * wsg_stream_finish are discarded). */
 int wsg_stream_predict_begin(wsg_stream *s, const void *dirty);
-/* Predicts nrows rows into vis (nrows x nchan of vis_type). */
+/* Predicts nrows rows into vis (nrows x nchan of vis_type).  The call
+ * returns with vis in place, except with the context in pipelined mode
+ * (wsg_ctx_set_async) and vis in page-locked host memory: the chunk is then
+ * copied back while the next chunk is computed, and vis is in place after
+ * wsg_ctx_synchronize. */
 int wsg_stream_predict(wsg_stream *s, size_t nrows, const double *uvw, void *vis,
                        const void *wgt, const uint8_t *mask);
 /* Grid choice of the stream (timings are zero). */

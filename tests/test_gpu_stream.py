@@ -139,3 +139,35 @@ def test_stream_predict_then_grid(cfg5):
         d = s.finish()
     ref = G.ms2dirty(uvw, freq, vis, nx, nx, px, px, 1e-5, dirty_dtype=np.float64, **KW)
     assert O.rel_rms(d, ref) < 5e-6
+
+
+def test_stream_pipelined_prediction(cfg5):
+    """With the context pipelined (wsg_ctx_set_async), predictions into
+    page-locked memory return once enqueued, are copied back while the next
+    chunk is computed, and are in place after synchronize(): they equal the
+    chunk-by-chunk synchronous predictions."""
+    from wsclean_b200 import gridder as G
+    from wsclean_b200 import synth
+    c, _ = cfg5
+    uvw, freq, nx, px = c["uvw"], c["freq"], c["npix_x"], c["pixsize"]
+    rng = np.random.default_rng(7)
+    ix, iy, flux = synth.point_sky(100, nx, nx, rng)
+    model = synth.sky_image(nx, nx, ix, iy, flux).astype(np.float32)
+    ext = G.data_extent(uvw, freq)
+    parts = chunks(len(uvw), 6)
+    ctx = G.Context(0)
+    try:
+        with G.Stream(freq, nx, nx, px, px, 1e-5, ext, context=ctx, **KW) as s:
+            s.predict_begin(model)
+            ref = np.concatenate([s.predict(uvw[a:b]) for a, b in parts])
+            h_uvw = torch.as_tensor(uvw).pin_memory()
+            out = torch.zeros((len(uvw), len(freq)), dtype=torch.complex64).pin_memory()
+            ctx.set_async(True)
+            s.predict_begin(model)
+            for a, b in parts:
+                s.predict(h_uvw[a:b], vis=out[a:b])
+            ctx.synchronize()
+            ctx.set_async(False)
+    finally:
+        ctx.close()
+    assert O.rel_rms(out.numpy(), ref) < 1e-7

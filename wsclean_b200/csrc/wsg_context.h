@@ -337,6 +337,10 @@ class StreamGridder {
     DevBuf uvw, vis, wgt, mask;
     PinnedBuf h_uvw, h_vis, h_wgt, h_mask;
     cudaEvent_t copied = nullptr, done = nullptr;
+    // pipelined prediction into page-locked host memory: the slot's device
+    // output and the end of its copy back
+    DevBuf vout;
+    cudaEvent_t vcopied = nullptr;
   };
   template <typename R>
   void add_t(const Staged &s, size_t nrows);

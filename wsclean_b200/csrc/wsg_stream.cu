@@ -91,6 +91,7 @@ StreamGridder::StreamGridder(Context &cx, const wsg_args &a, double wmin, double
   for (auto &sl : slots_) {
     CK(cudaEventCreateWithFlags(&sl.copied, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&sl.vcopied, cudaEventDisableTiming));
   }
   for (auto &b : batch_) {
     CK(cudaEventCreateWithFlags(&b.filled, cudaEventDisableTiming));
@@ -117,6 +118,7 @@ StreamGridder::StreamGridder(Context &cx, const wsg_args &a, double wmin, double
 StreamGridder::~StreamGridder() {
   cudaSetDevice(cx_.device);
   cudaStreamSynchronize(cx_.stream);
+  cudaStreamSynchronize(cx_.d2h);  // pipelined predictions still copying back
   if (copy_) {
     cudaStreamSynchronize(copy_);
     cudaStreamDestroy(copy_);
@@ -124,7 +126,8 @@ StreamGridder::~StreamGridder() {
   for (auto &sl : slots_) {
     if (sl.copied) cudaEventDestroy(sl.copied);
     if (sl.done) cudaEventDestroy(sl.done);
-    for (DevBuf *b : {&sl.uvw, &sl.vis, &sl.wgt, &sl.mask}) b->release();
+    if (sl.vcopied) cudaEventDestroy(sl.vcopied);
+    for (DevBuf *b : {&sl.uvw, &sl.vis, &sl.wgt, &sl.mask, &sl.vout}) b->release();
     for (PinnedBuf *b : {&sl.h_uvw, &sl.h_vis, &sl.h_wgt, &sl.h_mask}) b->release();
   }
   for (auto &b : batch_) {
@@ -506,14 +509,31 @@ void StreamGridder::predict(size_t nrows, const double *uvw, void *vis, const vo
   Staged s = stage(sl, nrows, uvw, nullptr, wgt, mask);
   const size_t vbytes = nrows * a_.nchan * (a_.vis_type == WSG_C128 ? 16 : 8);
   const bool vdev = is_device_pointer(vis);
-  void *vout = vdev ? vis : vout_.ensure(vbytes);
+  // pipelined (wsg_ctx_set_async) into page-locked host memory: the chunk is
+  // predicted into the slot's own device buffer and copied back on the
+  // context's read-back stream while the next chunk is computed; the caller
+  // finds vis in place after wsg_ctx_synchronize
+  bool pinned = false;
+  if (!vdev && cx_.async_mode) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, vis) == cudaSuccess)
+      pinned = at.type == cudaMemoryTypeHost;
+    else
+      cudaGetLastError();
+  }
+  void *vout = vdev ? vis : pinned ? sl.vout.ensure(vbytes) : vout_.ensure(vbytes);
+  if (pinned) CK(cudaStreamWaitEvent(cx_.stream, sl.vcopied, 0));  // the slot's last copy is out
   CK(cudaMemsetAsync(vout, 0, vbytes, cx_.stream));
   if (dbl_)
     predict_t<double>(s, nrows, vout);
   else
     predict_t<float>(s, nrows, vout);
   CK(cudaEventRecord(sl.done, cx_.stream));
-  if (!vdev) {
+  if (pinned) {
+    CK(cudaStreamWaitEvent(cx_.d2h, sl.done, 0));
+    CK(cudaMemcpyAsync(vis, vout, vbytes, cudaMemcpyDeviceToHost, cx_.d2h));
+    CK(cudaEventRecord(sl.vcopied, cx_.d2h));
+  } else if (!vdev) {
     CK(cudaMemcpyAsync(vis, vout, vbytes, cudaMemcpyDeviceToHost, cx_.stream));
     CK(cudaStreamSynchronize(cx_.stream));
   }
