@@ -624,6 +624,8 @@ __device__ __forceinline__ bool stage_meta(const Rec &rr, int lane, int tu, int 
   if (lu < 0 || lu >= g.T || lv < 0 || lv >= g.T || int(rr.mp) != mp) {
     atomicOr(err, 1);
     luv[lane] = kSkip;
+    vv[2 * lane] = R(0);
+    vv[2 * lane + 1] = R(0);
     return false;
   }
   luv[lane] = (uint32_t(lu) << 16) | uint32_t(lv);
@@ -662,10 +664,13 @@ __device__ __forceinline__ void stage_batch(const Rec *recs, int b0, int nb, int
   constexpr int KST = KStride<R, W>::value;
   if (lane < nb) {
     const Rec rr = recs[b0 + lane];
-    if (stage_meta<R>(rr, lane, tu, tv, mp, g, vv, luv, err, bb0, bb1, bb2, bb3, vis_in,
-                      vis_in_double)) {
+    R *row = kv + lane * KST;
+    if (!stage_meta<R>(rr, lane, tu, tv, mp, g, vv, luv, err, bb0, bb1, bb2, bb3, vis_in,
+                       vis_in_double)) {
+#pragma unroll
+      for (int i = 0; i < 3 * W; ++i) row[i] = R(0);
+    } else {
       R vals[W];
-      R *row = kv + lane * KST;
       eval_const<W>(kc, rr.xu, vals);
 #pragma unroll
       for (int i = 0; i < W; ++i) row[i] = vals[i];
@@ -872,13 +877,21 @@ k_spread(GridArgs a, DevGeom g, DevKernel<R> kc) {
         for (int c = 0; c < W; ++c) acc[k][c].x = acc[k][c].y = R(0);
       uint32_t cur = 0xffffffffu;
       int bb0 = 1 << 30, bb1 = -1, bb2 = 1 << 30, bb3 = -1;
+      // the lane's kernel-row indices and tile offsets, fixed for the chunk
+      int kwi[PPL], kui[PPL], coff[PPL];
+#pragma unroll
+      for (int k = 0; k < PPL; ++k) {
+        kwi[k] = 2 * W + (ok[k] ? pp[k] : 0);
+        kui[k] = ok[k] ? cu[k] : 0;
+        coff[k] = pp[k] * tl.PS + cu[k] * tl.RS;
+      }
       auto commit = [&]() {
-        if (cur == 0xffffffffu) return;
-        const int lu = int(cur >> 16), lv = int(cur & 0xffffu);
+        if (cur >= kSkip) return;  // nothing accumulated, or skipped records only
+        const int o = int(cur >> 16) * tl.RS + int(cur & 0xffffu);
 #pragma unroll
         for (int k = 0; k < PPL; ++k) {
           if (!ok[k]) continue;
-          const int base = pp[k] * tl.PS + (lu + cu[k]) * tl.RS + lv;
+          const int base = coff[k] + o;
 #pragma unroll
           for (int c = 0; c < W; ++c) {
             atomicAdd(&tre[base + c], acc[k][c].x);
@@ -900,16 +913,27 @@ k_spread(GridArgs a, DevGeom g, DevKernel<R> kc) {
                             bb2, bb3, a.vis_in, a.vis_in_double);
           __syncwarp();
         }
+        if (grp == 0) {
+          // the batch's new footprint origins, by a ballot over the staged
+          // records (a skipped record counts as one; a repeated origin in the
+          // list is harmless, its cells being taken by atomic exchange)
+          const uint32_t my = lane < nb ? luvs[lane] : 0u;
+          uint32_t prev = __shfl_up_sync(0xffffffffu, my, 1);
+          if (lane == 0) prev = cur;
+          const unsigned nm = __ballot_sync(0xffffffffu, lane < nb && my != prev && my != kSkip);
+          if (nm) {
+            int base = 0;
+            if (lane == 0) base = atomicAdd(&sh_norig, __popc(nm));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            const int k = base + __popc(nm & ((1u << lane) - 1u));
+            if (((nm >> lane) & 1u) && k < kMaxOrig) sh_orig[k] = my;
+          }
+        }
         for (int jj = 0; jj < nb; ++jj) {
           const uint32_t luv = luvs[jj];
-          if (luv == kSkip) continue;
-          if (luv != cur) {
+          if (__any_sync(0xffffffffu, luv != cur)) {  // warp-uniform: luv is one value
             commit();
             cur = luv;
-            if (lane == 0 && grp == 0) {
-              const int k = atomicAdd(&sh_norig, 1);
-              if (k < kMaxOrig) sh_orig[k] = luv;
-            }
           }
           const R *kb = kv + jj * KST;
           R kvv[W];
@@ -918,7 +942,7 @@ k_spread(GridArgs a, DevGeom g, DevKernel<R> kc) {
           const R vr = vx.x, vi = vx.y;
 #pragma unroll
           for (int k = 0; k < PPL; ++k) {
-            const R f = kb[2 * W + (ok[k] ? pp[k] : 0)] * kb[ok[k] ? cu[k] : 0];
+            const R f = kb[kwi[k]] * kb[kui[k]];
             C a;
             a.x = vr * f;
             a.y = vi * f;
