@@ -789,7 +789,7 @@ void Context::degrid_core(const wsg_args &a, const Staged &s, const double *img,
   ga.vis_double = a.vis_type == WSG_C128;
   ga.vis_accumulate = vis_acc ? 1 : 0;
   const bool multi = P < gp.nplanes;
-  const bool need_acc = multi || grid_groups<R>(gp.kernel.W) > 1;
+  const bool need_acc = multi || grid_needs_acc<R>(gp.kernel.W);
   ga.acc = need_acc ? b_acc.ensure(gp.nvis * cs) : nullptr;
   if (need_acc) CK(cudaMemsetAsync(ga.acc, 0, gp.nvis * cs, stream));
 

@@ -885,8 +885,15 @@ k_spread(GridArgs a, DevGeom g, DevKernel<R> kc) {
         kui[k] = ok[k] ? cu[k] : 0;
         coff[k] = pp[k] * tl.PS + cu[k] * tl.RS;
       }
+      // When every warp works on the same records (SPLIT), the warps reach
+      // each commit together, and for one origin every tile cell belongs to
+      // one lane: a barrier before the commit orders it after the previous
+      // origin's, and the commit is a plain read-modify-write (FP64 shared
+      // atomics cost a quarter of the spread).  Otherwise warps of other
+      // slices may commit to the same cells at any time: shared atomics.
       auto commit = [&]() {
-        if (cur >= kSkip) return;  // nothing accumulated, or skipped records only
+        if (cur >= kSkip) return;  // nothing accumulated, or skipped records only (uniform)
+        if constexpr (SPLIT) __syncthreads();
         const int o = int(cur >> 16) * tl.RS + int(cur & 0xffffu);
 #pragma unroll
         for (int k = 0; k < PPL; ++k) {
@@ -894,8 +901,13 @@ k_spread(GridArgs a, DevGeom g, DevKernel<R> kc) {
           const int base = coff[k] + o;
 #pragma unroll
           for (int c = 0; c < W; ++c) {
-            atomicAdd(&tre[base + c], acc[k][c].x);
-            atomicAdd(&tim[base + c], acc[k][c].y);
+            if constexpr (SPLIT) {
+              tre[base + c] += acc[k][c].x;
+              tim[base + c] += acc[k][c].y;
+            } else {
+              atomicAdd(&tre[base + c], acc[k][c].x);
+              atomicAdd(&tim[base + c], acc[k][c].y);
+            }
             acc[k][c].x = acc[k][c].y = R(0);
           }
         }
@@ -1084,7 +1096,9 @@ k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
   R *vv = kv + 32 * KST;
   uint32_t *luvs = reinterpret_cast<uint32_t *>(vv + 64);
   const Rec *recs = reinterpret_cast<const Rec *>(a.rec);
-  const bool direct = a.last_pass && a.first_pass && NG == 1;
+  // finalised in place in a single plane pass, when one warp owns each
+  // record or all warps share every record (SPLIT: warp 0 adds their sums)
+  const bool direct = a.last_pass && a.first_pass && (NG == 1 || SPLIT);
 
   int pp[PPL], cu[PPL];
   bool ok[PPL];
@@ -1259,11 +1273,26 @@ k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
           }
         }
         __syncwarp();
-        const R osr = lane < nb ? osum[2 * lane] : R(0);
-        const R osi = lane < nb ? osum[2 * lane + 1] : R(0);
+        R osr = lane < nb ? osum[2 * lane] : R(0);
+        R osi = lane < nb ? osum[2 * lane + 1] : R(0);
+        if constexpr (SPLIT) {
+          // every warp summed its pairs of the same records: warp 0 adds the
+          // warps' sums from their staging areas (free until the next
+          // batch's barrier), so each record has one writer
+          __syncthreads();
+          if (warp == 0 && lane < nb) {
+            for (int w = 1; w < NWARP; ++w) {
+              const R *os = reinterpret_cast<const R *>(
+                                smem_raw + size_t(2 * W * tl.PS) * sizeof(R) +
+                                size_t(w) * WarpStage<R, W>::bytes) + 32 * KST;
+              osr += os[2 * lane];
+              osi += os[2 * lane + 1];
+            }
+          }
+        }
         // lanes finalise their own records of the batch together (one
         // coalesced record load, instead of one lane per record in turn)
-        if (lane < nb && luvs[lane] != kSkip) {
+        if ((!SPLIT || warp == 0) && lane < nb && luvs[lane] != kSkip) {
           const int s = b0 + lane;
           if (direct) {
             const Rec rr = recs[s];
@@ -1272,6 +1301,10 @@ k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
             const double orr = double(rr.vr) * double(osr) - double(rr.vi) * double(si);
             const double oi = double(rr.vr) * double(si) + double(rr.vi) * double(osr);
             store_vis(a.vis_out, a.vis_double, a.vis_accumulate, idx, orr, oi);
+          } else if constexpr (SPLIT) {  // the record's one writer in this pass
+            C *accp = reinterpret_cast<C *>(a.acc) + s;
+            accp->x += osr;
+            accp->y += osi;
           } else {
             C *accp = reinterpret_cast<C *>(a.acc) + s;
             atomicAdd(&accp->x, osr);

@@ -225,6 +225,11 @@ size_t grid_smem_bytes(const TileLayout &tl, int W, bool spread);
 // Warps that share one record.
 template <typename R>
 int grid_groups(int W);
+// Whether the interpolation of one plane pass needs the per-record
+// accumulator (and k_finalize): when a record is shared by some but not
+// all of a CTA's warps (all warps sharing it add their sums in the kernel).
+template <typename R>
+bool grid_needs_acc(int W);
 // One persistent spread (or interpolation) launch over the chunks.
 template <typename R>
 void grid_dispatch(int W, bool spread, int nsm, size_t smem, cudaStream_t st, const GridArgs &a,

@@ -299,6 +299,11 @@ int grid_groups(int W) {
   return GridKernels<R>::groups(W);
 }
 template <typename R>
+bool grid_needs_acc(int W) {
+  const int ng = GridKernels<R>::groups(W);
+  return ng > 1 && ng < GridKernels<R>::NWARP;
+}
+template <typename R>
 void grid_dispatch(int W, bool spread, int nsm, size_t smem, cudaStream_t st, const GridArgs &a,
                    const DevGeom &g, const DevKernel<R> &kc) {
   static_assert(GridKernels<R>::SB == grid_sb<R>(), "sub-batch size");
@@ -326,6 +331,7 @@ void launch_screen_put(dim3 grid, cudaStream_t st, const ScreenArgs &s, const vo
 #define WSG_LAUNCHERS(R)                                                                     \
   template size_t grid_smem_bytes<R>(const TileLayout &, int, bool);                         \
   template int grid_groups<R>(int);                                                          \
+  template bool grid_needs_acc<R>(int);                                                      \
   template void grid_dispatch<R>(int, bool, int, size_t, cudaStream_t, const GridArgs &,     \
                                  const DevGeom &, const DevKernel<R> &);                     \
   template void col_run<R>(int, bool, const ColArgs &, int, cudaStream_t, int *);            \

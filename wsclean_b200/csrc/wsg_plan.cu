@@ -244,7 +244,7 @@ void Plan::build(const std::vector<wsg_job> &js) {
   CK(cudaMemcpyAsync(cf_.p, cf_host.data(), cf_host.size() * sizeof(double), cudaMemcpyHostToDevice, st));
   tw_.ensure(std::max<size_t>(tw_host.size(), 1));
   CK(cudaMemcpyAsync(tw_.p, tw_host.data(), tw_host.size(), cudaMemcpyHostToDevice, st));
-  need_acc_ = grid_groups<R>(W_) > 1;
+  need_acc_ = grid_needs_acc<R>(W_);
   if (need_acc_) acc_.ensure(nrec_ * cs);
   CK(cudaStreamSynchronize(st));
 }

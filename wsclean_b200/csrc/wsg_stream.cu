@@ -487,7 +487,7 @@ void StreamGridder::predict_t(const Staged &s, size_t nrows, void *vis_dev) {
   ga.vis_out = vis_dev;
   ga.vis_double = a_.vis_type == WSG_C128;
   ga.first_pass = ga.last_pass = 1;
-  const bool need_acc = grid_groups<R>(g.kernel.W) > 1;
+  const bool need_acc = grid_needs_acc<R>(g.kernel.W);
   ga.acc = need_acc ? cx_.b_acc.ensure(g.nvis * cs) : nullptr;
   if (need_acc) CK(cudaMemsetAsync(ga.acc, 0, g.nvis * cs, st));
   grid_dispatch<R>(g.kernel.W, false, cx_.num_sms, smem, st, ga, make_geom(g),
