@@ -1144,13 +1144,13 @@ k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
     {
       // stage the cells the chunk reads: footprint by footprint when few
       // origins are used (cells shared by footprints are written twice with
-      // the same value), else the bounding box; four loads in flight
+      // the same value), else the bounding box; eight loads in flight
       const int lu0 = sh_bb[0], lv0 = sh_bb[2];
       const int nbu = max(sh_bb[1] + W - lu0, 0), nbv = max(sh_bb[3] + W - lv0, 0);
       const int ucorner = tu * g.T - g.nsafe, vcorner = tv * g.T - g.nsafe;
       const int norig = sh_norig;
       const bool by_list = norig <= kMaxOrig && norig * W * W < nbu * nbv;
-      // (plane, row) lines over warps, lanes along v, four lines in flight
+      // (plane, row) lines over warps, lanes along v, eight lines in flight
       const int nline = by_list ? norig * W * W : W * nbu;
       const int linelen = by_list ? W : nbv;
       const JobRegs jr(jb);
@@ -1158,11 +1158,11 @@ k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
       // NWARP lines without a division
       int bp = 0, br = warp;
       while (!by_list && nbu > 0 && br >= nbu) { br -= nbu; ++bp; }
-      for (int l0 = warp; l0 < nline; l0 += 4 * NWARP) {
-        C val[4];
-        int sidx[4];
+      for (int l0 = warp; l0 < nline; l0 += 8 * NWARP) {
+        C val[8];
+        int sidx[8];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < 8; ++q) {
           const int line = l0 + q * NWARP;
           const int lp = bp, lr = br;
           if (!by_list) {
@@ -1197,7 +1197,7 @@ k_interp(GridArgs a, DevGeom g, DevKernel<R> kc) {
           }
         }
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < 8; ++q) {
           if (sidx[q] >= 0) {
             tre[sidx[q]] = val[q].x;
             tim[sidx[q]] = val[q].y;
