@@ -49,7 +49,7 @@ struct GridKernels {
       fn<<<grid, NWARP * 32, smem, st>>>(a, g, kc);
     }
     cuda_check(cudaGetLastError(), spread ? "k_spread launch" : "k_interp launch");
-  g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
   }
   template <int W>
   static int occupancy(bool spread, size_t smem) {
@@ -216,17 +216,33 @@ struct ColKernels {
     const size_t extra = size_t(a.K) * (M / 16 + 32) * cs;
     auto *k0 = k_ucol_fwd_bulk<R, LOGM, false>;
     auto *k1 = k_ucol_fwd_bulk<R, LOGM, true>;
+    // resident CTAs of each instantiation at these sizes, memoised (the
+    // query is a driver call, and plans enqueue while a stream is captured)
+    static std::mutex mu;
+    static std::map<std::tuple<size_t, size_t, int>, std::pair<int, int>> memo;
+    int dev0 = 0;
+    cuda_check(cudaGetDevice(&dev0), "cudaGetDevice");
+    const auto key = std::make_tuple(base, extra, dev0);
     int n0 = 0, n1 = 0;
     smem_attr(k0, base);
-    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n0, k0, Cfg::THREADS, base),
-               "occupancy");
-    if (n0 < 1) return false;
-    if (base + extra <= 227 * 1024) {
-      smem_attr(k1, base + extra);
-      cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n1, k1, Cfg::THREADS,
-                                                               base + extra),
-                 "occupancy");
+    if (base + extra <= 227 * 1024) smem_attr(k1, base + extra);
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      auto it = memo.find(key);
+      if (it != memo.end()) {
+        n0 = it->second.first;
+        n1 = it->second.second;
+      } else {
+        cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n0, k0, Cfg::THREADS, base),
+                   "occupancy");
+        if (base + extra <= 227 * 1024)
+          cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n1, k1, Cfg::THREADS,
+                                                                   base + extra),
+                     "occupancy");
+        memo[key] = std::make_pair(n0, n1);
+      }
     }
+    if (n0 < 1) return false;
     const bool tws = n1 >= n0;
     const size_t smem = tws ? base + extra : base;
     auto *kern = tws ? k1 : k0;
