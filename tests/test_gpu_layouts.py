@@ -1,0 +1,73 @@
+"""Awkward image geometries for the u transform's segmented rows: widths that
+are not multiples of 32, unequal sides, and u bands narrow enough that the
+transform of an image column runs as several twisted passes (nu = K M with
+K > 1, so each row holds K segments).  Both precisions, both directions,
+against the FP64 DFT, plus the adjoint identity."""
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+KW = dict(negate_v=True, divide_by_n=False, sigma_min=1.1, sigma_max=2.0)
+C = 299792458.0
+# (nx, ny): odd multiples of 2, one side far from a multiple of 32
+CASES = [(1000, 1002), (1234, 778), (258, 1030), (998, 64)]
+TOL = {"mixed": (1e-5, 1e-5), "fp64": (1e-12, 1e-11)}  # (epsilon, tolerance vs DFT)
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    from wsclean_b200.gridder import Context
+    c = Context(0)
+    yield c
+    c.close()
+
+
+def _problem(nx, ny, seed):
+    rng = np.random.default_rng(seed)
+    nrow, nchan = 4000, 2
+    px = np.deg2rad(10 / 3600)
+    freq = np.array([1.40e8, 1.45e8])
+    # |u|, |v| up to 0.12 / px wavelengths: the data fill about a quarter of
+    # the grid along u, so the pruned u transform needs K > 1 passes
+    umax = 0.12 / px * C / freq.max()
+    uvw = rng.uniform(-1, 1, (nrow, 3)) * np.array([umax, umax, 0.2 * umax])
+    vis = rng.normal(size=(nrow, nchan)) + 1j * rng.normal(size=(nrow, nchan))
+    return rng, uvw, freq, vis, px
+
+
+@pytest.mark.parametrize("prec", ["mixed", "fp64"])
+@pytest.mark.parametrize("nx,ny", CASES)
+def test_segmented_rows_match_dft_and_adjoint(ctx, prec, nx, ny):
+    eps, tol = TOL[prec]
+    rng, uvw, freq, vis, px = _problem(nx, ny, nx * 7 + ny)
+    cdt = np.complex64 if prec == "mixed" else np.complex128
+    vis = vis.astype(cdt)
+    d = ctx.ms2dirty(uvw, freq, vis, nx, ny, px, px, eps, precision=prec,
+                     dirty_dtype=np.float64, **KW)
+    st = ctx.stats()
+    assert 2 * st["band_rows"] <= st["nu"]  # a pruned band: K = nu / M >= 2
+    pix = np.concatenate([rng.integers(0, nx * ny, 48), [0, ny - 1, (nx - 1) * ny, nx * ny - 1]])
+    dft = O.dft_ms2dirty(uvw, freq, vis, nx, ny, px, px, negate_v=True, divide_by_n=False,
+                         pixels=pix)
+    assert O.rel_rms(d.ravel()[pix], dft) < tol
+    # prediction of a sparse model, including the image's corner pixels
+    model = np.zeros((nx, ny))
+    model[rng.integers(0, nx, 30), rng.integers(0, ny, 30)] = rng.uniform(0.5, 2, 30)
+    model[0, 0] = model[nx - 1, ny - 1] = model[0, ny - 1] = model[nx - 1, 0] = 1.0
+    fdt = np.float32 if prec == "mixed" else np.float64
+    v = ctx.dirty2ms(uvw, freq, model.astype(fdt), px, px, eps, precision=prec,
+                     vis_dtype=np.complex128, **KW)
+    sel = rng.choice(v.size, 3000, replace=False)
+    vdft = O.dft_dirty2ms(uvw, freq, model, px, px, negate_v=True, divide_by_n=False, select=sel)
+    assert O.rel_rms(v.ravel()[sel], vdft) < tol
+    # <y, A x> = <A^H y, x> with A = dirty2ms
+    x = rng.normal(size=(nx, ny))
+    ax = ctx.dirty2ms(uvw, freq, x.astype(fdt), px, px, eps, precision=prec,
+                      vis_dtype=np.complex128, **KW)
+    aty = ctx.ms2dirty(uvw, freq, vis, nx, ny, px, px, eps, precision=prec,
+                       dirty_dtype=np.float64, **KW)
+    a = np.vdot(vis.astype(np.complex128).ravel(), ax.ravel()).real
+    b = np.vdot(aty.ravel(), x.ravel()).real
+    assert abs(a - b) / (np.linalg.norm(vis) * np.linalg.norm(ax)) < (1e-6 if prec == "mixed" else 1e-12)
