@@ -171,3 +171,37 @@ def test_stream_pipelined_prediction(cfg5):
     finally:
         ctx.close()
     assert O.rel_rms(out.numpy(), ref) < 1e-7
+
+
+def test_stream_in_plane_passes(monkeypatch):
+    """A stream whose w planes do not all fit its transformed-row buffer
+    (here capped at three planes a pass, as memory pressure would) transforms
+    the planes in passes; with several twisted passes a row is longer than
+    the image, which the pass count must allow for.  The image and the
+    predictions equal the single calls'."""
+    from wsclean_b200 import gridder as G
+    monkeypatch.setenv("WSG_MAX_PLANES", "3")
+    rng = np.random.default_rng(8)
+    nrow, nx, ny = 6000, 256, 200
+    freq = np.array([1.40e8, 1.45e8])
+    px = np.deg2rad(20 / 3600)
+    umax = 0.1 / px * 299792458.0 / freq.max()
+    uvw = rng.uniform(-1, 1, (nrow, 3)) * np.array([umax, umax, 0.6 * umax])
+    vis = (rng.normal(size=(nrow, 2)) + 1j * rng.normal(size=(nrow, 2))).astype(np.complex64)
+    ext = G.data_extent(uvw, freq)
+    parts = chunks(nrow, 4)
+    with G.Stream(freq, nx, ny, px, px, 1e-5, ext, nvis=vis.size, dirty_dtype=np.float64,
+                  **KW) as s:
+        for a, b in parts:
+            s.add(uvw[a:b], vis[a:b])
+        d = s.finish()
+        st = s.stats()
+        assert st["nplanes"] > 3 and 2 * st["band_rows"] <= st["nu"]
+        model = np.zeros((nx, ny), np.float32)
+        model[rng.integers(0, nx, 20), rng.integers(0, ny, 20)] = 1.0
+        s.predict_begin(model)
+        v = np.concatenate([s.predict(uvw[a:b]) for a, b in parts])
+    ref = G.ms2dirty(uvw, freq, vis, nx, ny, px, px, 1e-5, dirty_dtype=np.float64, **KW)
+    assert O.rel_rms(d, ref) < 5e-6
+    vref = G.dirty2ms(uvw, freq, model, px, px, 1e-5, **KW)
+    assert O.rel_rms(v, vref) < 1e-6

@@ -206,6 +206,10 @@ struct ColKernels {
     using Cfg = ColCfg<R, M>;
     constexpr int NB = Cfg::NB;
     if (!err || env_int("WSG_UCOL_TMA", 1) == 0) return false;
+    // a CTA of one column (M = 8192 in FP32, 4096 in FP64) waits on each of
+    // its copies with nothing else to do: the plain kernel is faster there
+    // (config 5's forward transform: 30 ms plain, 65 ms staged)
+    if (NB < 2) return false;
     const size_t cs = 2 * sizeof(R);
     if ((size_t(a.hseg) * cs) % 16 != 0 || (reinterpret_cast<uintptr_t>(a.H) & 15) != 0)
       return false;

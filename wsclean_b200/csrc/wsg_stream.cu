@@ -145,7 +145,10 @@ size_t StreamGridder::plane_batch() const {
   size_t freeb = 0, total = 0;
   CK(cudaMemGetInfo(&freeb, &total));
   const size_t per = gp_.hrow() * gp_.ny * (dbl_ ? 16 : 8);
-  return std::max<size_t>(1, std::min<size_t>(gp_.nplanes, (freeb / 4) / std::max<size_t>(per, 1)));
+  size_t P = std::max<size_t>(1, std::min<size_t>(gp_.nplanes, (freeb / 4) / std::max<size_t>(per, 1)));
+  const int lim = env_int("WSG_MAX_PLANES", 0);  // a test and debugging limit
+  if (lim > 0) P = std::min<size_t>(P, size_t(lim));
+  return P;
 }
 
 // Stages a chunk: device pointers are used in place; page-locked host
@@ -366,7 +369,9 @@ void StreamGridder::finish_t(void *dirty, int accumulate) {
   else
     CF(cufftExecC2C(fft_, reinterpret_cast<cufftComplex *>(band_.p),
                     reinterpret_cast<cufftComplex *>(band_.p), CUFFT_INVERSE));
-  const size_t P = std::max<size_t>(1, H_.n / (npix * cs));
+  // planes per pass: as many u-transformed plane images (ny rows of hrow
+  // entries) as H holds
+  const size_t P = std::max<size_t>(1, H_.n / (g.hrow() * g.ny * cs));
   int *d_err = reinterpret_cast<int *>(reinterpret_cast<char *>(cx_.b_small.p) + 3072);
   if (!err_armed_) {
     CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
@@ -410,9 +415,13 @@ template <typename R>
 void StreamGridder::predict_begin_t(const double *img) {
   const GridPlan &g = gp_;
   cudaStream_t st = cx_.stream;
-  const size_t cs = 2 * sizeof(R), npix = g.nx * g.ny;
+  const size_t cs = 2 * sizeof(R);
+  int *d_err = reinterpret_cast<int *>(reinterpret_cast<char *>(cx_.b_small.ensure(4096)) + 3072);
+  CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
   CK(cudaMemsetAsync(band_.p, 0, band_.n, st));
-  const size_t P = std::max<size_t>(1, H_.n / (npix * cs));
+  // planes per pass: as many u-transformed plane images (ny rows of hrow
+  // entries) as H holds
+  const size_t P = std::max<size_t>(1, H_.n / (g.hrow() * g.ny * cs));
   for (size_t p0 = 0; p0 < g.nplanes; p0 += P) {
     const size_t np = std::min(P, g.nplanes - p0);
     ScreenArgs sa = make_screen(g, reinterpret_cast<const double *>(cf_.p), cc_, np);
@@ -421,7 +430,7 @@ void StreamGridder::predict_begin_t(const double *img) {
     const dim3 sg = screen_grid(g);
     launch_screen_put<R>(sg, st, sa, img, 0, H_.p);
     ColArgs ca = make_col(g, g.nplanes, tw_.p, static_cast<char *>(band_.p) + p0 * g.nv * cs, H_.p);
-    col_run<R>(g.logM, false, ca, int(np), st);
+    col_run<R>(g.logM, false, ca, int(np), st, d_err);  // (the staged forms report on d_err)
   }
   CF(cufftSetStream(fft_, st));
   CF(cufftSetWorkArea(fft_, fftwork_.p));
@@ -431,6 +440,9 @@ void StreamGridder::predict_begin_t(const double *img) {
   else
     CF(cufftExecC2C(fft_, reinterpret_cast<cufftComplex *>(band_.p),
                     reinterpret_cast<cufftComplex *>(band_.p), CUFFT_FORWARD));
+  // a staged copy of the u transform that did not complete (once per model;
+  // synchronises the stream)
+  cx_.check_device_error(d_err);
 }
 
 void StreamGridder::predict_begin(const void *dirty) {
