@@ -1867,6 +1867,90 @@ __device__ __forceinline__ void col_fft_inplace(C (&v)[16], C *buf, const C *tw,
   col_tail_inplace<C, M, 16, TPF, SIGN>(buf, tw, t, o);
 }
 
+// One-column geometries (M = 8192 in FP32, where a CTA of M/16 threads
+// takes one image column): k_ucol_bwd_pair gives a CTA two adjacent columns,
+// loads both -- 16 bytes a band row instead of 8, half the sectors fetched
+// for the data used -- and transforms them in turn, each in place in its own
+// buffer (the band values of the column in hand stay in registers across
+// the twist passes).
+template <typename R, int LOGM>
+__global__ void __launch_bounds__(ColCfg<R, (1 << LOGM)>::THREADS, 1)
+k_ucol_bwd_pair(ColArgs a) {
+  using C = typename Cplx<R>::type;
+  constexpr int M = 1 << LOGM, TPF = ColCfg<R, M>::TPF;
+  static_assert(ColCfg<R, M>::NB == 1, "for one-column CTAs");
+  constexpr int THREADS = TPF;
+  constexpr int BL = FftBuf<M>::value;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *buf = reinterpret_cast<C *>(smem_raw);  // [2][BL]
+  C *tws = buf + 2 * BL;                     // [M]
+  const int t = threadIdx.x;
+  const int lp = blockIdx.y, j0 = blockIdx.x * 2;
+  const C *band = reinterpret_cast<const C *>(a.band);
+  const C *twB = reinterpret_cast<const C *>(a.twB);
+  const C *twQ = reinterpret_cast<const C *>(a.twQ);
+  fill_table<C, M, THREADS>(tws, reinterpret_cast<const C *>(a.twM));
+  // both columns, slot-major with the column pair innermost (adjacent threads
+  // read the two columns of one band row), eight loads in flight a thread
+#pragma unroll
+  for (int h = 0; h < 4; ++h) {
+    C val[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int item = t + (h * 8 + q) * THREADS;
+      const int c = item & 1, b = item >> 1;
+      const int jj = j0 + c;
+      val[q].x = R(0);
+      val[q].y = R(0);
+      const int u = slot_u(a, b, M);
+      if (jj < a.ny && u < (1 << 29)) {
+        int jx = jj + a.nv - a.ny / 2;
+        jx -= (jx >= a.nv) ? a.nv : 0;
+        val[q] = band[(size_t(slot_bi(a, u)) * a.P + lp) * a.nv + jx];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int item = t + (h * 8 + q) * THREADS;
+      buf[(item & 1) * BL + fpad(item >> 1)] = val[q];
+    }
+  }
+  __syncthreads();
+#pragma unroll 1
+  for (int c = 0; c < 2; ++c) {
+    const int j = j0 + c;
+    const bool jv = j < a.ny;
+    C *A = buf + c * BL;
+    C g[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) g[q] = A[fpad(t + TPF * q)];
+    C *rowp = reinterpret_cast<C *>(a.H) + (size_t(lp) * a.ny + (jv ? j : 0)) * (size_t(a.K) * a.hseg);
+    for (int k2 = 0; k2 < a.K; ++k2) {
+      C v[16];
+      if (k2 == 0) {
+#pragma unroll
+        for (int q = 0; q < 16; ++q) v[q] = g[q];
+      } else {
+        const C base = __ldg(&twB[k2 * TPF + t]);
+#pragma unroll
+        for (int q = 0; q < 16; ++q)
+          v[q] = cmul(g[q], col_twist<C, TPF>(a, twB, twQ, k2, t, q, M, base));
+      }
+      C o[16];
+      // (its first barrier keeps the in-place writes after every thread's reads of A)
+      col_fft_inplace<C, M, TPF, +1>(v, A, tws, t, o);
+      if (jv) {
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          bool keep;
+          const int pos = h_pos<TPF>(a, k2, t, q, keep);
+          if (keep) rowp[pos] = o[q];
+        }
+      }
+    }
+  }
+}
+
 template <typename R, int LOGM, bool TWS>
 __global__ void __launch_bounds__(ColCfg<R, (1 << LOGM)>::THREADS, ColCfg<R, (1 << LOGM)>::MINB)
 k_ucol_bwd_tma(ColArgs a, const __grid_constant__ CUtensorMap tmap, int npl, int *err) {

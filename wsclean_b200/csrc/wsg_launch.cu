@@ -267,6 +267,18 @@ struct ColKernels {
     using Cfg = ColCfg<R, M>;
     if (bwd && run_tma<LOGM>(a, npl, st, err)) return;
     if (!bwd && run_bulk<LOGM>(a, npl, st, err)) return;
+    if constexpr (sizeof(R) == 4 && Cfg::NB == 1) {
+      if (bwd) {  // one-column CTAs: two columns a CTA, loaded together
+        const size_t smem = (2 * size_t(FftBuf<M>::value) + M) * 2 * sizeof(R);
+        auto *kern = k_ucol_bwd_pair<R, LOGM>;
+        smem_attr(kern, smem);
+        dim3 grid((a.ny + 1) / 2, npl);
+        kern<<<grid, Cfg::THREADS, smem, st>>>(a);
+        cuda_check(cudaGetLastError(), "k_ucol_bwd_pair launch");
+        g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+        return;
+      }
+    }
     const size_t smem = ColSmem2<R, M>::bytes();
     dim3 grid((a.ny + Cfg::NB - 1) / Cfg::NB, npl);
     if (bwd) {
