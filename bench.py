@@ -597,6 +597,22 @@ def leg_config5(torch, dev, ctx, grids, with_cpu, args):
         out["accuracy"]["ms2dirty_rel_rms_vs_dft_8px"] = rel_rms(
             h_dirty.numpy().ravel()[pix],
             dft_pixels(uvw, freq, h_vis.numpy(), nx, nx, px, px, pix, torch, dev))
+        # the streamed ms2dirty again with Briggs(0) imaging weights, looked
+        # up on the device while each batch is scanned and recorded; the
+        # weight grid is built from every chunk first, as WSClean does
+        from wsclean_b200.gridder import ImageWeights
+        iw = ImageWeights("briggs", 0.0, nx, nx, px, px, context=ctx)
+        try:
+            def build_weights():
+                for a, b in parts:
+                    iw.grid(h_uvw[a:b], freq)
+                iw.finish()
+            t_wbuild = wall(build_weights)
+            s.set_imaging_weights(iw)
+            t_m2d_briggs = wall(lambda: m2d(h_uvw, h_vis, h_dirty))
+            s.set_imaging_weights(None)
+        finally:
+            iw.close()
         # the same passes with the data resident in HBM
         d_uvw = h_uvw.to(dev)
         d_vis = h_vis.to(dev)
@@ -619,6 +635,8 @@ def leg_config5(torch, dev, ctx, grids, with_cpu, args):
     out.update({
         "ms2dirty_mvis_s": nvis / t_m2d / 1e3, "dirty2ms_mvis_s": nvis / t_d2m / 1e3,
         "dirty2ms_synchronous_chunks_mvis_s": nvis / t_d2m_sync / 1e3,
+        "ms2dirty_briggs_weights_mvis_s": nvis / t_m2d_briggs / 1e3,
+        "briggs_weights_build_ms": t_wbuild,
         "value": nvis / (t_m2d + t_d2m) / 1e3, "ms_per_step": t_m2d + t_d2m,
         "resident_ms2dirty_mvis_s": nvis / r_m2d / 1e3, "resident_dirty2ms_mvis_s": nvis / r_d2m / 1e3,
         "resident_value": nvis / (r_m2d + r_d2m) / 1e3,
