@@ -302,9 +302,6 @@ void set_band(GridPlan &g) {
 
 }  // namespace
 
-// nu = K * 2^m with 2^m >= 2L+1, so that the occupied u band fits one pruned
-// FFT of length 2^m (or K = 1, 2^m = nu when the band covers the grid);
-// the smallest such nu >= n0.
 // Shared memory of one spread / interpolation CTA: the W-plane tile of
 // (T + W - 1)^2 cells (odd row stride, plane stride 8 mod 32, real and
 // imaginary parts) and 8 warps' record staging (the layout of the device
@@ -319,10 +316,12 @@ size_t tile_smem_bytes(int T, int W, bool fp32) {
   return ((rs * 2 * size_t(W) * PS + 15) & ~size_t(15)) + 8 * stage;
 }
 
-bool pick_nu(double n0, double umax_px, int W, bool fp32, size_t &nu, int &logM, int &K) {
-  const int mmax = fp32 ? 13 : 12;
+// nu = K * 2^m with 2^m >= 2L+1, so that the occupied u band fits one pruned
+// FFT of length 2^m, 256 <= 2^m <= 8192 (or K = 1, 2^m = nu when the band
+// covers the grid); the smallest such nu >= n0.
+bool pick_nu(double n0, double umax_px, int W, size_t &nu, int &logM, int &K) {
   size_t best = ~size_t(0);
-  for (int m = 8; m <= mmax; ++m) {
+  for (int m = 8; m <= 13; ++m) {
     const size_t M = size_t(1) << m;
     const size_t k = std::max<size_t>(1, size_t(std::ceil(n0 / double(M))));
     const size_t n = k * M;
@@ -384,7 +383,7 @@ void choose_grid(GridPlan &g, double sigma_min, double sigma_max, int tile, bool
     if (g.force_W && (k.W != g.force_W || std::fabs(k.sigma - g.force_sigma) > 1e-12)) continue;
     GridPlan t = g;
     t.kernel = k;
-    if (!pick_nu(g.nx * k.sigma, umax_px, k.W, g.fp32, t.nu, t.logM, t.K)) continue;
+    if (!pick_nu(g.nx * k.sigma, umax_px, k.W, t.nu, t.logM, t.K)) continue;
     t.nv = 2 * good_size_v(size_t(g.ny * k.sigma * 0.5) + 1);
     if (pow2_v) {
       size_t p2 = 256;

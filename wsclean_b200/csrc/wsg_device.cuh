@@ -1867,12 +1867,12 @@ __device__ __forceinline__ void col_fft_inplace(C (&v)[16], C *buf, const C *tw,
   col_tail_inplace<C, M, 16, TPF, SIGN>(buf, tw, t, o);
 }
 
-// One-column geometries (M = 8192 in FP32, where a CTA of M/16 threads
-// takes one image column): k_ucol_bwd_pair gives a CTA two adjacent columns,
-// loads both -- 16 bytes a band row instead of 8, half the sectors fetched
-// for the data used -- and transforms them in turn, each in place in its own
-// buffer (the band values of the column in hand stay in registers across
-// the twist passes).
+// One-column geometries (M = 4096 and 8192 in FP32, where a CTA of M/16
+// threads takes one image column): k_ucol_bwd_pair gives a CTA two adjacent
+// columns, loads both -- 16 bytes a band row instead of 8, half the sectors
+// fetched for the data used -- and transforms them in turn, each in place in
+// its own buffer (the band values of the column in hand stay in registers
+// across the twist passes).
 template <typename R, int LOGM>
 __global__ void __launch_bounds__(ColCfg<R, (1 << LOGM)>::THREADS, 1)
 k_ucol_bwd_pair(ColArgs a) {
@@ -1948,6 +1948,261 @@ k_ucol_bwd_pair(ColArgs a) {
         }
       }
     }
+  }
+}
+
+// The forward transform of one-column geometries, as k_ucol_bwd_pair: two
+// adjacent columns a CTA, each transformed and accumulated in its own buffer
+// in turn, then both stored together -- 16 bytes a band row instead of 8.
+template <typename R, int LOGM>
+__global__ void __launch_bounds__(ColCfg<R, (1 << LOGM)>::THREADS, 1)
+k_ucol_fwd_pair(ColArgs a) {
+  using C = typename Cplx<R>::type;
+  constexpr int M = 1 << LOGM, TPF = ColCfg<R, M>::TPF;
+  static_assert(ColCfg<R, M>::NB == 1, "for one-column CTAs");
+  constexpr int THREADS = TPF;
+  constexpr int BL = FftBuf<M>::value;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *buf = reinterpret_cast<C *>(smem_raw);  // [2][BL]
+  C *tws = buf + 2 * BL;                     // [M]
+  const int t = threadIdx.x;
+  const int lp = blockIdx.y, j0 = blockIdx.x * 2;
+  C *band = reinterpret_cast<C *>(a.band);
+  const C *twB = reinterpret_cast<const C *>(a.twB);
+  const C *twQ = reinterpret_cast<const C *>(a.twQ);
+  fill_table<C, M, THREADS>(tws, reinterpret_cast<const C *>(a.twM));
+  __syncthreads();  // the stage table is in place
+#pragma unroll 1
+  for (int c = 0; c < 2; ++c) {
+    const int j = j0 + c;
+    const bool jv = j < a.ny;
+    C *A = buf + c * BL;
+    const C *rowp = reinterpret_cast<const C *>(a.H) +
+                    (size_t(lp) * a.ny + (jv ? j : 0)) * (size_t(a.K) * a.hseg);
+    C acc[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) acc[q].x = acc[q].y = R(0);
+    for (int k2 = 0; k2 < a.K; ++k2) {
+      C v[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        bool keep;
+        const int pos = h_pos<TPF>(a, k2, t, q, keep);
+        v[q].x = R(0);
+        v[q].y = R(0);
+        if (jv && keep) v[q] = rowp[pos];
+      }
+      C o[16];
+      col_fft_inplace<C, M, TPF, -1>(v, A, tws, t, o);
+      if (k2 == 0) {
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          acc[q].x += o[q].x;
+          acc[q].y += o[q].y;
+        }
+      } else {
+        const C base = __ldg(&twB[k2 * TPF + t]);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          C w = col_twist<C, TPF>(a, twB, twQ, k2, t, q, M, base);
+          w.y = -w.y;
+          const C val = cmul(o[q], w);
+          acc[q].x += val.x;
+          acc[q].y += val.y;
+        }
+      }
+    }
+    __syncthreads();  // the last transform's reads of A are done
+#pragma unroll
+    for (int q = 0; q < 16; ++q) A[fpad(t + TPF * q)] = acc[q];
+  }
+  __syncthreads();
+  // both columns, the pair innermost: adjacent threads store one band row's
+  // two columns
+  for (int item = t; item < 2 * M; item += THREADS) {
+    const int c = item & 1, b = item >> 1;
+    const int jj = j0 + c;
+    const int u = slot_u(a, b, M);
+    if (jj < a.ny && u < (1 << 29)) {
+      int jx = jj + a.nv - a.ny / 2;
+      jx -= (jx >= a.nv) ? a.nv : 0;
+      band[(size_t(slot_bi(a, u)) * a.P + lp) * a.nv + jx] = buf[c * BL + fpad(b)];
+    }
+  }
+}
+
+// ---- FP64 transforms of 8192 points ----
+//
+// One column a CTA of M/16 = 512 threads, transformed in place in one padded
+// buffer (139 KB).  The stage tables of every stage but the last (4080
+// entries, 65 KB) are in shared memory; the last stage (radix 2, stride
+// 4096) reads its 4096 twiddles from global memory, where every CTA reads
+// the same 64 KB (L1/L2-resident).  Outputs leave the last stage through
+// emit(q, X[t + TPF q]) as they are made, so no register array of outputs
+// outlives the transform (512 threads leave 128 registers a thread).
+
+// Stride of the last stage of an M-point transform (radix-16 stages before it).
+template <int M>
+struct ColLastNS {
+  static constexpr int get() {
+    int ns = 1;
+    while (M / ns > 16) ns *= 16;
+    return ns;
+  }
+  static constexpr int value = get();
+};
+
+template <typename C, int M, int NS, int TPF, int SIGN, typename Emit>
+__device__ __forceinline__ void col_tail_emit(C *buf, const C *tws, const C *twg, int t,
+                                              Emit &emit) {
+  if constexpr (M / NS > 16) {
+    C v[16];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r] = buf[fpad(t + r * TPF)];
+    const int k = t & (NS - 1);
+    constexpr int off = TwOffset<NS>::value;
+#pragma unroll
+    for (int r = 1; r < 16; ++r) {
+      C w = tws[off + (r - 1) * NS + k];
+      if (SIGN < 0) w.y = -w.y;
+      v[r] = cmul(v[r], w);
+    }
+    dft_reg<16>(v, SIGN);
+    const int d = (t / NS) * NS * 16 + k;
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 16; ++r) buf[fpad(d + r * NS)] = v[r];
+    __syncthreads();
+    col_tail_emit<C, M, NS * 16, TPF, SIGN>(buf, tws, twg, t, emit);
+  } else {
+    constexpr int RL = M / NS, IT = 16 / RL;
+    constexpr int off = TwOffset<NS>::value;
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+      const int j = t + TPF * it;
+      C v[RL];
+#pragma unroll
+      for (int r = 0; r < RL; ++r) v[r] = buf[fpad(j + r * NS)];
+#pragma unroll
+      for (int r = 1; r < RL; ++r) {
+        C w = __ldg(&twg[off + (r - 1) * NS + j]);
+        if (SIGN < 0) w.y = -w.y;
+        v[r] = cmul(v[r], w);
+      }
+      dft_reg<RL>(v, SIGN);
+#pragma unroll
+      for (int r = 0; r < RL; ++r) emit(it + r * IT, v[r]);
+    }
+  }
+}
+
+// v[q] = x[t + TPF q] -> emit(q, X[t + TPF q]); tws: the shared stage tables
+// before the last stage's, twg: the full table in global memory.
+template <typename C, int M, int TPF, int SIGN, typename Emit>
+__device__ __forceinline__ void col_fft_emit(C (&v)[16], C *buf, const C *tws, const C *twg,
+                                             int t, Emit &emit) {
+  dft_reg<16>(v, SIGN);
+  __syncthreads();  // earlier readers of buf are done
+#pragma unroll
+  for (int r = 0; r < 16; ++r) buf[fpad(16 * t + r)] = v[r];
+  __syncthreads();
+  col_tail_emit<C, M, 16, TPF, SIGN>(buf, tws, twg, t, emit);
+}
+
+template <int M>
+struct ColBig {
+  static constexpr int TPF = M / 16;
+  static constexpr int NTAB = TwOffset<ColLastNS<M>::value>::value;  // shared table entries
+  static constexpr size_t bytes() { return (size_t(FftBuf<M>::value) + NTAB) * 2 * sizeof(double); }
+};
+
+// ms2dirty direction (band rows -> H image rows, backward transform), one
+// image column j = blockIdx.x of plane lp = blockIdx.y.  The band column is
+// read again for each twisted pass (from L2 after the first).
+template <int LOGM>
+__global__ void __launch_bounds__(ColBig<(1 << LOGM)>::TPF, 1) k_ucol_bwd_big(ColArgs a) {
+  using C = double2;
+  constexpr int M = 1 << LOGM, TPF = ColBig<M>::TPF;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *buf = reinterpret_cast<C *>(smem_raw);
+  C *tws = buf + FftBuf<M>::value;
+  const int t = threadIdx.x, j = blockIdx.x, lp = blockIdx.y;
+  const C *band = reinterpret_cast<const C *>(a.band);
+  const C *twB = reinterpret_cast<const C *>(a.twB);
+  const C *twQ = reinterpret_cast<const C *>(a.twQ);
+  const C *twg = reinterpret_cast<const C *>(a.twM);
+  C *rowp = reinterpret_cast<C *>(a.H) + (size_t(lp) * a.ny + j) * (size_t(a.K) * a.hseg);
+  int jx = j + a.nv - a.ny / 2;
+  jx -= (jx >= a.nv) ? a.nv : 0;
+  // (ordered before its first use by the transform's barriers)
+  fill_table<C, ColBig<M>::NTAB, TPF>(tws, twg);
+  for (int k2 = 0; k2 < a.K; ++k2) {
+    C v[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const int u = slot_u(a, t + TPF * q, M);
+      v[q].x = v[q].y = 0.0;
+      if (u < (1 << 29)) v[q] = band[(size_t(slot_bi(a, u)) * a.P + lp) * a.nv + jx];
+    }
+    if (k2 > 0) {
+      const C base = __ldg(&twB[k2 * TPF + t]);
+#pragma unroll
+      for (int q = 0; q < 16; ++q) v[q] = cmul(v[q], col_twist<C, TPF>(a, twB, twQ, k2, t, q, M, base));
+    }
+    auto emit = [&](int q, C val) {
+      bool keep;
+      const int pos = h_pos<TPF>(a, k2, t, q, keep);
+      if (keep) rowp[pos] = val;
+    };
+    col_fft_emit<C, M, TPF, +1>(v, buf, tws, twg, t, emit);
+  }
+}
+
+// dirty2ms direction (H image rows -> band rows, forward transform).  Each
+// pass's twisted outputs are summed in the band array itself: every thread
+// owns the same band slots in every pass, so the read-modify-write needs no
+// synchronisation.
+template <int LOGM>
+__global__ void __launch_bounds__(ColBig<(1 << LOGM)>::TPF, 1) k_ucol_fwd_big(ColArgs a) {
+  using C = double2;
+  constexpr int M = 1 << LOGM, TPF = ColBig<M>::TPF;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *buf = reinterpret_cast<C *>(smem_raw);
+  C *tws = buf + FftBuf<M>::value;
+  const int t = threadIdx.x, j = blockIdx.x, lp = blockIdx.y;
+  C *band = reinterpret_cast<C *>(a.band);
+  const C *twB = reinterpret_cast<const C *>(a.twB);
+  const C *twQ = reinterpret_cast<const C *>(a.twQ);
+  const C *twg = reinterpret_cast<const C *>(a.twM);
+  const C *rowp = reinterpret_cast<const C *>(a.H) + (size_t(lp) * a.ny + j) * (size_t(a.K) * a.hseg);
+  int jx = j + a.nv - a.ny / 2;
+  jx -= (jx >= a.nv) ? a.nv : 0;
+  fill_table<C, ColBig<M>::NTAB, TPF>(tws, twg);
+  for (int k2 = 0; k2 < a.K; ++k2) {
+    C v[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      bool keep;
+      const int pos = h_pos<TPF>(a, k2, t, q, keep);
+      v[q].x = v[q].y = 0.0;
+      if (keep) v[q] = rowp[pos];
+    }
+    const C base = k2 > 0 ? __ldg(&twB[k2 * TPF + t]) : make_double2(1.0, 0.0);
+    auto emit = [&](int q, C val) {
+      const int u = slot_u(a, t + TPF * q, M);
+      if (u >= (1 << 29)) return;
+      C *dst = &band[(size_t(slot_bi(a, u)) * a.P + lp) * a.nv + jx];
+      if (k2 > 0) {
+        C w = col_twist<C, TPF>(a, twB, twQ, k2, t, q, M, base);
+        w.y = -w.y;
+        val = cmul(val, w);
+        const C old = *dst;
+        val.x += old.x;
+        val.y += old.y;
+      }
+      *dst = val;
+    };
+    col_fft_emit<C, M, TPF, -1>(v, buf, tws, twg, t, emit);
   }
 }
 

@@ -265,19 +265,36 @@ struct ColKernels {
   static void run1(bool bwd, const ColArgs &a, int npl, cudaStream_t st, int *err) {
     constexpr int M = 1 << LOGM;
     using Cfg = ColCfg<R, M>;
+    if constexpr (sizeof(R) == 8 && LOGM == 13) {
+      // FP64 8192-point transforms: one column a CTA, the last stage's
+      // twiddles from global memory
+      const size_t smem = ColBig<M>::bytes();
+      auto *kern = bwd ? k_ucol_bwd_big<LOGM> : k_ucol_fwd_big<LOGM>;
+      smem_attr(kern, smem);
+      dim3 grid(a.ny, npl);
+      kern<<<grid, ColBig<M>::TPF, smem, st>>>(a);
+      cuda_check(cudaGetLastError(), bwd ? "k_ucol_bwd_big launch" : "k_ucol_fwd_big launch");
+      g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+    } else {
+      run1s<LOGM>(bwd, a, npl, st, err);
+    }
+  }
+  template <int LOGM>
+  static void run1s(bool bwd, const ColArgs &a, int npl, cudaStream_t st, int *err) {
+    constexpr int M = 1 << LOGM;
+    using Cfg = ColCfg<R, M>;
     if (bwd && run_tma<LOGM>(a, npl, st, err)) return;
     if (!bwd && run_bulk<LOGM>(a, npl, st, err)) return;
     if constexpr (sizeof(R) == 4 && Cfg::NB == 1) {
-      if (bwd) {  // one-column CTAs: two columns a CTA, loaded together
-        const size_t smem = (2 * size_t(FftBuf<M>::value) + M) * 2 * sizeof(R);
-        auto *kern = k_ucol_bwd_pair<R, LOGM>;
-        smem_attr(kern, smem);
-        dim3 grid((a.ny + 1) / 2, npl);
-        kern<<<grid, Cfg::THREADS, smem, st>>>(a);
-        cuda_check(cudaGetLastError(), "k_ucol_bwd_pair launch");
-        g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
-        return;
-      }
+      // one-column CTAs: two columns a CTA, loaded or stored together
+      const size_t smem = (2 * size_t(FftBuf<M>::value) + M) * 2 * sizeof(R);
+      auto *kern = bwd ? k_ucol_bwd_pair<R, LOGM> : k_ucol_fwd_pair<R, LOGM>;
+      smem_attr(kern, smem);
+      dim3 grid((a.ny + 1) / 2, npl);
+      kern<<<grid, Cfg::THREADS, smem, st>>>(a);
+      cuda_check(cudaGetLastError(), bwd ? "k_ucol_bwd_pair launch" : "k_ucol_fwd_pair launch");
+      g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+      return;
     }
     const size_t smem = ColSmem2<R, M>::bytes();
     dim3 grid((a.ny + Cfg::NB - 1) / Cfg::NB, npl);
@@ -309,12 +326,7 @@ struct ColKernels {
       case 10: run1<10>(bwd, a, npl, st, err); break;
       case 11: run1<11>(bwd, a, npl, st, err); break;
       case 12: run1<12>(bwd, a, npl, st, err); break;
-      case 13:
-        if constexpr (sizeof(R) == 4) {
-          run1<13>(bwd, a, npl, st, err);
-          break;
-        }
-        [[fallthrough]];
+      case 13: run1<13>(bwd, a, npl, st, err); break;
       default: throw std::runtime_error("unsupported pruned FFT length");
     }
   }
