@@ -25,6 +25,7 @@
 #include <cuda.h>  // CUtensorMap (the type only; no driver-API calls here)
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <type_traits>
 
 namespace wsg {
 
@@ -100,6 +101,15 @@ __device__ __forceinline__ double2 cexp_turns(double t) {
   double s, c;
   sincospi(2.0 * t, &s, &c);
   return make_double2(c, s);
+}
+
+// exp(2 pi i t) to FP32 accuracy: the argument reduced in turns in FP64, the
+// sine and cosine of the remainder (|t| <= 1/2) in FP32.
+__device__ __forceinline__ float2 cexp_turns_f(double t) {
+  t -= rint(t);
+  float s, c;
+  sincospif(2.0f * float(t), &s, &c);
+  return make_float2(c, s);
 }
 
 // Complex sum and difference: one packed two-lane instruction each in FP32
@@ -2789,6 +2799,18 @@ __device__ __forceinline__ void pixel_terms(const ScreenArgs &s, int i, int j,
   q = nm1 + s.nshift;
 }
 
+// The w-screen phase factor exp(2 pi i t) in the precision of the grid: in
+// mixed precision the argument is reduced in FP64 and the rest is FP32
+// (phases good to ~1e-7 turns, far inside the 1e-5 accuracy that mixed
+// precision serves); FP64 throughout otherwise.
+template <typename R>
+__device__ __forceinline__ auto screen_phase(double t) {
+  if constexpr (sizeof(R) == 4)
+    return cexp_turns_f(t);
+  else
+    return cexp_turns(t);
+}
+
 // Image row of entry mm of H-row segment k2, or -1 for an entry that holds
 // no image row.  A screen CTA covers 32 consecutive entries of one segment
 // (blockIdx.x = k2 * nbs + block) by 32 image columns, so that its H
@@ -2799,12 +2821,13 @@ __device__ __forceinline__ int screen_row(const ScreenArgs &s, int k2, int mm) {
 }
 
 // ms2dirty: img(i,j) += corr(i,j) * sum_p Re(H[p][j][pos(i)] * exp(-2 pi i w_p q)),
-// FP64 phases (recurrence over planes) and FP64 accumulation.
+// FP64 pixel terms, the phases by a recurrence over planes in the grid's
+// precision (screen_phase), FP64 accumulation of the per-block sums.
 template <typename R>
 // out_mode 0: img += the sum (FP64 accumulator); 1 / 2: out = the sum as
 // FP32 / FP64 (the caller's image, when one pass covers all planes and
 // nothing is accumulated)
-__global__ void __launch_bounds__(256) k_screen_add(ScreenArgs s, const void *Hv, double *img,
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 3) k_screen_add(ScreenArgs s, const void *Hv, double *img,
                                                     void *out, int out_mode) {
   using C = typename Cplx<R>::type;
   const C *H = reinterpret_cast<const C *>(Hv);
@@ -2831,12 +2854,12 @@ __global__ void __launch_bounds__(256) k_screen_add(ScreenArgs s, const void *Hv
       bool inside;
       pixel_terms(s, i, j, corr, q, inside);
       const bool screen = s.do_w && inside;
-      double2 sc = make_double2(1.0, 0.0), st = make_double2(1.0, 0.0);
-      if (screen) {
-        const double w0 = s.wmin + s.pb0 * s.dw;
-        sc = cexp_turns(-w0 * q);
-        st = cexp_turns(-s.dw * q);
-      }
+      using SC = typename std::conditional<sizeof(R) == 4, float2, double2>::type;
+      SC sc, st;
+      sc.x = st.x = 1;
+      sc.y = st.y = 0;
+      const double w0 = s.wmin + s.pb0 * s.dw;
+      if (screen) st = screen_phase<R>(-s.dw * q);
       double acc = 0;
       for (int p0 = 0; p0 < s.npl; p0 += PB) {
         if (p0 > 0) {
@@ -2845,15 +2868,20 @@ __global__ void __launch_bounds__(256) k_screen_add(ScreenArgs s, const void *Hv
             if (p0 + u < s.npl) hb[u] = hp[(p0 + u) * pstride];
         }
         if (screen) {
+          // in FP32 each block of PB planes starts from its exact phase, so
+          // that the recurrence's rounding does not build up over many planes
+          if (sizeof(R) == 4 || p0 == 0) sc = screen_phase<R>(-(w0 + p0 * s.dw) * q);
+          R part = 0;
 #pragma unroll
           for (int u = 0; u < PB; ++u) {
             if (p0 + u < s.npl) {
-              acc += double(hb[u].x) * sc.x - double(hb[u].y) * sc.y;
-              const double nr = sc.x * st.x - sc.y * st.y;
+              part += hb[u].x * sc.x - hb[u].y * sc.y;
+              const auto nr = sc.x * st.x - sc.y * st.y;
               sc.y = sc.x * st.y + sc.y * st.x;
               sc.x = nr;
             }
           }
+          acc += double(part);
         } else {
 #pragma unroll
           for (int u = 0; u < PB; ++u)
@@ -2915,16 +2943,23 @@ __global__ void __launch_bounds__(256) k_screen_put(ScreenArgs s, const void *im
     C *hp = H + size_t(j) * hrow + (size_t(k2) * s.hseg + mm0 + tx);
     if (s.do_w && inside) {
       const double w0 = s.wmin + s.pb0 * s.dw;
-      double2 sc = cexp_turns(w0 * q);
-      const double2 st = cexp_turns(s.dw * q);
-      for (int p = 0; p < s.npl; ++p) {
-        C o;
-        o.x = R(val * sc.x);
-        o.y = R(val * sc.y);
-        hp[p * pstride] = o;
-        const double nr = sc.x * st.x - sc.y * st.y;
-        sc.y = sc.x * st.y + sc.y * st.x;
-        sc.x = nr;
+      const auto st = screen_phase<R>(s.dw * q);
+      const R rv = R(val);
+      auto sc = st;
+      for (int p0 = 0; p0 < s.npl; p0 += 16) {
+        // (in FP32 the exact phase at the start of every 16 planes, as in
+        // k_screen_add)
+        if (sizeof(R) == 4 || p0 == 0) sc = screen_phase<R>((w0 + p0 * s.dw) * q);
+        const int pe = min(s.npl, p0 + 16);
+        for (int p = p0; p < pe; ++p) {
+          C o;
+          o.x = rv * sc.x;
+          o.y = rv * sc.y;
+          hp[p * pstride] = o;
+          const auto nr = sc.x * st.x - sc.y * st.y;
+          sc.y = sc.x * st.y + sc.y * st.x;
+          sc.x = nr;
+        }
       }
     } else {
       for (int p = 0; p < s.npl; ++p) {
