@@ -166,8 +166,8 @@ int wsg_tuning_choice(const wsg_args *a, size_t nvis_all, double wmin, double wm
  * image whose kernels all need a longer grid is rejected), so the grid can
  * differ from wsg_ms2dirty's; results agree within epsilon.
  * The first call in a CUDA context (once per device, again after a device
- * reset) looks up the array's device address and should come before any
- * stream capture.  The call synchronises its stream: it reads the visibility
+ * reset) looks up the array's device address.  The call synchronises its
+ * stream: it reads the visibility
  * scan's statistics back to the host to plan the grid.  All calls share the
  * array: calls that overlap on the GPU race and must be serialised by the
  * caller.  stream may be NULL (the legacy default stream).  The image is

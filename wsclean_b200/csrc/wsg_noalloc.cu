@@ -26,9 +26,9 @@ namespace wsg {
 // address is looked up (cudaGetSymbolAddress, with the device current) on the
 // first call in each CUDA context -- once per device, unless the device was
 // reset and a new context created, in which case the module is loaded again,
-// the array may move and the lookup is repeated.  That first call should come
-// before any stream capture.  The call synchronises its stream while it runs
-// (it reads the visibility scan's statistics back to plan the grid).  All
+// the array may move and the lookup is repeated.  The call synchronises its
+// stream while it runs (it reads the visibility scan's statistics back to
+// plan the grid).  All
 // calls share the one array: calls that overlap on the GPU (different
 // streams, or different host threads on one device) race on it and must be
 // serialised by the caller.  Each call clears what must start at zero (image,
