@@ -97,3 +97,21 @@ def test_long_transforms_match_dft_and_adjoint(ctx, prec, nx, ny, frac, nu, m):
     # M: the band rounded up to a power of two; K = nu / M passes
     assert st["nu"] == nu
     assert 1 << int(np.ceil(np.log2(st["band_rows"]))) == m
+
+
+# Occupied u bands wider than the longest pruned column transform (8192
+# points): the grid keeps every u row (nu of any 2,3,5,7-smooth length) and
+# the u transform runs over whole grid columns; once with all w planes in
+# one pass, once five planes a pass.
+@pytest.mark.parametrize("prec", ["mixed", "fp64"])
+@pytest.mark.parametrize("max_planes", [0, 5])
+def test_bands_wider_than_the_pruned_transform(ctx, monkeypatch, prec, max_planes):
+    nx, ny, frac = 6000, 32, 0.45
+    if max_planes:
+        monkeypatch.setenv("WSG_MAX_PLANES", str(max_planes))
+    rng, uvw, freq, vis, px = _problem(nx, ny, 77 + max_planes, frac)
+    vis = vis.astype(np.complex64 if prec == "mixed" else np.complex128)
+    st = _check(ctx, prec, nx, ny, rng, uvw, freq, vis, px, dict(KW, sigma_min=1.5))
+    assert st["band_rows"] == st["nu"] > 8192
+    if max_planes:
+        assert st["plane_batch"] <= max_planes < st["nplanes"]

@@ -75,6 +75,25 @@ def test_plan_mixed_bench_workload():
     assert s["nplanes"] == int(1764.0 / s["dw"] + s["supp"])
 
 
+def test_plan_keeps_pruned_bands_up_to_8192_rows_in_both_precisions():
+    # config 5's geometry (8192^2 at 2", |u| px up to 0.2): a 6.7k-row band,
+    # pruned 8192-point column transforms in two twisted passes
+    for prec, eps in (("mixed", 1e-5), ("fp64", 1e-12)):
+        s = plan(npix_x=8192, npix_y=8192, pixsize_x=2 * ARCSEC, pixsize_y=2 * ARCSEC,
+                 epsilon=eps, precision=prec, wmax=8400.0, umax=0.2 / (2 * ARCSEC))
+        assert 4096 < s["band_rows"] <= 8192 and s["nu"] == 16384
+
+
+def test_plan_wider_bands_keep_every_u_row():
+    # 16384^2 at 2" with |u| px up to 0.2, and 8192^2 at 3 pixels a beam: the
+    # band exceeds the longest pruned column transform, so the grid keeps
+    # every u row (the library FFT transforms whole columns)
+    for n, f in ((16384, 0.2), (8192, 0.33)):
+        s = plan(npix_x=n, npix_y=n, pixsize_x=2 * ARCSEC, pixsize_y=2 * ARCSEC,
+                 wmax=0.4 * f / (2 * ARCSEC), umax=f / (2 * ARCSEC))
+        assert s["band_rows"] == s["nu"] >= 1.1 * n and s["nu"] % 2 == 0
+
+
 def test_plan_fp64_uses_wider_kernel():
     m = plan()
     d = plan(precision="fp64", epsilon=1e-12)

@@ -300,6 +300,13 @@ void set_band(GridPlan &g) {
   }
 }
 
+// Every u row of the grid (the library-FFT layout, GridPlan::ucufft).
+void set_full_band(GridPlan &g) {
+  g.band_full = true;
+  g.Lu = g.nu / 2;
+  g.band_rows = g.nu;
+}
+
 }  // namespace
 
 // Shared memory of one spread / interpolation CTA: the W-plane tile of
@@ -379,11 +386,19 @@ void choose_grid(GridPlan &g, double sigma_min, double sigma_max, int tile, bool
   KernelSpec bestk{};
   size_t bnu = 0, bnv = 0;
   int blogM = 0, bK = 1;
+  bool bucufft = false;
   for (const auto &k : cands) {
     if (g.force_W && (k.W != g.force_W || std::fabs(k.sigma - g.force_sigma) > 1e-12)) continue;
     GridPlan t = g;
     t.kernel = k;
-    if (!pick_nu(g.nx * k.sigma, umax_px, k.W, t.nu, t.logM, t.K)) continue;
+    t.ucufft = false;
+    if (!pick_nu(g.nx * k.sigma, umax_px, k.W, t.nu, t.logM, t.K)) {
+      if (pow2_v) continue;  // (the allocation-free path has no library FFT)
+      t.nu = 2 * good_size_v(size_t(g.nx * k.sigma * 0.5) + 1);
+      t.logM = 0;
+      t.K = 1;
+      t.ucufft = true;
+    }
     t.nv = 2 * good_size_v(size_t(g.ny * k.sigma * 0.5) + 1);
     if (pow2_v) {
       size_t p2 = 256;
@@ -392,6 +407,7 @@ void choose_grid(GridPlan &g, double sigma_min, double sigma_max, int tile, bool
       t.nv = p2;
     }
     set_band(t);
+    if (t.ucufft) set_full_band(t);
     double planes = 1;
     if (g.do_w) {
       double of = std::min(double(t.nu) / g.nx, double(t.nv) / g.ny);
@@ -399,9 +415,13 @@ void choose_grid(GridPlan &g, double sigma_min, double sigma_max, int tile, bool
       planes = std::floor((g.wmax_d - g.wmin_d) / dw + k.W);
     }
     const double M = double(size_t(1) << t.logM);
-    double per_plane = cs * (4.0 * t.band_rows * t.nv + 1.0 * t.band_rows * g.ny +
-                             3.0 * g.nx * g.ny) / hbm +
-                       c_fftpt * g.ny * t.K * M * t.logM / 148.0;
+    // (the library's column FFT transforms all nv columns, nu points each,
+    // and moves the whole grid twice more)
+    double per_plane = t.ucufft
+        ? cs * (8.0 * t.band_rows * t.nv + 3.0 * g.nx * g.ny) / hbm +
+              c_fftpt * t.nv * double(t.nu) * std::log2(double(t.nu)) / 148.0
+        : cs * (4.0 * t.band_rows * t.nv + 1.0 * t.band_rows * g.ny + 3.0 * g.nx * g.ny) / hbm +
+              c_fftpt * g.ny * t.K * M * t.logM / 148.0;
     double fft = planes * per_plane;
     double grid = double(g.nvis) * k.W * k.W * (g.do_w ? k.W : 1) * c_cell;
     double cost = fft + grid;
@@ -412,6 +432,7 @@ void choose_grid(GridPlan &g, double sigma_min, double sigma_max, int tile, bool
       bnv = t.nv;
       blogM = t.logM;
       bK = t.K;
+      bucufft = t.ucufft;
     }
   }
   require(bnu > 0, "no grid size satisfies the pruned-FFT layout (image or band too large)");
@@ -421,6 +442,7 @@ void choose_grid(GridPlan &g, double sigma_min, double sigma_max, int tile, bool
   g.nv = bnv;
   g.logM = blogM;
   g.K = bK;
+  g.ucufft = bucufft;
   g.ofactor = std::min(double(g.nu) / g.nx, double(g.nv) / g.ny);
   const int W = bestk.W;
   g.nsafe = (W + 1) / 2;
@@ -442,7 +464,9 @@ void choose_grid(GridPlan &g, double sigma_min, double sigma_max, int tile, bool
     g.nplanes = 1;
   }
   set_band(g);
-  if (g.band_full)
+  if (g.ucufft)
+    set_full_band(g);
+  else if (g.band_full)
     require(g.K == 1 && (size_t(1) << g.logM) == g.nu, "internal: full band needs K == 1");
   else
     require((size_t(1) << g.logM) >= g.band_rows, "internal: band exceeds the pruned FFT");

@@ -189,10 +189,20 @@ cufftHandle Context::fft_plan(int n, int istride, int idist, int ostride, int od
   cufftHandle h;
   CF(cufftCreate(&h));
   CF(cufftSetAutoAllocation(h, 0));
-  int nn = n, inembed = n, onembed = n;
   size_t work = 0;
-  CF(cufftMakePlanMany(h, 1, &nn, &inembed, istride, idist, &onembed, ostride, odist,
-                       dbl ? CUFFT_Z2Z : CUFFT_C2C, batch, &work));
+  // the 64-bit interface only where an element index can pass 2^31 (a batch
+  // of whole grid columns, or a large band grid)
+  const long long last_in = (long long)(batch - 1) * idist + (long long)(n - 1) * istride;
+  const long long last_out = (long long)(batch - 1) * odist + (long long)(n - 1) * ostride;
+  if (std::max(last_in, last_out) < (1LL << 31) - 1) {
+    int nn = n, inembed = n, onembed = n;
+    CF(cufftMakePlanMany(h, 1, &nn, &inembed, istride, idist, &onembed, ostride, odist,
+                         dbl ? CUFFT_Z2Z : CUFFT_C2C, batch, &work));
+  } else {
+    long long nn = n, inembed = n, onembed = n;
+    CF(cufftMakePlanMany64(h, 1, &nn, &inembed, istride, idist, &onembed, ostride, odist,
+                           dbl ? CUFFT_Z2Z : CUFFT_C2C, batch, &work));
+  }
   fft_work_need = std::max(fft_work_need, work);
   fft_plans[key] = h;
   return h;
@@ -599,6 +609,29 @@ size_t Context::choose_planes(const GridPlan &g, bool gridding) {
   return std::min(P, g.nplanes);
 }
 
+// The u transform of whole grid columns by the library FFT (the layout of
+// GridPlan::ucufft), plane by plane: plane p's columns are nv interleaved
+// sequences of nu entries at stride P nv in the grid layout [nu][P][nv], and
+// one row of nu entries each in the row layout [P][nv][nu].  dir backward:
+// grid -> rows (ms2dirty); forward: rows -> grid (dirty2ms).
+void Context::u_columns(void *grid_side, void *rows_side, const GridPlan &g, size_t P, size_t npl,
+                        int dir, bool dbl) {
+  const size_t cs = dbl ? 16 : 8, nu = g.nu, nv = g.nv;
+  require(P * nv < (size_t(1) << 31) && nu * nv < (size_t(1) << 31),
+          "grid too large for the library u transform");
+  const bool to_rows = dir == CUFFT_INVERSE;
+  cufftHandle h = to_rows ? fft_plan(int(nu), int(P * nv), 1, 1, int(nu), int(nv), dbl)
+                          : fft_plan(int(nu), 1, int(nu), int(P * nv), 1, int(nv), dbl);
+  for (size_t p = 0; p < npl; ++p) {
+    char *gp = static_cast<char *>(grid_side) + p * nv * cs;
+    char *rp = static_cast<char *>(rows_side) + p * nv * nu * cs;
+    if (to_rows)
+      fft_exec(h, gp, rp, dir, dbl);
+    else
+      fft_exec(h, rp, gp, dir, dbl);
+  }
+}
+
 template <typename R>
 bool Context::grid_core(const wsg_args &a, const Staged &s, double *img, bool accumulate,
                         void *direct_out, size_t ld) {
@@ -647,9 +680,10 @@ bool Context::grid_core(const wsg_args &a, const Staged &s, double *img, bool ac
   const size_t rowsP = gp.band_rows * P;
   char *band = reinterpret_cast<char *>(b_band.ensure(rowsP * nv * cs));
   char *bandf = reinterpret_cast<char *>(b_bandf.ensure(rowsP * nv * cs));
-  char *H = reinterpret_cast<char *>(b_H.ensure(P * gp.ny * gp.hrow() * cs));
-  const void *tw = upload_twiddles(gp, dbl);
-  ColArgs ca = make_col(gp, P, tw, bandf, H);
+  // (whole-column transforms write their rows back into `band`)
+  char *H = gp.ucufft ? band : reinterpret_cast<char *>(b_H.ensure(P * gp.ny * gp.hrow() * cs));
+  ColArgs ca{};
+  if (!gp.ucufft) ca = make_col(gp, P, upload_twiddles(gp, dbl), bandf, H);
   const long Lv = band_v_halfwidth(gp);
   const TileLayout tl = make_layout(gp.T, gp.kernel.W);
   const size_t smem = grid_smem_bytes<R>(tl, gp.kernel.W, true);
@@ -686,8 +720,15 @@ bool Context::grid_core(const wsg_args &a, const Staged &s, double *img, bool ac
       cufftHandle h = fft_plan(int(nv), 1, int(nv), 1, int(nv), int(rowsP), dbl);
       fft_exec(h, band, bandf, dir, dbl);
     }
-    // pruned transform along u: band rows of the image columns -> image rows
-    col_run<R>(gp.logM, true, ca, int(npl), stream, d_err);
+    if (gp.ucufft) {
+      // whole grid columns along u (stride P nv in bandf), plane by plane,
+      // into rows of nu entries, [P][nv][nu], in `band`
+      u_columns(bandf, band, gp, P, npl, dir, dbl);
+      band_dirty = BandDirty{};  // every entry of `band` written
+    } else {
+      // pruned transform along u: band rows of the image columns -> image rows
+      col_run<R>(gp.logM, true, ca, int(npl), stream, d_err);
+    }
     CK(cudaEventRecord(ev[4], stream));
     ScreenArgs sa = make_screen(gp, cf_cur, cc, P);
     sa.pb0 = int(pb0);
@@ -765,9 +806,15 @@ void Context::degrid_core(const wsg_args &a, const Staged &s, const double *img,
   const size_t rowsP = gp.band_rows * P;
   char *bandi = reinterpret_cast<char *>(b_bandd.ensure(rowsP * nv * cs));
   char *band = reinterpret_cast<char *>(b_bandf.ensure(rowsP * nv * cs));
-  char *H = reinterpret_cast<char *>(b_H.ensure(P * gp.ny * gp.hrow() * cs));
-  const void *tw = upload_twiddles(gp, dbl);
-  ColArgs ca = make_col(gp, P, tw, bandi, H);
+  // (whole-column transforms: the screen writes rows of nu entries,
+  // [P][nv][nu], into `bandi`, zero outside the image's rows and columns)
+  char *H = gp.ucufft ? bandi : reinterpret_cast<char *>(b_H.ensure(P * gp.ny * gp.hrow() * cs));
+  ColArgs ca{};
+  if (!gp.ucufft) ca = make_col(gp, P, upload_twiddles(gp, dbl), bandi, H);
+  if (gp.ucufft) {
+    bandd_zero = BandDirty{};
+    CK(cudaMemsetAsync(bandi, 0, rowsP * nv * cs, stream));
+  }
   const TileLayout tl = make_layout(gp.T, gp.kernel.W);
   const size_t smem = grid_smem_bytes<R>(tl, gp.kernel.W, false);
   int *counter = reinterpret_cast<int *>(reinterpret_cast<char *>(b_small.p) + 2048);
@@ -808,18 +855,24 @@ void Context::degrid_core(const wsg_args &a, const Staged &s, const double *img,
     const int src_f32 = (direct_in && a.dirty_type == WSG_F32) ? 1 : 0;
     launch_screen_put<R>(sg, stream, sa, src, src_f32, H);
     CK(cudaEventRecord(ev[3], stream));
-    // pruned transform along u (transposed): image rows -> band rows of the
-    // image columns; the other columns of the band grid stay zero
-    const BandDirty zl{bandi, rowsP, nv, cs, long(gp.ny)};
-    if (!(bandd_zero.p == zl.p && bandd_zero.rows == zl.rows && bandd_zero.nv == zl.nv &&
-          bandd_zero.cs == zl.cs && bandd_zero.Lv == zl.Lv)) {
-      bandd_zero = BandDirty{};
-      clear_outside_columns(bandi, rowsP, nv, gp.ny, cs, stream);
-      bandd_zero = zl;
-    }
-    col_run<R>(gp.logM, false, ca, int(npl), stream, d_err);
-    // transform along v
-    {
+    if (gp.ucufft) {
+      // whole grid columns: rows of nu entries (`bandi`) -> grid columns
+      // along u in `band` (stride P nv), then along v in place
+      u_columns(band, bandi, gp, P, npl, dir, dbl);
+      cufftHandle h = fft_plan(int(nv), 1, int(nv), 1, int(nv), int(rowsP), dbl);
+      fft_exec(h, band, band, dir, dbl);
+    } else {
+      // pruned transform along u (transposed): image rows -> band rows of the
+      // image columns; the other columns of the band grid stay zero
+      const BandDirty zl{bandi, rowsP, nv, cs, long(gp.ny)};
+      if (!(bandd_zero.p == zl.p && bandd_zero.rows == zl.rows && bandd_zero.nv == zl.nv &&
+            bandd_zero.cs == zl.cs && bandd_zero.Lv == zl.Lv)) {
+        bandd_zero = BandDirty{};
+        clear_outside_columns(bandi, rowsP, nv, gp.ny, cs, stream);
+        bandd_zero = zl;
+      }
+      col_run<R>(gp.logM, false, ca, int(npl), stream, d_err);
+      // transform along v
       cufftHandle h = fft_plan(int(nv), 1, int(nv), 1, int(nv), int(rowsP), dbl);
       fft_exec(h, bandi, band, dir, dbl);
     }

@@ -177,6 +177,8 @@ class Context {
   // be zero (Lv holds ny; p == nullptr: unknown)
   BandDirty bandd_zero;
   void clear_band(void *band, size_t rows, size_t nv, size_t cs);
+  void u_columns(void *grid_side, void *rows_side, const GridPlan &g, size_t P, size_t npl,
+                 int dir, bool dbl);
   DevBuf b_img, b_img2, b_acc, b_fftwork, b_out;
 
  private:

@@ -2760,6 +2760,7 @@ struct ScreenArgs {
   int do_w, divide_by_n;
   int P, pb0, npl;          // layout planes, first plane, planes in this pass
   int K, hseg, hm0, nbs;    // H row layout (ColArgs), 32-entry blocks per segment
+  int ufull;                // H holds whole transformed grid columns (GridPlan::ucufft)
   const double *cfu, *cfv;  // nx/2+1, ny/2+1 grid-correction factors
   double cheb[kDMaxCheb];   // corfunc(v) as Chebyshev series in y=v^2
   int ncheb;
@@ -2799,6 +2800,26 @@ __device__ __forceinline__ void pixel_terms(const ScreenArgs &s, int i, int j,
   q = nm1 + s.nshift;
 }
 
+// Offset in H of pixel (i, j)'s entry -- image row i being entry mm of
+// segment k2 -- in the first plane, and the stride between planes.  The
+// segmented rows: [P][ny][K hseg].  With whole transformed grid columns
+// (ufull): [P][nv][nu], grid column jx of image column j, entry u = i - nx/2
+// (mod nu) of the column's transform.
+__device__ __forceinline__ size_t screen_h_off(const ScreenArgs &s, int i, int j, int k2, int mm,
+                                               size_t &pstride) {
+  if (s.ufull) {
+    int jx = j + s.nv - s.ny / 2;
+    jx -= (jx >= s.nv) ? s.nv : 0;
+    int u = i - s.nx / 2;
+    u += (u < 0) ? s.nu : 0;
+    pstride = size_t(s.nv) * size_t(s.nu);
+    return size_t(jx) * size_t(s.nu) + size_t(u);
+  }
+  const size_t hrow = size_t(s.K) * s.hseg;
+  pstride = size_t(s.ny) * hrow;
+  return size_t(j) * hrow + (size_t(k2) * s.hseg + mm);
+}
+
 // The w-screen phase factor exp(2 pi i t) in the precision of the grid: in
 // mixed precision the argument is reduced in FP64 and the rest is FP32
 // (phases good to ~1e-7 turns, far inside the 1e-5 accuracy that mixed
@@ -2836,7 +2857,6 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 3) k_screen_add(Scre
   const int j0 = blockIdx.y * 32;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
   const int i = screen_row(s, k2, mm0 + tx);
-  const size_t hrow = size_t(s.K) * s.hseg;
   // planes loaded together; the first batch is in flight while the pixel's
   // FP64 terms are computed
   constexpr int PB = sizeof(R) == 4 ? 16 : 8;
@@ -2844,8 +2864,8 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 3) k_screen_add(Scre
     const int j = j0 + ty + 8 * k;
     double val = 0;
     if (i >= 0 && j < s.ny) {
-      const C *hp = H + size_t(j) * hrow + (size_t(k2) * s.hseg + mm0 + tx);
-      const size_t pstride = size_t(s.ny) * hrow;
+      size_t pstride;
+      const C *hp = H + screen_h_off(s, i, j, k2, mm0 + tx, pstride);
       C hb[PB];
 #pragma unroll
       for (int u = 0; u < PB; ++u)
@@ -2931,8 +2951,6 @@ __global__ void __launch_bounds__(256) k_screen_put(ScreenArgs s, const void *im
   }
   __syncthreads();
   const int i = screen_row(s, k2, mm0 + tx);
-  const size_t hrow = size_t(s.K) * s.hseg;
-  const size_t pstride = size_t(s.ny) * hrow;
   for (int k = 0; k < 4; ++k) {
     const int j = j0 + ty + 8 * k;
     if (i < 0 || j >= s.ny) continue;
@@ -2940,7 +2958,8 @@ __global__ void __launch_bounds__(256) k_screen_put(ScreenArgs s, const void *im
     bool inside;
     pixel_terms(s, i, j, corr, q, inside);
     const double val = tile[ty + 8 * k][tx] * corr;
-    C *hp = H + size_t(j) * hrow + (size_t(k2) * s.hseg + mm0 + tx);
+    size_t pstride;
+    C *hp = H + screen_h_off(s, i, j, k2, mm0 + tx, pstride);
     if (s.do_w && inside) {
       const double w0 = s.wmin + s.pb0 * s.dw;
       const auto st = screen_phase<R>(s.dw * q);

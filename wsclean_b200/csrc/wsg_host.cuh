@@ -169,6 +169,7 @@ inline ScreenArgs make_screen(const GridPlan &g, const double *d_cf, const ChebC
   s.hseg = int(g.hseg());
   s.hm0 = g.hm0();
   s.nbs = int((g.hseg() + 31) / 32);
+  s.ufull = g.ucufft ? 1 : 0;
   s.cfu = d_cf;
   s.cfv = d_cf + g.nx / 2 + 1;
   s.ncheb = cc.n;

@@ -121,6 +121,13 @@ struct GridPlan {
   // nu = K * 2^logM with 2^logM >= band_rows: the u transform of an image
   // column is K pruned FFTs of length 2^logM
   int logM = 0, K = 1;
+  // No pruned layout fits (the occupied u band is wider than the longest
+  // column transform, 8192 points): the grid keeps every u row (band_full,
+  // K = 1, nu any 2,3,5,7-smooth length) and the u transform is a library
+  // FFT over whole grid columns, whose output rows (one per plane and grid
+  // column, nu entries) the w-screens read and write in place of the
+  // segmented rows below.
+  bool ucufft = false;
   // Layout of one u-transformed image row (the array between the u
   // transform and the w-screen): pixel row i, at s = i - nx/2 = K m + k2
   // (0 <= k2 < K), is written by the k2-th pruned FFT as its output m.  The

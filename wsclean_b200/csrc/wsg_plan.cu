@@ -152,6 +152,9 @@ void Plan::build(const std::vector<wsg_job> &js) {
     gp.force_W = forceW;
     gp.force_sigma = forceS;
     const bool any = cx_.prepare<R>(aj, sj, false, nullptr, gp);
+    require(!any || !gp.ucufft,
+            "plan job: the occupied u band exceeds the longest pruned column transform "
+            "(8192 points); grid this image with the single-call operators");
     if (forceW == 0 && any) {  // the largest job with active visibilities
       forceW = gp.kernel.W;
       forceS = gp.kernel.sigma;

@@ -65,6 +65,9 @@ StreamGridder::StreamGridder(Context &cx, const wsg_args &a, double wmin, double
   g.umax = umax;
   g.vmax = vmax;
   choose_grid(g, a.sigma_min, a.sigma_max, default_tile(!dbl_));
+  require(!g.ucufft,
+          "stream: the occupied u band exceeds the longest pruned column transform "
+          "(8192 points); grid this image with the single-call operators");
   g.fixed = true;
   const size_t cs = dbl_ ? 16 : 8;
   band_.ensure(g.band_rows * g.nplanes * g.nv * cs);
