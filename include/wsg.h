@@ -300,7 +300,9 @@ typedef struct {
  * mask, pixel sizes, epsilon, flags, sigma range, precision, vis_type,
  * dirty_type).  jobs: njobs job descriptions, or NULL for one job over all
  * channels with a->npix_x, npix_y, center_x, center_y.  The coordinate
- * arrays are read during the call only. */
+ * arrays are read during the call only.  A job whose occupied u band is
+ * wider than 8192 grid rows (which the single-call operators grid with a
+ * full-grid layout) is rejected with WSG_ERR_INVALID. */
 int wsg_plan_create(wsg_ctx *ctx, const wsg_args *a, const wsg_job *jobs, size_t njobs,
                     wsg_plan **out);
 int wsg_plan_destroy(wsg_plan *p);
@@ -337,7 +339,9 @@ int wsg_ctx_synchronize(wsg_ctx *ctx);
  * every chunk); nrows, uvw, wgt, mask are ignored.  wmin, wmax: |w| range
  * and umax, vmax: max |u|, |v| in wavelengths over all chunks (a chunk
  * outside is rejected); nvis: expected number of visibilities (kernel
- * choice only). */
+ * choice only).  An extent whose occupied u band is wider than 8192 grid
+ * rows is rejected with WSG_ERR_INVALID (the single-call operators take
+ * it). */
 typedef struct wsg_stream wsg_stream;
 int wsg_stream_create(wsg_ctx *ctx, const wsg_args *a, double wmin, double wmax, double umax,
                       double vmax, size_t nvis, wsg_stream **out);
