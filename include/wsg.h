@@ -339,9 +339,9 @@ int wsg_ctx_synchronize(wsg_ctx *ctx);
  * every chunk); nrows, uvw, wgt, mask are ignored.  wmin, wmax: |w| range
  * and umax, vmax: max |u|, |v| in wavelengths over all chunks (a chunk
  * outside is rejected); nvis: expected number of visibilities (kernel
- * choice only).  An extent whose occupied u band is wider than 8192 grid
- * rows is rejected with WSG_ERR_INVALID (the single-call operators take
- * it). */
+ * choice only).  The stream holds every w plane of its grid: with an
+ * occupied u band wider than 8192 grid rows that is the whole nu x nv grid
+ * a plane. */
 typedef struct wsg_stream wsg_stream;
 int wsg_stream_create(wsg_ctx *ctx, const wsg_args *a, double wmin, double wmax, double umax,
                       double vmax, size_t nvis, wsg_stream **out);

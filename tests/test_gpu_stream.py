@@ -240,3 +240,36 @@ def test_stream_fp64_long_transforms_in_plane_passes(monkeypatch):
     vref = G.dirty2ms(uvw, freq, model, px, px, 1e-12, precision="fp64",
                       vis_dtype=np.complex128, **kw)
     assert O.rel_rms(v, vref) < 1e-12
+
+
+def test_stream_band_wider_than_the_pruned_transform(monkeypatch):
+    """A u band wider than the longest pruned column transform (the full-grid
+    layout, u transform by the library FFT) through a stream, five planes a
+    pass: image and predictions equal the single calls'."""
+    from wsclean_b200 import gridder as G
+    monkeypatch.setenv("WSG_MAX_PLANES", "5")
+    rng = np.random.default_rng(10)
+    nrow, nx, ny = 4000, 6000, 32
+    freq = np.array([1.40e8, 1.45e8])
+    px = np.deg2rad(10 / 3600)
+    umax = 0.45 / px * 299792458.0 / freq.max()
+    uvw = rng.uniform(-1, 1, (nrow, 3)) * np.array([umax, umax, 0.2 * umax])
+    vis = (rng.normal(size=(nrow, 2)) + 1j * rng.normal(size=(nrow, 2))).astype(np.complex64)
+    ext = G.data_extent(uvw, freq)
+    parts = chunks(nrow, 3)
+    kw = dict(KW, sigma_min=1.5)
+    with G.Stream(freq, nx, ny, px, px, 1e-5, ext, nvis=vis.size, dirty_dtype=np.float64,
+                  **kw) as s:
+        for a, b in parts:
+            s.add(uvw[a:b], vis[a:b])
+        d = s.finish()
+        st = s.stats()
+        assert st["band_rows"] == st["nu"] > 8192 and st["nplanes"] > 5
+        model = np.zeros((nx, ny), np.float32)
+        model[rng.integers(0, nx, 20), rng.integers(0, ny, 20)] = 1.0
+        s.predict_begin(model)
+        v = np.concatenate([s.predict(uvw[a:b]) for a, b in parts])
+    ref = G.ms2dirty(uvw, freq, vis, nx, ny, px, px, 1e-5, dirty_dtype=np.float64, **kw)
+    assert O.rel_rms(d, ref) < 5e-6
+    vref = G.dirty2ms(uvw, freq, model, px, px, 1e-5, **kw)
+    assert O.rel_rms(v, vref) < 1e-6

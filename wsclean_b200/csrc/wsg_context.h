@@ -355,6 +355,7 @@ class StreamGridder {
   Staged stage(Slot &sl, size_t nrows, const double *uvw, const void *vis, const void *wgt,
                const uint8_t *mask);
   size_t plane_batch() const;
+  size_t row_plane_bytes() const;
   // Gridding batches: the chunks passed to add() are gathered on the device
   // and sorted and spread together, so that a (tile, w-plane) bin holds the
   // records of many chunks and its tile is flushed to the grid once for all

@@ -65,23 +65,22 @@ StreamGridder::StreamGridder(Context &cx, const wsg_args &a, double wmin, double
   g.umax = umax;
   g.vmax = vmax;
   choose_grid(g, a.sigma_min, a.sigma_max, default_tile(!dbl_));
-  require(!g.ucufft,
-          "stream: the occupied u band exceeds the longest pruned column transform "
-          "(8192 points); grid this image with the single-call operators");
   g.fixed = true;
   const size_t cs = dbl_ ? 16 : 8;
   band_.ensure(g.band_rows * g.nplanes * g.nv * cs);
   img_.ensure(g.nx * g.ny * sizeof(double));
   cc_ = cx_.upload_corrections(g);
-  const void *twd = cx_.upload_twiddles(g, dbl_);
+  const void *twd = g.ucufft ? nullptr : cx_.upload_twiddles(g, dbl_);
   CK(cudaStreamSynchronize(cx_.stream));  // the uploads are stream-ordered
   const size_t ncf = g.nx / 2 + 1 + g.ny / 2 + 1;
   cf_.ensure(ncf * sizeof(double));
   CK(cudaMemcpy(cf_.p, cx_.cf_cur, ncf * sizeof(double), cudaMemcpyDeviceToDevice));
-  const size_t M = size_t(1) << g.logM;
-  const size_t ntw = col_table_entries(M, size_t(g.K)) * cs;
-  tw_.ensure(ntw);
-  CK(cudaMemcpy(tw_.p, twd, ntw, cudaMemcpyDeviceToDevice));
+  if (!g.ucufft) {  // (whole-column transforms use the library FFT, no tables)
+    const size_t M = size_t(1) << g.logM;
+    const size_t ntw = col_table_entries(M, size_t(g.K)) * cs;
+    tw_.ensure(ntw);
+    CK(cudaMemcpy(tw_.p, twd, ntw, cudaMemcpyDeviceToDevice));
+  }
   CF(cufftCreate(&fft_));
   CF(cufftSetAutoAllocation(fft_, 0));
   int n = int(g.nv), inembed = n, onembed = n;
@@ -89,7 +88,7 @@ StreamGridder::StreamGridder(Context &cx, const wsg_args &a, double wmin, double
   CF(cufftMakePlanMany(fft_, 1, &n, &inembed, 1, n, &onembed, 1, n, dbl_ ? CUFFT_Z2Z : CUFFT_C2C,
                        int(g.band_rows * g.nplanes), &work));
   fftwork_.ensure(std::max<size_t>(work, 256));
-  H_.ensure(plane_batch() * g.hrow() * g.ny * cs);
+  H_.ensure(plane_batch() * row_plane_bytes());
   CK(cudaStreamCreateWithFlags(&copy_, cudaStreamNonBlocking));
   for (auto &sl : slots_) {
     CK(cudaEventCreateWithFlags(&sl.copied, cudaEventDisableTiming));
@@ -142,12 +141,19 @@ StreamGridder::~StreamGridder() {
   for (DevBuf *b : {&band_, &H_, &img_, &cf_, &tw_, &fftwork_, &vout_, &lambda_}) b->release();
 }
 
+// Bytes of one plane's u-transformed rows: ny segmented rows of hrow
+// entries, or (whole-column transforms) nv rows of nu entries.
+size_t StreamGridder::row_plane_bytes() const {
+  const size_t cs = dbl_ ? 16 : 8;
+  return gp_.ucufft ? gp_.nv * gp_.nu * cs : gp_.hrow() * gp_.ny * cs;
+}
+
 // Planes per pass of the final transforms (the u-transformed rows of a pass
 // are held in H): all of them when they fit in a quarter of the free memory.
 size_t StreamGridder::plane_batch() const {
   size_t freeb = 0, total = 0;
   CK(cudaMemGetInfo(&freeb, &total));
-  const size_t per = gp_.hrow() * gp_.ny * (dbl_ ? 16 : 8);
+  const size_t per = row_plane_bytes();
   size_t P = std::max<size_t>(1, std::min<size_t>(gp_.nplanes, (freeb / 4) / std::max<size_t>(per, 1)));
   const int lim = env_int("WSG_MAX_PLANES", 0);  // a test and debugging limit
   if (lim > 0) P = std::min<size_t>(P, size_t(lim));
@@ -372,9 +378,8 @@ void StreamGridder::finish_t(void *dirty, int accumulate) {
   else
     CF(cufftExecC2C(fft_, reinterpret_cast<cufftComplex *>(band_.p),
                     reinterpret_cast<cufftComplex *>(band_.p), CUFFT_INVERSE));
-  // planes per pass: as many u-transformed plane images (ny rows of hrow
-  // entries) as H holds
-  const size_t P = std::max<size_t>(1, H_.n / (g.hrow() * g.ny * cs));
+  // planes per pass: as many planes of u-transformed rows as H holds
+  const size_t P = std::max<size_t>(1, H_.n / row_plane_bytes());
   int *d_err = reinterpret_cast<int *>(reinterpret_cast<char *>(cx_.b_small.p) + 3072);
   if (!err_armed_) {
     CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
@@ -383,8 +388,13 @@ void StreamGridder::finish_t(void *dirty, int accumulate) {
   for (size_t p0 = 0; p0 < g.nplanes; p0 += P) {
     const size_t np = std::min(P, g.nplanes - p0);
     // the band layout is [row][plane][nv]: a pass starts p0 planes into each row
-    ColArgs ca = make_col(g, g.nplanes, tw_.p, static_cast<char *>(band_.p) + p0 * g.nv * cs, H_.p);
-    col_run<R>(g.logM, true, ca, int(np), st, d_err);
+    char *band_p0 = static_cast<char *>(band_.p) + p0 * g.nv * cs;
+    if (g.ucufft) {
+      cx_.u_columns(band_p0, H_.p, g, g.nplanes, np, CUFFT_INVERSE, sizeof(R) == 8);
+    } else {
+      ColArgs ca = make_col(g, g.nplanes, tw_.p, band_p0, H_.p);
+      col_run<R>(g.logM, true, ca, int(np), st, d_err);
+    }
     ScreenArgs sa = make_screen(g, reinterpret_cast<const double *>(cf_.p), cc_, np);
     sa.pb0 = int(p0);
     sa.npl = int(np);
@@ -422,9 +432,11 @@ void StreamGridder::predict_begin_t(const double *img) {
   int *d_err = reinterpret_cast<int *>(reinterpret_cast<char *>(cx_.b_small.ensure(4096)) + 3072);
   CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
   CK(cudaMemsetAsync(band_.p, 0, band_.n, st));
-  // planes per pass: as many u-transformed plane images (ny rows of hrow
-  // entries) as H holds
-  const size_t P = std::max<size_t>(1, H_.n / (g.hrow() * g.ny * cs));
+  // (whole-column rows: zero outside the image's rows and columns, which the
+  // screen does not write)
+  if (g.ucufft) CK(cudaMemsetAsync(H_.p, 0, H_.n, st));
+  // planes per pass: as many planes of u-transformed rows as H holds
+  const size_t P = std::max<size_t>(1, H_.n / row_plane_bytes());
   for (size_t p0 = 0; p0 < g.nplanes; p0 += P) {
     const size_t np = std::min(P, g.nplanes - p0);
     ScreenArgs sa = make_screen(g, reinterpret_cast<const double *>(cf_.p), cc_, np);
@@ -432,8 +444,13 @@ void StreamGridder::predict_begin_t(const double *img) {
     sa.npl = int(np);
     const dim3 sg = screen_grid(g);
     launch_screen_put<R>(sg, st, sa, img, 0, H_.p);
-    ColArgs ca = make_col(g, g.nplanes, tw_.p, static_cast<char *>(band_.p) + p0 * g.nv * cs, H_.p);
-    col_run<R>(g.logM, false, ca, int(np), st, d_err);  // (the staged forms report on d_err)
+    char *band_p0 = static_cast<char *>(band_.p) + p0 * g.nv * cs;
+    if (g.ucufft) {
+      cx_.u_columns(band_p0, H_.p, g, g.nplanes, np, CUFFT_FORWARD, sizeof(R) == 8);
+    } else {
+      ColArgs ca = make_col(g, g.nplanes, tw_.p, band_p0, H_.p);
+      col_run<R>(g.logM, false, ca, int(np), st, d_err);  // (the staged forms report on d_err)
+    }
   }
   CF(cufftSetStream(fft_, st));
   CF(cufftSetWorkArea(fft_, fftwork_.p));
