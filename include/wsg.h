@@ -117,7 +117,9 @@ void wsg_args_init(wsg_args *a);
 
 /* Replaces ducc0::ms2dirty (wgridder.h:1696-1710): dirty = gridded image of
  * vis (nrows x nchan of vis_type).  If accumulate != 0 the result is added to
- * dirty instead of overwriting it. */
+ * dirty instead of overwriting it.  Limits beyond the reference's checks: at
+ * most 2^31 - 1 visibilities a call, and an oversampled grid below 65535
+ * cells a side (WSG_ERR_INVALID otherwise). */
 int wsg_ms2dirty(wsg_ctx *ctx, const wsg_args *a, const void *vis, void *dirty,
                  int accumulate);
 /* Replaces ducc0::dirty2ms (wgridder.h:1712-1729), the exact adjoint. */
