@@ -302,9 +302,7 @@ typedef struct {
  * mask, pixel sizes, epsilon, flags, sigma range, precision, vis_type,
  * dirty_type).  jobs: njobs job descriptions, or NULL for one job over all
  * channels with a->npix_x, npix_y, center_x, center_y.  The coordinate
- * arrays are read during the call only.  A job whose occupied u band is
- * wider than 8192 grid rows (which the single-call operators grid with a
- * full-grid layout) is rejected with WSG_ERR_INVALID. */
+ * arrays are read during the call only. */
 int wsg_plan_create(wsg_ctx *ctx, const wsg_args *a, const wsg_job *jobs, size_t njobs,
                     wsg_plan **out);
 int wsg_plan_destroy(wsg_plan *p);

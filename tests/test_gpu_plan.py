@@ -254,3 +254,35 @@ def test_context_outlives_its_plans():
     view = L.lib().wsg_gridder_ctx(g._h)
     assert L.lib().wsg_ctx_set_async(ctypes.c_void_p(view), 1) == L.WSG_ERR_INVALID
     g.close()
+
+
+@pytest.mark.parametrize("prec,tol", [("mixed", 1e-6), ("fp64", 1e-12)])
+def test_plan_band_wider_than_the_pruned_transform(prec, tol):
+    """A job whose u band is wider than the longest pruned column transform
+    (the full-grid layout, u transform by the library FFT): plan calls equal
+    the single calls."""
+    from wsclean_b200 import gridder as G
+    rng = np.random.default_rng(12)
+    nrow, nx, ny = 4000, 6000, 32
+    freq = np.array([1.40e8, 1.45e8])
+    px = np.deg2rad(10 / 3600)
+    umax = 0.45 / px * 299792458.0 / freq.max()
+    uvw = rng.uniform(-1, 1, (nrow, 3)) * np.array([umax, umax, 0.2 * umax])
+    vdt = np.complex64 if prec == "mixed" else np.complex128
+    vis = (rng.normal(size=(nrow, 2)) + 1j * rng.normal(size=(nrow, 2))).astype(vdt)
+    eps = 1e-5 if prec == "mixed" else 1e-12
+    kw = dict(KW, sigma_min=1.5)
+    with G.Plan(uvw, freq, px, px, eps, nx, ny, precision=prec, vis_dtype=vdt,
+                dirty_dtype=np.float64, **kw) as plan:
+        d = plan.ms2dirty(torch.as_tensor(vis, device=DEV))[0]
+        model = torch.as_tensor(rng.normal(size=(nx, ny)), device=DEV)
+        v = plan.dirty2ms(model)
+        torch.cuda.synchronize()
+        st = plan.stats(0)
+        assert st["band_rows"] == st["nu"] > 8192
+    raw = G.ms2dirty(uvw, freq, vis, nx, ny, px, px, eps, precision=prec,
+                     dirty_dtype=np.float64, **kw)
+    assert O.rel_rms(d.cpu().numpy(), raw) < tol
+    rawv = G.dirty2ms(uvw, freq, model.cpu().numpy(), px, px, eps, precision=prec,
+                      vis_dtype=vdt, **kw)
+    assert O.rel_rms(v.cpu().numpy(), rawv) < tol

@@ -262,6 +262,8 @@ struct PlanJob {
   size_t tw_off = 0;        // bytes in the plan's twiddle buffer
   ChebCorr cc;
   cufftHandle fft = 0;
+  // whole-column u transforms (GridPlan::ucufft): grid -> rows, rows -> grid
+  cufftHandle ufft_rows = 0, ufft_grid = 0;
 };
 
 // Reusable plan over one or more jobs sharing the visibilities.
