@@ -609,27 +609,54 @@ size_t Context::choose_planes(const GridPlan &g, bool gridding) {
   return std::min(P, g.nplanes);
 }
 
-// The u transform of whole grid columns by the library FFT (the layout of
-// GridPlan::ucufft), plane by plane: plane p's columns are nv interleaved
-// sequences of nu entries at stride P nv in the grid layout [nu][P][nv], and
-// one row of nu entries each in the row layout [P][nv][nu].  dir backward:
-// grid -> rows (ms2dirty); forward: rows -> grid (dirty2ms).
-void Context::u_columns(void *grid_side, void *rows_side, const GridPlan &g, size_t P, size_t npl,
-                        int dir, bool dbl) {
-  const size_t cs = dbl ? 16 : 8, nu = g.nu, nv = g.nv;
-  require(P * nv < (size_t(1) << 31) && nu * nv < (size_t(1) << 31),
-          "grid too large for the library u transform");
-  const bool to_rows = dir == CUFFT_INVERSE;
-  cufftHandle h = to_rows ? fft_plan(int(nu), int(P * nv), 1, 1, int(nu), int(nv), dbl)
-                          : fft_plan(int(nu), 1, int(nu), int(P * nv), 1, int(nv), dbl);
+// The 2-D transform of one plane in place in the grid layout [nu][P][nv]
+// (row stride P nv), the whole-grid layout's transform (GridPlan::ucufft).
+// 64-bit sizes: the rows of a large grid span more than 2^31 entries.
+cufftHandle make_grid_fft_plan(size_t nu, size_t nv, size_t P, bool dbl, size_t &work) {
+  cufftHandle h;
+  CF(cufftCreate(&h));
+  CF(cufftSetAutoAllocation(h, 0));
+  long long n[2] = {(long long)nu, (long long)nv};
+  long long emb[2] = {(long long)nu, (long long)(P * nv)};
+  work = 0;
+  CF(cufftMakePlanMany64(h, 2, n, emb, 1, (long long)nv, emb, 1, (long long)nv,
+                         dbl ? CUFFT_Z2Z : CUFFT_C2C, 1, &work));
+  return h;
+}
+
+// Runs the plane transform of make_grid_fft_plan on npl consecutive planes
+// starting at grid (plane p at p nv entries).
+void exec_grid_fft(cufftHandle h, void *grid, size_t nv, size_t npl, int dir, bool dbl,
+                   cudaStream_t st, void *work) {
+  const size_t cs = dbl ? 16 : 8;
+  CF(cufftSetStream(h, st));
+  CF(cufftSetWorkArea(h, work));
   for (size_t p = 0; p < npl; ++p) {
-    char *gp = static_cast<char *>(grid_side) + p * nv * cs;
-    char *rp = static_cast<char *>(rows_side) + p * nv * nu * cs;
-    if (to_rows)
-      fft_exec(h, gp, rp, dir, dbl);
+    void *g = static_cast<char *>(grid) + p * nv * cs;
+    if (dbl)
+      CF(cufftExecZ2Z(h, reinterpret_cast<cufftDoubleComplex *>(g),
+                      reinterpret_cast<cufftDoubleComplex *>(g), dir));
     else
-      fft_exec(h, rp, gp, dir, dbl);
+      CF(cufftExecC2C(h, reinterpret_cast<cufftComplex *>(g), reinterpret_cast<cufftComplex *>(g),
+                      dir));
   }
+}
+
+// The context's cached plane transform for a grid layout of P planes.
+void Context::grid_fft(void *grid, const GridPlan &g, size_t P, size_t npl, int dir, bool dbl) {
+  auto key = std::make_tuple(-int(g.nu), int(g.nv), int(P), 0, 0, 1, int(dbl));
+  auto it = fft_plans.find(key);
+  cufftHandle h;
+  if (it != fft_plans.end()) {
+    h = it->second;
+  } else {
+    size_t work = 0;
+    h = make_grid_fft_plan(g.nu, g.nv, P, dbl, work);
+    fft_work_need = std::max(fft_work_need, work);
+    fft_plans[key] = h;
+  }
+  void *work = b_fftwork.ensure(std::max<size_t>(fft_work_need, 256));
+  exec_grid_fft(h, grid, g.nv, npl, dir, dbl, stream, work);
 }
 
 template <typename R>
@@ -679,9 +706,9 @@ bool Context::grid_core(const wsg_args &a, const Staged &s, double *img, bool ac
   // so `band` stays zero outside the columns the spread wrote
   const size_t rowsP = gp.band_rows * P;
   char *band = reinterpret_cast<char *>(b_band.ensure(rowsP * nv * cs));
-  char *bandf = reinterpret_cast<char *>(b_bandf.ensure(rowsP * nv * cs));
-  // (whole-column transforms write their rows back into `band`)
-  char *H = gp.ucufft ? band : reinterpret_cast<char *>(b_H.ensure(P * gp.ny * gp.hrow() * cs));
+  // (the whole-grid layout transforms in place and screens the grid itself)
+  char *bandf = gp.ucufft ? nullptr : reinterpret_cast<char *>(b_bandf.ensure(rowsP * nv * cs));
+  char *H = gp.ucufft ? nullptr : reinterpret_cast<char *>(b_H.ensure(P * gp.ny * gp.hrow() * cs));
   ColArgs ca{};
   if (!gp.ucufft) ca = make_col(gp, P, upload_twiddles(gp, dbl), bandf, H);
   const long Lv = band_v_halfwidth(gp);
@@ -715,17 +742,14 @@ bool Context::grid_core(const wsg_args &a, const Staged &s, double *img, bool ac
     grid_dispatch<R>(gp.kernel.W, true, num_sms, smem, stream, ga, g, kc);
     band_dirty = BandDirty{band, rowsP, nv, cs, Lv};
     CK(cudaEventRecord(ev[3], stream));
-    // transform along v: every (band row, plane) is a contiguous row of nv
-    {
-      cufftHandle h = fft_plan(int(nv), 1, int(nv), 1, int(nv), int(rowsP), dbl);
-      fft_exec(h, band, bandf, dir, dbl);
-    }
     if (gp.ucufft) {
-      // whole grid columns along u (stride P nv in bandf), plane by plane,
-      // into rows of nu entries, [P][nv][nu], in `band`
-      u_columns(bandf, band, gp, P, npl, dir, dbl);
+      // the whole grid: each plane's 2-D transform in place
+      grid_fft(band, gp, P, npl, dir, dbl);
       band_dirty = BandDirty{};  // every entry of `band` written
     } else {
+      // transform along v: every (band row, plane) is a contiguous row of nv
+      cufftHandle h = fft_plan(int(nv), 1, int(nv), 1, int(nv), int(rowsP), dbl);
+      fft_exec(h, band, bandf, dir, dbl);
       // pruned transform along u: band rows of the image columns -> image rows
       col_run<R>(gp.logM, true, ca, int(npl), stream, d_err);
     }
@@ -735,7 +759,10 @@ bool Context::grid_core(const wsg_args &a, const Staged &s, double *img, bool ac
     sa.npl = int(npl);
     sa.ld = ld;
     const dim3 sg = screen_grid(gp);
-    launch_screen_add<R>(sg, stream, sa, H, img, direct_out, out_mode);
+    if (gp.ucufft)
+      launch_screen_add_grid<R>(sg, stream, sa, band, img, direct_out, out_mode);
+    else
+      launch_screen_add<R>(sg, stream, sa, H, img, direct_out, out_mode);
     CK(cudaEventRecord(ev[5], stream));
     float t = 0;
     if (!async_mode) CK(cudaEventSynchronize(ev[5]));
@@ -804,17 +831,13 @@ void Context::degrid_core(const wsg_args &a, const Staged &s, const double *img,
   // other columns stay zero from call to call; the v transform goes out of
   // place to `band`, which the interpolation reads
   const size_t rowsP = gp.band_rows * P;
-  char *bandi = reinterpret_cast<char *>(b_bandd.ensure(rowsP * nv * cs));
+  // (the whole-grid layout: the screen writes the grid `band` itself, which
+  // is transformed in place)
+  char *bandi = gp.ucufft ? nullptr : reinterpret_cast<char *>(b_bandd.ensure(rowsP * nv * cs));
   char *band = reinterpret_cast<char *>(b_bandf.ensure(rowsP * nv * cs));
-  // (whole-column transforms: the screen writes rows of nu entries,
-  // [P][nv][nu], into `bandi`, zero outside the image's rows and columns)
-  char *H = gp.ucufft ? bandi : reinterpret_cast<char *>(b_H.ensure(P * gp.ny * gp.hrow() * cs));
+  char *H = gp.ucufft ? nullptr : reinterpret_cast<char *>(b_H.ensure(P * gp.ny * gp.hrow() * cs));
   ColArgs ca{};
   if (!gp.ucufft) ca = make_col(gp, P, upload_twiddles(gp, dbl), bandi, H);
-  if (gp.ucufft) {
-    bandd_zero = BandDirty{};
-    CK(cudaMemsetAsync(bandi, 0, rowsP * nv * cs, stream));
-  }
   const TileLayout tl = make_layout(gp.T, gp.kernel.W);
   const size_t smem = grid_smem_bytes<R>(tl, gp.kernel.W, false);
   int *counter = reinterpret_cast<int *>(reinterpret_cast<char *>(b_small.p) + 2048);
@@ -853,14 +876,16 @@ void Context::degrid_core(const wsg_args &a, const Staged &s, const double *img,
     // the caller's image itself (FP32 or FP64) when given, else the FP64 copy
     const void *src = direct_in ? direct_in : static_cast<const void *>(img);
     const int src_f32 = (direct_in && a.dirty_type == WSG_F32) ? 1 : 0;
-    launch_screen_put<R>(sg, stream, sa, src, src_f32, H);
+    if (gp.ucufft) {
+      // zero outside the image's rows and columns, which the screen leaves
+      CK(cudaMemsetAsync(band, 0, rowsP * nv * cs, stream));
+      launch_screen_put_grid<R>(sg, stream, sa, src, src_f32, band);
+    } else {
+      launch_screen_put<R>(sg, stream, sa, src, src_f32, H);
+    }
     CK(cudaEventRecord(ev[3], stream));
     if (gp.ucufft) {
-      // whole grid columns: rows of nu entries (`bandi`) -> grid columns
-      // along u in `band` (stride P nv), then along v in place
-      u_columns(band, bandi, gp, P, npl, dir, dbl);
-      cufftHandle h = fft_plan(int(nv), 1, int(nv), 1, int(nv), int(rowsP), dbl);
-      fft_exec(h, band, band, dir, dbl);
+      grid_fft(band, gp, P, npl, dir, dbl);  // each plane's 2-D transform in place
     } else {
       // pruned transform along u (transposed): image rows -> band rows of the
       // image columns; the other columns of the band grid stay zero

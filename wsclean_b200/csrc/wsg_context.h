@@ -177,8 +177,7 @@ class Context {
   // be zero (Lv holds ny; p == nullptr: unknown)
   BandDirty bandd_zero;
   void clear_band(void *band, size_t rows, size_t nv, size_t cs);
-  void u_columns(void *grid_side, void *rows_side, const GridPlan &g, size_t P, size_t npl,
-                 int dir, bool dbl);
+  void grid_fft(void *grid, const GridPlan &g, size_t P, size_t npl, int dir, bool dbl);
   DevBuf b_img, b_img2, b_acc, b_fftwork, b_out;
 
  private:
@@ -253,6 +252,13 @@ class Context {
 };
 
 // One job of a plan (see wsg_plan_create).
+// The 2-D transform of one plane in place in the grid layout [nu][P][nv]
+// (the whole-grid layout, GridPlan::ucufft), and its execution over npl
+// consecutive planes (wsg_context.cu).
+cufftHandle make_grid_fft_plan(size_t nu, size_t nv, size_t P, bool dbl, size_t &work);
+void exec_grid_fft(cufftHandle h, void *grid, size_t nv, size_t npl, int dir, bool dbl,
+                   cudaStream_t st, void *work);
+
 struct PlanJob {
   GridPlan gp;              // the job's grid (shared kernel)
   size_t chan0 = 0, chan1 = 0;
@@ -262,8 +268,7 @@ struct PlanJob {
   size_t tw_off = 0;        // bytes in the plan's twiddle buffer
   ChebCorr cc;
   cufftHandle fft = 0;
-  // whole-column u transforms (GridPlan::ucufft): grid -> rows, rows -> grid
-  cufftHandle ufft_rows = 0, ufft_grid = 0;
+  cufftHandle gfft = 0;      // the whole-grid layout's plane transform (GridPlan::ucufft)
 };
 
 // Reusable plan over one or more jobs sharing the visibilities.

@@ -2760,7 +2760,6 @@ struct ScreenArgs {
   int do_w, divide_by_n;
   int P, pb0, npl;          // layout planes, first plane, planes in this pass
   int K, hseg, hm0, nbs;    // H row layout (ColArgs), 32-entry blocks per segment
-  int ufull;                // H holds whole transformed grid columns (GridPlan::ucufft)
   const double *cfu, *cfv;  // nx/2+1, ny/2+1 grid-correction factors
   double cheb[kDMaxCheb];   // corfunc(v) as Chebyshev series in y=v^2
   int ncheb;
@@ -2800,21 +2799,12 @@ __device__ __forceinline__ void pixel_terms(const ScreenArgs &s, int i, int j,
   q = nm1 + s.nshift;
 }
 
-// Offset in H of pixel (i, j)'s entry -- image row i being entry mm of
-// segment k2 -- in the first plane, and the stride between planes.  The
-// segmented rows: [P][ny][K hseg].  With whole transformed grid columns
-// (ufull): [P][nv][nu], grid column jx of image column j, entry u = i - nx/2
-// (mod nu) of the column's transform.
+// Offset in H, [P][ny][K hseg], of pixel (i, j)'s entry -- image row i
+// being entry mm of segment k2 -- in the first plane, and the stride between
+// planes.
 __device__ __forceinline__ size_t screen_h_off(const ScreenArgs &s, int i, int j, int k2, int mm,
                                                size_t &pstride) {
-  if (s.ufull) {
-    int jx = j + s.nv - s.ny / 2;
-    jx -= (jx >= s.nv) ? s.nv : 0;
-    int u = i - s.nx / 2;
-    u += (u < 0) ? s.nu : 0;
-    pstride = size_t(s.nv) * size_t(s.nu);
-    return size_t(jx) * size_t(s.nu) + size_t(u);
-  }
+  (void)i;
   const size_t hrow = size_t(s.K) * s.hseg;
   pstride = size_t(s.ny) * hrow;
   return size_t(j) * hrow + (size_t(k2) * s.hseg + mm);
@@ -2987,6 +2977,128 @@ __global__ void __launch_bounds__(256) k_screen_put(ScreenArgs s, const void *im
         o.y = R(0);
         hp[p * pstride] = o;
       }
+    }
+  }
+}
+
+// ---- screens on the whole grid (GridPlan::ucufft) ----
+//
+// When the grid keeps every u row, the 2-D transform of a plane runs in
+// place in the grid layout [nu][P][nv], and the screens read or write that
+// layout directly: pixel (i, j) of plane p is grid entry (u, p, jx) with
+// u = i - nx/2 (mod nu) and jx = j - ny/2 (mod nv).  Threads run along j,
+// which is contiguous in both the grid and the x-major image.
+__device__ __forceinline__ size_t grid_cell(const ScreenArgs &s, int i, int j) {
+  int jx = j + s.nv - s.ny / 2;
+  jx -= (jx >= s.nv) ? s.nv : 0;
+  int u = i - s.nx / 2;
+  u += (u < 0) ? s.nu : 0;
+  return size_t(u) * size_t(s.P) * size_t(s.nv) + size_t(jx);
+}
+
+// ms2dirty: img(i,j) (+)= corr(i,j) * sum_p Re(G[u][p][jx] * exp(-2 pi i w_p q))
+// (out_mode as k_screen_add).  G points at the pass's first plane.
+template <typename R>
+__global__ void __launch_bounds__(256) k_screen_add_grid(ScreenArgs s, const void *Gv, double *img,
+                                                         void *out, int out_mode) {
+  using C = typename Cplx<R>::type;
+  const C *G = reinterpret_cast<const C *>(Gv);
+  const int j = blockIdx.x * 32 + (threadIdx.x & 31);
+  const int i = blockIdx.y * 8 + (threadIdx.x >> 5);
+  if (i >= s.nx || j >= s.ny) return;
+  constexpr int PB = sizeof(R) == 4 ? 16 : 8;
+  const C *gp = G + grid_cell(s, i, j);
+  C hb[PB];
+#pragma unroll
+  for (int u = 0; u < PB; ++u)
+    if (u < s.npl) hb[u] = gp[size_t(u) * s.nv];
+  double corr, q;
+  bool inside;
+  pixel_terms(s, i, j, corr, q, inside);
+  const bool screen = s.do_w && inside;
+  using SC = typename std::conditional<sizeof(R) == 4, float2, double2>::type;
+  SC sc, st;
+  sc.x = st.x = 1;
+  sc.y = st.y = 0;
+  const double w0 = s.wmin + s.pb0 * s.dw;
+  if (screen) st = screen_phase<R>(-s.dw * q);
+  double acc = 0;
+  for (int p0 = 0; p0 < s.npl; p0 += PB) {
+    if (p0 > 0) {
+#pragma unroll
+      for (int u = 0; u < PB; ++u)
+        if (p0 + u < s.npl) hb[u] = gp[size_t(p0 + u) * s.nv];
+    }
+    R part = 0;
+    if (screen) {
+      if (sizeof(R) == 4 || p0 == 0) sc = screen_phase<R>(-(w0 + p0 * s.dw) * q);
+#pragma unroll
+      for (int u = 0; u < PB; ++u) {
+        if (p0 + u < s.npl) {
+          part += hb[u].x * sc.x - hb[u].y * sc.y;
+          const auto nr = sc.x * st.x - sc.y * st.y;
+          sc.y = sc.x * st.y + sc.y * st.x;
+          sc.x = nr;
+        }
+      }
+    } else {
+#pragma unroll
+      for (int u = 0; u < PB; ++u)
+        if (p0 + u < s.npl) part += hb[u].x;
+    }
+    acc += double(part);
+  }
+  const double x = acc * corr;
+  const size_t o = size_t(i) * s.ld + j;
+  if (out_mode == 0)
+    img[o] += x;
+  else if (out_mode == 1)
+    reinterpret_cast<float *>(out)[o] = float(x);
+  else
+    reinterpret_cast<double *>(out)[o] = x;
+}
+
+// dirty2ms: G[u][p][jx] = dirty(i,j) * corr(i,j) * exp(+2 pi i w_p q) for the
+// pass's planes (the grid's other entries are left as they are: zero).
+template <typename R>
+__global__ void __launch_bounds__(256) k_screen_put_grid(ScreenArgs s, const void *img, int in_f32,
+                                                         void *Gv) {
+  using C = typename Cplx<R>::type;
+  C *G = reinterpret_cast<C *>(Gv);
+  const int j = blockIdx.x * 32 + (threadIdx.x & 31);
+  const int i = blockIdx.y * 8 + (threadIdx.x >> 5);
+  if (i >= s.nx || j >= s.ny) return;
+  const size_t o = size_t(i) * s.ld + j;
+  const double x = in_f32 ? double(reinterpret_cast<const float *>(img)[o])
+                          : reinterpret_cast<const double *>(img)[o];
+  double corr, q;
+  bool inside;
+  pixel_terms(s, i, j, corr, q, inside);
+  const R rv = R(x * corr);
+  C *gp = G + grid_cell(s, i, j);
+  if (s.do_w && inside) {
+    const double w0 = s.wmin + s.pb0 * s.dw;
+    const auto st = screen_phase<R>(s.dw * q);
+    auto sc = st;
+    for (int p0 = 0; p0 < s.npl; p0 += 16) {
+      if (sizeof(R) == 4 || p0 == 0) sc = screen_phase<R>((w0 + p0 * s.dw) * q);
+      const int pe = min(s.npl, p0 + 16);
+      for (int p = p0; p < pe; ++p) {
+        C v;
+        v.x = rv * sc.x;
+        v.y = rv * sc.y;
+        gp[size_t(p) * s.nv] = v;
+        const auto nr = sc.x * st.x - sc.y * st.y;
+        sc.y = sc.x * st.y + sc.y * st.x;
+        sc.x = nr;
+      }
+    }
+  } else {
+    for (int p = 0; p < s.npl; ++p) {
+      C v;
+      v.x = rv;
+      v.y = R(0);
+      gp[size_t(p) * s.nv] = v;
     }
   }
 }

@@ -169,7 +169,6 @@ inline ScreenArgs make_screen(const GridPlan &g, const double *d_cf, const ChebC
   s.hseg = int(g.hseg());
   s.hm0 = g.hm0();
   s.nbs = int((g.hseg() + 31) / 32);
-  s.ufull = g.ucufft ? 1 : 0;
   s.cfu = d_cf;
   s.cfv = d_cf + g.nx / 2 + 1;
   s.ncheb = cc.n;
@@ -202,8 +201,10 @@ inline ColArgs make_col(const GridPlan &g, size_t P, const void *tw, void *band,
 }
 
 // Screen kernel grid: 32-entry blocks of every H-row segment by 32 image
-// columns.
+// columns; for the whole-grid screens (GridPlan::ucufft), 32 image columns
+// by 8 image rows a block.
 inline dim3 screen_grid(const GridPlan &g) {
+  if (g.ucufft) return dim3(unsigned((g.ny + 31) / 32), unsigned((g.nx + 7) / 8));
   return dim3(unsigned(size_t(g.K) * ((g.hseg() + 31) / 32)), unsigned((g.ny + 31) / 32));
 }
 
@@ -247,6 +248,14 @@ void launch_screen_add(dim3 grid, cudaStream_t st, const ScreenArgs &s, const vo
 template <typename R>
 void launch_screen_put(dim3 grid, cudaStream_t st, const ScreenArgs &s, const void *img,
                        int in_f32, void *H);
+// The screens on the whole grid (GridPlan::ucufft): G is the grid layout
+// [nu][P][nv] at the pass's first plane (grid: screen_grid).
+template <typename R>
+void launch_screen_add_grid(dim3 grid, cudaStream_t st, const ScreenArgs &s, const void *G,
+                            double *img, void *out, int out_mode);
+template <typename R>
+void launch_screen_put_grid(dim3 grid, cudaStream_t st, const ScreenArgs &s, const void *img,
+                            int in_f32, void *G);
 
 // ------------------------------------------------------------ the driver
 

@@ -372,6 +372,21 @@ void launch_screen_put(dim3 grid, cudaStream_t st, const ScreenArgs &s, const vo
   g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
+template <typename R>
+void launch_screen_add_grid(dim3 grid, cudaStream_t st, const ScreenArgs &s, const void *G,
+                            double *img, void *out, int out_mode) {
+  k_screen_add_grid<R><<<grid, 256, 0, st>>>(s, G, img, out, out_mode);
+  cuda_check(cudaGetLastError(), "k_screen_add_grid launch");
+  g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+}
+template <typename R>
+void launch_screen_put_grid(dim3 grid, cudaStream_t st, const ScreenArgs &s, const void *img,
+                            int in_f32, void *G) {
+  k_screen_put_grid<R><<<grid, 256, 0, st>>>(s, img, in_f32, G);
+  cuda_check(cudaGetLastError(), "k_screen_put_grid launch");
+  g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+}
+
 #define WSG_LAUNCHERS(R)                                                                     \
   template size_t grid_smem_bytes<R>(const TileLayout &, int, bool);                         \
   template int grid_groups<R>(int);                                                          \
@@ -382,7 +397,11 @@ void launch_screen_put(dim3 grid, cudaStream_t st, const ScreenArgs &s, const vo
   template void launch_screen_add<R>(dim3, cudaStream_t, const ScreenArgs &, const void *,  \
                                      double *, void *, int);                                 \
   template void launch_screen_put<R>(dim3, cudaStream_t, const ScreenArgs &, const void *,  \
-                                     int, void *);
+                                     int, void *);                                           \
+  template void launch_screen_add_grid<R>(dim3, cudaStream_t, const ScreenArgs &,            \
+                                          const void *, double *, void *, int);             \
+  template void launch_screen_put_grid<R>(dim3, cudaStream_t, const ScreenArgs &,            \
+                                          const void *, int, void *);
 WSG_LAUNCHERS(float)
 WSG_LAUNCHERS(double)
 #undef WSG_LAUNCHERS

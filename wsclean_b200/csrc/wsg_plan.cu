@@ -54,7 +54,7 @@ Plan::~Plan() {
   for (auto &g : graphs_)
     if (g.exec) cudaGraphExecDestroy(g.exec);
   for (auto &j : jobs_)
-    for (cufftHandle h : {j.fft, j.ufft_rows, j.ufft_grid})
+    for (cufftHandle h : {j.fft, j.gfft})
       if (h) cufftDestroy(h);
   for (DevBuf *b : {&rec_, &chunks_, &chunk_job_, &jobgeom_, &band_, &H_, &img_, &cf_, &tw_, &acc_,
                     &small_, &fftwork_})
@@ -63,48 +63,6 @@ Plan::~Plan() {
 
 namespace {
 
-// cuFFT plan of one plane's whole-column u transforms (GridPlan::ucufft) in
-// a band layout of P planes: nv interleaved columns of nu entries at stride
-// P nv <-> nv rows of nu entries.  to_rows: grid -> rows.
-cufftHandle u_column_plan(const GridPlan &g, size_t P, bool to_rows, bool dbl, size_t &work) {
-  require(P * g.nv < (size_t(1) << 31) && g.nu * g.nv < (size_t(1) << 31),
-          "grid too large for the library u transform");
-  cufftHandle h;
-  CF(cufftCreate(&h));
-  CF(cufftSetAutoAllocation(h, 0));
-  long long n = (long long)g.nu, emb = n;
-  const long long cstride = (long long)(P * g.nv);
-  work = 0;
-  // (64-bit sizes: the columns of a large grid span more than 2^31 entries)
-  if (to_rows)
-    CF(cufftMakePlanMany64(h, 1, &n, &emb, cstride, 1, &emb, 1, n, dbl ? CUFFT_Z2Z : CUFFT_C2C,
-                           (long long)g.nv, &work));
-  else
-    CF(cufftMakePlanMany64(h, 1, &n, &emb, 1, n, &emb, cstride, 1, dbl ? CUFFT_Z2Z : CUFFT_C2C,
-                           (long long)g.nv, &work));
-  return h;
-}
-
-// Runs a u_column_plan over every plane: plane p's columns start p nv
-// entries into the band grid, its rows p nv nu entries into rows.
-void u_column_exec(cufftHandle h, const GridPlan &g, void *band, void *rows, int dir, bool dbl,
-                   cudaStream_t st, void *work) {
-  const size_t cs = dbl ? 16 : 8;
-  CF(cufftSetStream(h, st));
-  CF(cufftSetWorkArea(h, work));
-  for (size_t p = 0; p < g.nplanes; ++p) {
-    void *gp = static_cast<char *>(band) + p * g.nv * cs;
-    void *rp = static_cast<char *>(rows) + p * g.nv * g.nu * cs;
-    void *in = dir == CUFFT_INVERSE ? gp : rp;
-    void *out = dir == CUFFT_INVERSE ? rp : gp;
-    if (dbl)
-      CF(cufftExecZ2Z(h, reinterpret_cast<cufftDoubleComplex *>(in),
-                      reinterpret_cast<cufftDoubleComplex *>(out), dir));
-    else
-      CF(cufftExecC2C(h, reinterpret_cast<cufftComplex *>(in), reinterpret_cast<cufftComplex *>(out),
-                      dir));
-  }
-}
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 }  // namespace
 
@@ -262,7 +220,7 @@ void Plan::build(const std::vector<wsg_job> &js) {
     PlanJob &pj = jobs_[j];
     if (pj.nrec == 0) continue;
     const GridPlan &gp = pj.gp;
-    hmax = std::max(hmax, gp.nplanes * (gp.ucufft ? gp.nv * gp.nu : gp.ny * gp.hrow()) * cs);
+    if (!gp.ucufft) hmax = std::max(hmax, gp.nplanes * gp.ny * gp.hrow() * cs);
     JobGeom &g = jg[j];
     g.nu = int(gp.nu);
     g.nv = int(gp.nv);
@@ -273,19 +231,18 @@ void Plan::build(const std::vector<wsg_job> &js) {
     g.pb0 = 0;
     g.pb1 = int(gp.nplanes);
     g.grid = static_cast<char *>(band_.p) + pj.band_off;
-    CF(cufftCreate(&pj.fft));
-    CF(cufftSetAutoAllocation(pj.fft, 0));
-    int n = int(gp.nv), inembed = n, onembed = n;
     size_t w = 0;
-    CF(cufftMakePlanMany(pj.fft, 1, &n, &inembed, 1, n, &onembed, 1, n,
-                         sizeof(R) == 8 ? CUFFT_Z2Z : CUFFT_C2C, int(gp.band_rows * gp.nplanes), &w));
-    work = std::max(work, w);
-    if (gp.ucufft) {
-      pj.ufft_rows = u_column_plan(gp, gp.nplanes, true, sizeof(R) == 8, w);
-      work = std::max(work, w);
-      pj.ufft_grid = u_column_plan(gp, gp.nplanes, false, sizeof(R) == 8, w);
-      work = std::max(work, w);
+    if (gp.ucufft) {  // the whole grid: each plane's 2-D transform in place
+      pj.gfft = make_grid_fft_plan(gp.nu, gp.nv, gp.nplanes, sizeof(R) == 8, w);
+    } else {
+      CF(cufftCreate(&pj.fft));
+      CF(cufftSetAutoAllocation(pj.fft, 0));
+      int n = int(gp.nv), inembed = n, onembed = n;
+      CF(cufftMakePlanMany(pj.fft, 1, &n, &inembed, 1, n, &onembed, 1, n,
+                           sizeof(R) == 8 ? CUFFT_Z2Z : CUFFT_C2C, int(gp.band_rows * gp.nplanes),
+                           &w));
     }
+    work = std::max(work, w);
   }
   H_.ensure(hmax);
   img_.ensure(max_npix_ * sizeof(double));
@@ -342,18 +299,18 @@ void Plan::enqueue_grid(const void *vis, void *const *dirty, int accumulate) {
       continue;
     }
     char *band = static_cast<char *>(band_.p) + pj.band_off;
-    CF(cufftSetStream(pj.fft, st));
-    CF(cufftSetWorkArea(pj.fft, fftwork_.p));
-    if (sizeof(R) == 8)
-      CF(cufftExecZ2Z(pj.fft, reinterpret_cast<cufftDoubleComplex *>(band),
-                      reinterpret_cast<cufftDoubleComplex *>(band), CUFFT_INVERSE));
-    else
-      CF(cufftExecC2C(pj.fft, reinterpret_cast<cufftComplex *>(band),
-                      reinterpret_cast<cufftComplex *>(band), CUFFT_INVERSE));
     if (gp.ucufft) {
-      u_column_exec(pj.ufft_rows, gp, band, H_.p, CUFFT_INVERSE, sizeof(R) == 8, st,
+      exec_grid_fft(pj.gfft, band, gp.nv, gp.nplanes, CUFFT_INVERSE, sizeof(R) == 8, st,
                     fftwork_.p);
     } else {
+      CF(cufftSetStream(pj.fft, st));
+      CF(cufftSetWorkArea(pj.fft, fftwork_.p));
+      if (sizeof(R) == 8)
+        CF(cufftExecZ2Z(pj.fft, reinterpret_cast<cufftDoubleComplex *>(band),
+                        reinterpret_cast<cufftDoubleComplex *>(band), CUFFT_INVERSE));
+      else
+        CF(cufftExecC2C(pj.fft, reinterpret_cast<cufftComplex *>(band),
+                        reinterpret_cast<cufftComplex *>(band), CUFFT_INVERSE));
       ColArgs ca = make_col(gp, gp.nplanes, static_cast<char *>(tw_.p) + pj.tw_off, band, H_.p);
       col_run<R>(gp.logM, true, ca, int(gp.nplanes), st, d_err);
     }
@@ -371,7 +328,10 @@ void Plan::enqueue_grid(const void *vis, void *const *dirty, int accumulate) {
     sa.pb0 = 0;
     sa.npl = int(gp.nplanes);
     const dim3 sg = screen_grid(gp);
-    launch_screen_add<R>(sg, st, sa, H_.p, img, nullptr, 0);
+    if (gp.ucufft)
+      launch_screen_add_grid<R>(sg, st, sa, band, img, nullptr, 0);
+    else
+      launch_screen_add<R>(sg, st, sa, H_.p, img, nullptr, 0);
     if (a_.dirty_type == WSG_F64)
       k_store_image<double><<<nb, 256, 0, st>>>(npix, img, (double *)dirty[j]);
     else
@@ -411,25 +371,25 @@ void Plan::enqueue_degrid(const void *const *dirty, void *vis) {
     const dim3 sg = screen_grid(gp);
     char *band = static_cast<char *>(band_.p) + pj.band_off;
     if (gp.ucufft) {
-      // whole-column rows, zero outside the image's rows and columns
-      CK(cudaMemsetAsync(H_.p, 0, gp.nplanes * gp.nv * gp.nu * cs, st));
-      launch_screen_put<R>(sg, st, sa, img, 0, H_.p);
-      u_column_exec(pj.ufft_grid, gp, band, H_.p, CUFFT_FORWARD, sizeof(R) == 8, st,
+      // the whole grid, zero outside the image, screened and transformed in place
+      CK(cudaMemsetAsync(band, 0, pj.band_bytes, st));
+      launch_screen_put_grid<R>(sg, st, sa, img, 0, band);
+      exec_grid_fft(pj.gfft, band, gp.nv, gp.nplanes, CUFFT_FORWARD, sizeof(R) == 8, st,
                     fftwork_.p);
     } else {
       launch_screen_put<R>(sg, st, sa, img, 0, H_.p);
       clear_outside_columns(band, gp.band_rows * gp.nplanes, gp.nv, gp.ny, cs, st);
       ColArgs ca = make_col(gp, gp.nplanes, static_cast<char *>(tw_.p) + pj.tw_off, band, H_.p);
       col_run<R>(gp.logM, false, ca, int(gp.nplanes), st, d_err);
+      CF(cufftSetStream(pj.fft, st));
+      CF(cufftSetWorkArea(pj.fft, fftwork_.p));
+      if (sizeof(R) == 8)
+        CF(cufftExecZ2Z(pj.fft, reinterpret_cast<cufftDoubleComplex *>(band),
+                        reinterpret_cast<cufftDoubleComplex *>(band), CUFFT_FORWARD));
+      else
+        CF(cufftExecC2C(pj.fft, reinterpret_cast<cufftComplex *>(band),
+                        reinterpret_cast<cufftComplex *>(band), CUFFT_FORWARD));
     }
-    CF(cufftSetStream(pj.fft, st));
-    CF(cufftSetWorkArea(pj.fft, fftwork_.p));
-    if (sizeof(R) == 8)
-      CF(cufftExecZ2Z(pj.fft, reinterpret_cast<cufftDoubleComplex *>(band),
-                      reinterpret_cast<cufftDoubleComplex *>(band), CUFFT_FORWARD));
-    else
-      CF(cufftExecC2C(pj.fft, reinterpret_cast<cufftComplex *>(band),
-                      reinterpret_cast<cufftComplex *>(band), CUFFT_FORWARD));
     g_kernel_launches.fetch_add(2, std::memory_order_relaxed);
   }
   CK(cudaMemsetAsync(counter, 0, sizeof(int), st));  // (the error word stays until read)

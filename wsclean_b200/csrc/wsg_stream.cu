@@ -88,7 +88,7 @@ StreamGridder::StreamGridder(Context &cx, const wsg_args &a, double wmin, double
   CF(cufftMakePlanMany(fft_, 1, &n, &inembed, 1, n, &onembed, 1, n, dbl_ ? CUFFT_Z2Z : CUFFT_C2C,
                        int(g.band_rows * g.nplanes), &work));
   fftwork_.ensure(std::max<size_t>(work, 256));
-  H_.ensure(plane_batch() * row_plane_bytes());
+  if (!g.ucufft) H_.ensure(plane_batch() * row_plane_bytes());
   CK(cudaStreamCreateWithFlags(&copy_, cudaStreamNonBlocking));
   for (auto &sl : slots_) {
     CK(cudaEventCreateWithFlags(&sl.copied, cudaEventDisableTiming));
@@ -142,10 +142,10 @@ StreamGridder::~StreamGridder() {
 }
 
 // Bytes of one plane's u-transformed rows: ny segmented rows of hrow
-// entries, or (whole-column transforms) nv rows of nu entries.
+// entries (none with the whole-grid layout, which is screened in place).
 size_t StreamGridder::row_plane_bytes() const {
   const size_t cs = dbl_ ? 16 : 8;
-  return gp_.ucufft ? gp_.nv * gp_.nu * cs : gp_.hrow() * gp_.ny * cs;
+  return gp_.ucufft ? 0 : gp_.hrow() * gp_.ny * cs;
 }
 
 // Planes per pass of the final transforms (the u-transformed rows of a pass
@@ -370,16 +370,22 @@ void StreamGridder::finish_t(void *dirty, int accumulate) {
   } else {
     CK(cudaMemsetAsync(img, 0, npix * sizeof(double), st));
   }
-  CF(cufftSetStream(fft_, st));
-  CF(cufftSetWorkArea(fft_, fftwork_.p));
-  if (sizeof(R) == 8)
-    CF(cufftExecZ2Z(fft_, reinterpret_cast<cufftDoubleComplex *>(band_.p),
-                    reinterpret_cast<cufftDoubleComplex *>(band_.p), CUFFT_INVERSE));
-  else
-    CF(cufftExecC2C(fft_, reinterpret_cast<cufftComplex *>(band_.p),
-                    reinterpret_cast<cufftComplex *>(band_.p), CUFFT_INVERSE));
-  // planes per pass: as many planes of u-transformed rows as H holds
-  const size_t P = std::max<size_t>(1, H_.n / row_plane_bytes());
+  if (g.ucufft) {
+    // the whole grid: each plane's 2-D transform in place, screened in place
+    cx_.grid_fft(band_.p, g, g.nplanes, g.nplanes, CUFFT_INVERSE, sizeof(R) == 8);
+  } else {
+    CF(cufftSetStream(fft_, st));
+    CF(cufftSetWorkArea(fft_, fftwork_.p));
+    if (sizeof(R) == 8)
+      CF(cufftExecZ2Z(fft_, reinterpret_cast<cufftDoubleComplex *>(band_.p),
+                      reinterpret_cast<cufftDoubleComplex *>(band_.p), CUFFT_INVERSE));
+    else
+      CF(cufftExecC2C(fft_, reinterpret_cast<cufftComplex *>(band_.p),
+                      reinterpret_cast<cufftComplex *>(band_.p), CUFFT_INVERSE));
+  }
+  // planes per pass: as many planes of u-transformed rows as H holds (all of
+  // them with the whole-grid layout)
+  const size_t P = g.ucufft ? g.nplanes : std::max<size_t>(1, H_.n / row_plane_bytes());
   int *d_err = reinterpret_cast<int *>(reinterpret_cast<char *>(cx_.b_small.p) + 3072);
   if (!err_armed_) {
     CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
@@ -389,17 +395,17 @@ void StreamGridder::finish_t(void *dirty, int accumulate) {
     const size_t np = std::min(P, g.nplanes - p0);
     // the band layout is [row][plane][nv]: a pass starts p0 planes into each row
     char *band_p0 = static_cast<char *>(band_.p) + p0 * g.nv * cs;
-    if (g.ucufft) {
-      cx_.u_columns(band_p0, H_.p, g, g.nplanes, np, CUFFT_INVERSE, sizeof(R) == 8);
-    } else {
-      ColArgs ca = make_col(g, g.nplanes, tw_.p, band_p0, H_.p);
-      col_run<R>(g.logM, true, ca, int(np), st, d_err);
-    }
-    ScreenArgs sa = make_screen(g, reinterpret_cast<const double *>(cf_.p), cc_, np);
+    ScreenArgs sa = make_screen(g, reinterpret_cast<const double *>(cf_.p), cc_, g.nplanes);
     sa.pb0 = int(p0);
     sa.npl = int(np);
     const dim3 sg = screen_grid(g);
-    launch_screen_add<R>(sg, st, sa, H_.p, img, nullptr, 0);
+    if (g.ucufft) {
+      launch_screen_add_grid<R>(sg, st, sa, band_p0, img, nullptr, 0);
+    } else {
+      ColArgs ca = make_col(g, g.nplanes, tw_.p, band_p0, H_.p);
+      col_run<R>(g.logM, true, ca, int(np), st, d_err);
+      launch_screen_add<R>(sg, st, sa, H_.p, img, nullptr, 0);
+    }
   }
   void *dout = ddev ? dirty : cx_.b_out.ensure(npix * dsz);
   if (a_.dirty_type == WSG_F64)
@@ -432,9 +438,17 @@ void StreamGridder::predict_begin_t(const double *img) {
   int *d_err = reinterpret_cast<int *>(reinterpret_cast<char *>(cx_.b_small.ensure(4096)) + 3072);
   CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
   CK(cudaMemsetAsync(band_.p, 0, band_.n, st));
-  // (whole-column rows: zero outside the image's rows and columns, which the
-  // screen does not write)
-  if (g.ucufft) CK(cudaMemsetAsync(H_.p, 0, H_.n, st));
+  if (g.ucufft) {
+    // the whole grid (zero outside the image, as cleared above): screened
+    // in place, then each plane's 2-D transform in place
+    ScreenArgs sa = make_screen(g, reinterpret_cast<const double *>(cf_.p), cc_, g.nplanes);
+    sa.pb0 = 0;
+    sa.npl = int(g.nplanes);
+    launch_screen_put_grid<R>(screen_grid(g), st, sa, img, 0, band_.p);
+    cx_.grid_fft(band_.p, g, g.nplanes, g.nplanes, CUFFT_FORWARD, sizeof(R) == 8);
+    cx_.check_device_error(d_err);
+    return;
+  }
   // planes per pass: as many planes of u-transformed rows as H holds
   const size_t P = std::max<size_t>(1, H_.n / row_plane_bytes());
   for (size_t p0 = 0; p0 < g.nplanes; p0 += P) {
@@ -444,13 +458,8 @@ void StreamGridder::predict_begin_t(const double *img) {
     sa.npl = int(np);
     const dim3 sg = screen_grid(g);
     launch_screen_put<R>(sg, st, sa, img, 0, H_.p);
-    char *band_p0 = static_cast<char *>(band_.p) + p0 * g.nv * cs;
-    if (g.ucufft) {
-      cx_.u_columns(band_p0, H_.p, g, g.nplanes, np, CUFFT_FORWARD, sizeof(R) == 8);
-    } else {
-      ColArgs ca = make_col(g, g.nplanes, tw_.p, band_p0, H_.p);
-      col_run<R>(g.logM, false, ca, int(np), st, d_err);  // (the staged forms report on d_err)
-    }
+    ColArgs ca = make_col(g, g.nplanes, tw_.p, static_cast<char *>(band_.p) + p0 * g.nv * cs, H_.p);
+    col_run<R>(g.logM, false, ca, int(np), st, d_err);  // (the staged forms report on d_err)
   }
   CF(cufftSetStream(fft_, st));
   CF(cufftSetWorkArea(fft_, fftwork_.p));
