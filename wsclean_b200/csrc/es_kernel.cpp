@@ -647,8 +647,11 @@ Facet tuning_facet(size_t nx, size_t ny, int nfx, int nfy, int ifx, int ify, dou
 
 size_t plan_bytes(const GridPlan &g, size_t planes, bool gridding) {
   const size_t cs = g.fp32 ? 8 : 16;
-  // both directions keep the grid and its v transform apart
   (void)gridding;
+  // the whole-grid layout transforms and screens one grid in place
+  if (g.ucufft) return planes * cs * g.band_rows * g.nv;
+  // both directions keep the grid and its v transform apart, plus the
+  // u-transformed rows
   return planes * cs * (2 * g.band_rows * g.nv + g.ny * g.hrow());
 }
 

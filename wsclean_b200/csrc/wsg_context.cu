@@ -190,8 +190,8 @@ cufftHandle Context::fft_plan(int n, int istride, int idist, int ostride, int od
   CF(cufftCreate(&h));
   CF(cufftSetAutoAllocation(h, 0));
   size_t work = 0;
-  // the 64-bit interface only where an element index can pass 2^31 (a batch
-  // of whole grid columns, or a large band grid)
+  // the 64-bit interface only where an element index can pass 2^31 (a large
+  // band grid)
   const long long last_in = (long long)(batch - 1) * idist + (long long)(n - 1) * istride;
   const long long last_out = (long long)(batch - 1) * odist + (long long)(n - 1) * ostride;
   if (std::max(last_in, last_out) < (1LL << 31) - 1) {
