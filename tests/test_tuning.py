@@ -95,7 +95,7 @@ def test_tuning_choice_matches_reference(nrow, nx, pxas, wmax, power, eps, nchan
 @pytest.mark.skipif(not O.ref_available(), reason="compiled reference missing")
 def test_tuning_choice_with_mask_and_shift():
     """The histogram counts masked-in visibilities only, and the field
-    centre moves the n-1 range the facets are judged by."""
+    centre moves the n-1 range that decides the facet split."""
     uvw, freq, vis, rng = _data(30000, 5000.0, 6.0, seed=7)
     mask = (rng.uniform(size=vis.shape) > 0.3).astype(np.uint8)
     px = np.deg2rad(60 / 3600)
