@@ -981,8 +981,9 @@ void Context::print_report(const GridPlan &g, bool gridding, size_t P) {
   if (g.do_w) std::printf("x%zu", g.nplanes);
   std::printf("), supp=%d, eps=%g (kernel %.3g, sigma %.2f)\n", g.kernel.W, g.eps, g.kernel.err,
               g.kernel.sigma);
-  std::printf("  nvis=%zu, w=[%g; %g], dw=%g, planes per pass=%zu, u band rows=%zu\n", g.nvis,
-              g.wmin_d, g.wmax_d, g.dw, P, g.band_rows);
+  std::printf("  nvis=%zu, w=[%g; %g], dw=%g, planes per pass=%zu, u band rows=%zu%s\n", g.nvis,
+              g.wmin_d, g.wmax_d, g.dw, P, g.band_rows,
+              g.ucufft ? " (whole grid, 2-D library FFT a plane)" : "");
   std::fflush(stdout);
 }
 
